@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the H.psi / Taylor path on B200.
+
+Workload (one "step"): one full FP64 Hamiltonian application H.psi
+(kinetic order-4 star + local potential + KB projectors) on the sphere system
+R = 12 bohr, h = 0.2 (904,089 inner points), 32 atoms x 9 projectors, 128
+complex128 states -- the configuration the headline metric is quoted on.
+Inputs are seeded synthetic data (no data set exists for this path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hpsi|reference]
+
+value  = point-states per second of H.psi with psi resident in HBM (the batch,
+         2.2 GB, is far larger than the 126 MB L2, so no flush is needed);
+e2e    = the same metric through the C ABI with pinned host buffers (the
+         host->device copy of psi and the device->host copy of H psi inside
+         the timed region of every step);
+extra  = FP32-storage H.psi, the fused Taylor step (FP64 and FP32).
+Multi-GPU: independent replicas (the path has no exchange step), weak scaling.
+--impl reference times the reference CPU path (the reference's own compiled
+stencil kernel plus the oracle's restatement of the rest) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "octopus-debian-package_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "H·ψ Gpoint-states/s (FP64, full H with KB)"
+UNIT = "Gpoint-states/s"
+WORKLOAD = "sphere R=12 h=0.2 (np=904089), 32 KB atoms x 9 projectors, 128 complex128 states"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="hpsi", choices=["hpsi", "reference"])
+    ap.add_argument("--small", action="store_true", help="small case (for profiler captures)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(path="profiles/pass_fp64_sphere128.md"):
+    """dram bytes per launch of the pass kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, path)) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_full_launch:"):
+                    return float(line.split(":")[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, gpu_index=0):
+        self.samples = []
+        self.proc = None
+        self.idx = gpu_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap,utilization.gpu",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                util = float(s[6])
+                if util < 50:
+                    continue
+                sm.append(float(s[0]))
+                mx = float(s[1])
+                for n, v in zip(names, s[2:6]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except Exception:
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(self.samples)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_system(small=False):
+    from hpsi import fixtures
+    if small:
+        return fixtures.config1(radius=8.0, spacing=0.2, natoms=8, nst=64, place_radius=5.5)
+    return fixtures.config1()
+
+
+def cpu_reference_rate(sysm, nst_sample, min_seconds=10.0, max_reps=200):
+    """Reference CPU H.psi rate (Gpoint-states/s) on a sample of the states."""
+    from oracle import oracle as O
+    from hpsi.stencil import laplacian_weights, star_points
+    m = sysm.mesh
+    P = O.Projectors(sysm.proj.maps, sysm.proj.mats, sysm.proj.scals) if sysm.proj else None
+    H = O.Hamiltonian(m, laplacian_weights(m.spacing), star_points(), v=sysm.v, projectors=P)
+    psi = np.ascontiguousarray(sysm.psi[:, :nst_sample])
+    H.apply(psi)  # warm
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        H.apply(psi)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or reps >= max_reps:
+            break
+    rate = m.np * nst_sample * reps / el / 1e9
+    kind = "reference" if H.used_reference_kernel else "port"
+    sample = (f"{reps} H.psi applications on {nst_sample} of the 128 states "
+              f"({el:.1f} s; stencil = reference operate.c compiled from source)" if kind == "reference"
+              else f"{reps} H.psi applications on {nst_sample} states ({el:.1f} s)")
+    return rate, H.nthreads, kind, sample
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference CPU path on the box's host cores."""
+    if rank != 0:
+        return
+    sysm = build_system(args.small)
+    from oracle import oracle as O
+    from hpsi.stencil import laplacian_weights, star_points
+    m = sysm.mesh
+    P = O.Projectors(sysm.proj.maps, sysm.proj.mats, sysm.proj.scals)
+    H = O.Hamiltonian(m, laplacian_weights(m.spacing), star_points(), v=sysm.v, projectors=P)
+    nst_sample = 8
+    psi = np.ascontiguousarray(sysm.psi[:, :nst_sample])
+    for _ in range(args.warmup):
+        H.apply(psi)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        H.apply(psi)
+    el = time.perf_counter() - t0
+    rate = m.np * nst_sample * args.steps / el / 1e9
+    kind = "reference" if H.used_reference_kernel else "port"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "sample_states": nst_sample},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": H.nthreads, "kind": kind,
+                         "sample": f"each step = one H.psi on {nst_sample} of the 128 states"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    sysm = build_system(args.small)
+    m = sysm.mesh
+    nst = sysm.psi.shape[1]
+    dm = lib.DeviceMesh(m)
+    ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=sysm.v, projectors=sysm.proj)
+    x = torch.from_numpy(sysm.psi).to(dev)
+    y = torch.zeros((m.np, nst), dtype=torch.complex128, device=dev)
+    st = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    # ---- headline: FP64 full H.psi, device resident ------------------------
+    for _ in range(args.warmup):
+        ham.apply(x, y)
+    torch.cuda.synchronize()
+    barrier()
+    n0 = lib.launch_count()
+    lib.profile_enable(True)
+    with Clocks(local) as clk:
+        ms = timed(lambda: ham.apply(x, y), args.steps, 0)
+    launches = lib.launch_count() - n0
+    npass, pass_ms = lib.profile_query("pass_fp64")
+    nbra, bra_ms = lib.profile_query("bra_fp64")
+    lib.profile_enable(False)
+    ms_step = ms / args.steps
+    value = world * m.np * nst * args.steps / (ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel (fused stencil pass)
+    S = 16
+    alg_bytes = m.np * nst * 2 * S + m.np * 8.0
+    pass_avg_ms = pass_ms / max(npass, 1)
+    achieved = alg_bytes / (pass_avg_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = profile_traffic()
+
+    # ---- extras: FP32 storage, Taylor steps ----------------------------------
+    x32 = x.to(torch.complex64)
+    y32 = y.to(torch.complex64)
+    ms32 = timed(lambda: ham.apply(x32, y32), args.steps, 2)
+    value32 = world * m.np * nst * args.steps / (ms32 / 1e3) / 1e9
+    tk = max(2, args.steps // 4)
+    xt = x.clone()
+    ms_t64 = timed(lambda: ham.taylor_step(xt, 0.02), tk, 1)
+    xt32 = x32.clone()
+    ms_t32 = timed(lambda: ham.taylor_step(xt32, 0.02), tk, 1)
+    del xt, xt32
+
+    # ---- e2e through the C ABI with pinned host buffers -----------------------
+    xh = torch.from_numpy(sysm.psi).pin_memory()
+    yh = torch.zeros((m.np, nst), dtype=torch.complex128).pin_memory()
+    ke = max(2, min(args.steps, 5))
+    for _ in range(1):
+        ham.apply(xh, yh)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        ham.apply(xh, yh)
+    torch.cuda.synchronize()
+    el = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * m.np * nst * ke / el / 1e9
+
+    # ---- CPU baseline (rank 0, N=1 only) -------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, kind, sample = cpu_reference_rate(sysm, 8)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD + (" [small]" if args.small else ""),
+                       "step": "one H.psi (kinetic + local + KB) over the whole batch",
+                       "l2": "inputs (2.2 GB) larger than L2; no flush",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(m.np_part * nst * S),
+                    "d2h_bytes_per_step": int(m.np * nst * S)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "pass_fp64 (fused stencil + vpsi + KB ket)",
+                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": pass_avg_ms},
+            "kernels": {"pass_fp64": {"launches": npass, "ms": pass_ms},
+                        "bra_fp64": {"launches": nbra, "ms": bra_ms}},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "extra": {
+                "fp32_storage_hpsi": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps},
+                "taylor4_fp64": {"steps_per_s": tk / (ms_t64 / 1e3), "ms_per_step": ms_t64 / tk},
+                "taylor4_fp32": {"steps_per_s": tk / (ms_t32 / 1e3), "ms_per_step": ms_t32 / tk},
+            },
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

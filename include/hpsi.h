@@ -1,0 +1,210 @@
+/*
+ * hpsi.h -- C ABI of the B200 Hamiltonian-apply and Taylor-propagation library.
+ *
+ * The library is a drop-in behind Octopus' X(hamiltonian_elec_apply_batch)
+ * and the Taylor branch of exponential_apply_batch.  The host keeps the mesh,
+ * the finite-difference weights, the projector matrices and the state batches;
+ * it hands them to the library as plain pointers and sizes.  Every entry point
+ * is `extern "C"`, callable from Fortran through iso_c_binding `bind(C)`
+ * interfaces (no hidden string arguments, no Fortran name mangling).
+ *
+ * Conventions
+ *  - Indices are 0-based.  Point arrays list the np inner points first and the
+ *    np_part - np boundary points after them, as mesh%idx does.
+ *  - A batch is "packed" in the reference's sense (src/grid/batch.F90:58-59,
+ *    zff_pack(ist, ip)): states fastest, `ld` complex numbers per point.
+ *  - Batch pointers may be device pointers (used in place, zero copy) or host
+ *    pointers (the library stages them through device memory; the call then
+ *    returns only when the result is back in host memory).
+ *  - Every call that takes a `stream` is ordered on that CUDA stream
+ *    (cudaStream_t passed as void*; NULL is the legacy default stream).
+ *  - Errors are returned as hpsi_status; the library never exits the process.
+ *    hpsi_last_error_string() gives a one-line message for the calling thread.
+ */
+#ifndef HPSI_H
+#define HPSI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t hpsi_status;
+#define HPSI_OK 0
+#define HPSI_ERR_ARG 1         /* bad argument (size, null pointer, layout) */
+#define HPSI_ERR_INDEX 2       /* an index map points outside its range */
+#define HPSI_ERR_NONFINITE 3   /* NaN or Inf found in an input or a result */
+#define HPSI_ERR_CUDA 4        /* a CUDA runtime call failed */
+#define HPSI_ERR_TIMEOUT 5     /* a bounded device wait gave up */
+#define HPSI_ERR_STATE 6       /* handle not ready (e.g. weights not set) */
+#define HPSI_ERR_NOMEM 7       /* device allocation failed */
+#define HPSI_ERR_RUNAWAY 8     /* norm growth beyond the runaway limit */
+#define HPSI_ERR_UNSUPPORTED 9 /* valid request this build does not handle */
+
+/* storage / arithmetic of a batch */
+#define HPSI_C128 0 /* complex128 storage, FP64 arithmetic */
+#define HPSI_C64 1  /* complex64 storage, FP32 arithmetic (FP64 reductions) */
+
+/* Hamiltonian terms: the TERM_* bits of
+ * src/hamiltonian/hamiltonian_elec_base.F90:149-158 that this path serves. */
+#define HPSI_TERM_KINETIC 1
+#define HPSI_TERM_LOCAL_POTENTIAL 2
+#define HPSI_TERM_NON_LOCAL_POTENTIAL 4
+#define HPSI_TERM_ALL 0x7fffffff
+
+typedef struct hpsi_mesh hpsi_mesh;
+typedef struct hpsi_hamiltonian hpsi_hamiltonian;
+
+/* ------------------------------------------------------------------ */
+/* Mesh: replaces the index arrays the reference builds in
+ * mesh_init_stage_2 (src/grid/mesh_init.F90:185-360) and the stencil run
+ * tables of nl_operator_build (src/grid/nl_operator.F90:308-456); the library
+ * derives its own cell maps from the point coordinates. */
+typedef struct {
+  int32_t np;             /* inner points */
+  int32_t np_part;        /* inner + boundary points */
+  const int32_t *lxyz;    /* 3*np_part integer coordinates, (x,y,z) per point */
+  double spacing[3];      /* mesh%spacing */
+  int32_t order;          /* stencil half-width (DerivativesOrder); 4 */
+  int32_t periodic;       /* 0: boundary points are zero-BC points,
+                             1: boundary point b is a periodic image of
+                                per_inner[b] (per_points, boundaries.F90) */
+  const int32_t *per_inner; /* np_part-np entries when periodic, else NULL */
+} hpsi_mesh_desc;
+
+/* Builds the device cell maps.  Fails with HPSI_ERR_INDEX if a stencil point
+ * of an inner point is not a mesh point (the reference asserts the same,
+ * nl_operator.F90:367). */
+hpsi_status hpsi_mesh_create(const hpsi_mesh_desc *desc, hpsi_mesh **out);
+hpsi_status hpsi_mesh_destroy(hpsi_mesh *mesh);
+/* dims[0..2]: padded cell box, dims[3..5]: inner bounding box */
+hpsi_status hpsi_mesh_info(const hpsi_mesh *mesh, int32_t dims[6]);
+
+/* ------------------------------------------------------------------ */
+/* Hamiltonian: the state of hamiltonian_elec_t that H.psi reads
+ * (src/hamiltonian/hamiltonian_elec.F90), bound to one mesh. */
+hpsi_status hpsi_hamiltonian_create(hpsi_mesh *mesh, hpsi_hamiltonian **out);
+hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *ham);
+
+/* Kinetic operator: the Laplacian weights op%w(:,1) of the order-4 star
+ * (W = 25 points in stencil_star_get_lapl order, src/grid/stencil_star.F90:59-93,
+ * solved by derivatives_make_discretization, src/grid/derivatives.F90:639-757)
+ * and the factor -1/(2m) that X(derivatives_batch_start) applies
+ * (src/hamiltonian/hamiltonian_elec_inc.F90:155).  `points` is 3*W offsets and
+ * must be the star of the mesh's order. */
+hpsi_status hpsi_hamiltonian_set_kinetic(hpsi_hamiltonian *ham, int32_t W,
+                                         const int32_t *points, const double *w,
+                                         double factor);
+
+/* Local potential v(np) for the spin channel of the batch
+ * (hm_base%potential, used by X(hamiltonian_elec_base_local_sub),
+ * src/hamiltonian/hamiltonian_elec_base_inc.F90:233-242).  Host pointer. */
+hpsi_status hpsi_hamiltonian_set_vloc(hpsi_hamiltonian *ham, const double *v);
+
+/* Length-gauge laser term folded into the local potential,
+ * v(r) += amplitude * pol . r (laser_potential, src/hamiltonian/lasers.F90:823-853). */
+hpsi_status hpsi_hamiltonian_set_field(hpsi_hamiltonian *ham, const double pol[3],
+                                       double amplitude);
+
+/* Bloch phase correction of the periodic boundary copy, one complex number
+ * per boundary point (hm_base%phase_corr(np+1:np_part, ik),
+ * src/hamiltonian/hamiltonian_elec.F90:634-647; applied in
+ * src/grid/boundaries_inc.F90:650-700).  2*(np_part-np) doubles, or NULL to
+ * remove it. */
+hpsi_status hpsi_hamiltonian_set_phase_corr(hpsi_hamiltonian *ham,
+                                            const double *phase_corr);
+
+/* Kleinman-Bylander projector matrices (projector_matrix_t,
+ * src/hamiltonian/projector_matrix.F90:37-90, built by
+ * hamiltonian_elec_base_build_proj, src/hamiltonian/hamiltonian_elec_base.F90:436-911).
+ * Matrix m has npoints[m] sphere points and nprojs[m] projectors; the arrays
+ * are the matrices concatenated in order:
+ *   map      sum(npoints)            mesh point of each sphere point (pmat%map)
+ *   matrices sum(npoints*nprojs)     point fastest within a matrix (dprojectors)
+ *   scal     sum(nprojs)             e_KB * vol_pp (pmat%scal, :628)
+ * nmat = 0 removes the projectors. */
+hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *ham, int32_t nmat,
+                                            const int32_t *npoints,
+                                            const int32_t *nprojs,
+                                            const int32_t *map,
+                                            const double *matrices,
+                                            const double *scal);
+
+/* ------------------------------------------------------------------ */
+/* A borrowed state batch (batch_t / wfs_elec_t in packed status). */
+typedef struct {
+  void *ptr;       /* device or host pointer to npts * ld complex numbers */
+  int64_t ld;      /* complex numbers per point (pack_size(1)) */
+  int32_t nst;     /* states in use, nst <= ld */
+  int32_t npts;    /* points held: np_part for an input, >= np for an output */
+  int32_t dtype;   /* HPSI_C128 or HPSI_C64 */
+} hpsi_batch;
+
+/* hpsi = H psi on the np inner points: replaces
+ * X(hamiltonian_elec_apply_batch)(hm, namespace, mesh, psib, hpsib, terms,
+ * set_bc) (src/hamiltonian/hamiltonian_elec_inc.F90:77-261) for the kinetic,
+ * local and KB terms.  set_bc != 0 applies the zero or periodic boundary
+ * condition to the values the stencil reads (the caller's boundary rows are
+ * not written); set_bc == 0 uses the boundary rows of psi as stored. */
+hpsi_status hpsi_apply_h(hpsi_hamiltonian *ham, const hpsi_batch *psi,
+                         hpsi_batch *hpsi, int32_t terms, int32_t set_bc,
+                         void *stream);
+
+/* Writes the boundary rows of psi as boundaries_set does
+ * (src/grid/boundaries_inc.F90:275-745): zeros, or periodic copies times the
+ * phase correction. */
+hpsi_status hpsi_boundaries_set(hpsi_hamiltonian *ham, hpsi_batch *psi,
+                                void *stream);
+
+/* psi <- sum_{k=0..order} (-i dt H)^k / k! psi on the np inner points:
+ * replaces the Taylor branch of exponential_apply_batch
+ * (src/electrons/exponential.F90:581-674, exponential_taylor_series_batch
+ * :677-757) without psib2 / inh_psib.  The polynomial is evaluated in Horner
+ * form, one fused stencil pass per order.  If `energy`, `dipole` or `norm2`
+ * is non-NULL, the per-state FP64 observables of the incoming psi are
+ * returned (host arrays of nst doubles):
+ *   energy[i] = dV * Re sum conj(psi_i) (H psi_i),
+ *   dipole[i] = dV * sum |psi_i|^2 (pol . r)   (pol from set_field, else z),
+ *   norm2[i]  = dV * sum |psi_i|^2. */
+hpsi_status hpsi_taylor_step(hpsi_hamiltonian *ham, hpsi_batch *psi, double dt_re,
+                             double dt_im, int32_t order, double *energy,
+                             double *dipole, double *norm2, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* FP64 reductions over the np inner points (dV = vol_pp), results in host
+ * arrays:
+ *   hpsi_nrm2        out[nst]      X(mesh_batch_nrm2), src/grid/mesh_batch_inc.F90:970-1167
+ *   hpsi_dotp_matrix out[2*nst*nst] (interleaved complex, row i = bra state,
+ *                    column j fastest) X(mesh_batch_dotp_matrix), :20-263
+ *   hpsi_orthonormalize_cholesky   S = U^H U, psi <- psi U^-1 in place,
+ *                    X(states_elec_orthogonalization_full) cholesky_serial,
+ *                    src/states/states_elec_calc_inc.F90:66-98 */
+hpsi_status hpsi_nrm2(hpsi_mesh *mesh, const hpsi_batch *psi, double *out,
+                      void *stream);
+hpsi_status hpsi_dotp_matrix(hpsi_mesh *mesh, const hpsi_batch *a,
+                             const hpsi_batch *b, double *out, void *stream);
+hpsi_status hpsi_orthonormalize_cholesky(hpsi_mesh *mesh, hpsi_batch *psi,
+                                         void *stream);
+
+/* ------------------------------------------------------------------ */
+/* Library-wide controls and diagnostics. */
+const char *hpsi_last_error_string(void);
+/* Number of this library's kernels launched since load (diagnostic). */
+int64_t hpsi_kernel_launch_count(void);
+/* Version string of this build. */
+const char *hpsi_version(void);
+/* Kernel timer (the analogue of the reference's profiling_in/out labels,
+ * src/basic/profiling.F90:503-625): when enabled, CUDA events are recorded on
+ * the launch stream around every kernel of the labels "pass_fp64",
+ * "pass_fp32", "bra_fp64" and "bra_fp32".  Enabling clears the records;
+ * hpsi_profile_query synchronises on them and returns the launch count and
+ * the summed device time of one label. */
+hpsi_status hpsi_profile_enable(int32_t on);
+hpsi_status hpsi_profile_query(const char *label, int64_t *launches, double *total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPSI_H */

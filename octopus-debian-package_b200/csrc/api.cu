@@ -1,0 +1,1039 @@
+// C ABI of the hpsi library: handles, validation, workspace and dispatch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "api_internal.cuh"
+#include "projector.cuh"
+#include "reduce.cuh"
+#include "stencil.cuh"
+
+namespace hpsi {
+
+std::atomic<int64_t> g_launches{0};
+static thread_local std::string t_last_error;
+void set_error(const std::string &msg) { t_last_error = msg; }
+
+// ---------------------------------------------------------------------------
+// kernel timer: CUDA events around each launch on its own stream (the
+// counterpart of the reference's profiling_in/out labels)
+namespace {
+struct ProfRec {
+  const char *label;
+  cudaEvent_t a, b;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof;
+std::vector<cudaEvent_t> g_prof_pool;
+size_t g_prof_used = 0;
+cudaEvent_t prof_event() {
+  if (g_prof_used == g_prof_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    g_prof_pool.push_back(e);
+  }
+  return g_prof_pool[g_prof_used++];
+}
+}  // namespace
+
+ProfScope::ProfScope(const char *label, cudaStream_t st) : st_(st) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on || g_prof.size() >= (1u << 20)) return;
+  ProfRec r{label, prof_event(), prof_event()};
+  cudaEventRecord(r.a, st);
+  g_prof.push_back(r);
+  idx_ = long(g_prof.size()) - 1;
+}
+ProfScope::~ProfScope() {
+  if (idx_ < 0) return;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  cudaEventRecord(g_prof[idx_].b, st_);
+}
+
+// ---------------------------------------------------------------------------
+// small device helpers
+namespace {
+
+__global__ void scatter_cells_kernel(const double *v, const int *cell_of_row, int n, double *vcell) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) vcell[cell_of_row[i]] = v[i];
+}
+
+template <typename T>
+__global__ void boundaries_kernel(T *psi, long long ld, int np, int nb, const int *per_inner, const T *phase,
+                                  int periodic) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)nb * ld;
+  if (i >= n) return;
+  const int b = int(i / ld), s = int(i % ld);
+  T *dst = psi + (long long)(np + b) * 2 * ld + 2 * s;
+  if (!periodic) {
+    dst[0] = T(0);
+    dst[1] = T(0);
+    return;
+  }
+  const T *src = psi + (long long)per_inner[b] * 2 * ld + 2 * s;
+  if (phase) {
+    const T pr = phase[2 * b], pi = phase[2 * b + 1];
+    const T xr = src[0], xi = src[1];
+    dst[0] = xr * pr - xi * pi;
+    dst[1] = xr * pi + xi * pr;
+  } else {
+    dst[0] = src[0];
+    dst[1] = src[1];
+  }
+}
+
+template <typename T>
+__global__ void copy_rows_kernel(const T *src, long long lds, T *dst, long long ldd, int nrows, int nst) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)nrows * nst;
+  if (i >= n) return;
+  const long long r = i / nst;
+  const int s = int(i % nst);
+  dst[r * 2 * ldd + 2 * s] = src[r * 2 * lds + 2 * s];
+  dst[r * 2 * ldd + 2 * s + 1] = src[r * 2 * lds + 2 * s + 1];
+}
+
+}  // namespace
+
+hpsi_status dev_alloc(void **p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    return HPSI_ERR_NOMEM;
+  }
+  return HPSI_OK;
+}
+
+void dev_free(void *p) {
+  if (p) cudaFree(p);
+}
+
+hpsi_status Workspace::ensure(size_t bytes) {
+  if (bytes <= size) return HPSI_OK;
+  dev_free(ptr);
+  ptr = nullptr;
+  size = 0;
+  hpsi_status s = dev_alloc(&ptr, bytes);
+  if (s == HPSI_OK) size = bytes;
+  return s;
+}
+
+void Workspace::release() {
+  dev_free(ptr);
+  ptr = nullptr;
+  size = 0;
+}
+
+// true if the pointer can be dereferenced by kernels on the current device
+bool is_device_ptr(const void *p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+hpsi_status check_batch(const hpsi_mesh *m, const hpsi_batch *b, int min_rows, const char *what) {
+  if (!b || !b->ptr) {
+    set_error(std::string(what) + ": null batch");
+    return HPSI_ERR_ARG;
+  }
+  if (b->dtype != HPSI_C128 && b->dtype != HPSI_C64) {
+    set_error(std::string(what) + ": unknown dtype");
+    return HPSI_ERR_ARG;
+  }
+  if (b->nst < 1 || b->ld < b->nst) {
+    set_error(std::string(what) + ": need 1 <= nst <= ld");
+    return HPSI_ERR_ARG;
+  }
+  if (b->npts < min_rows) {
+    set_error(std::string(what) + ": batch holds " + std::to_string(b->npts) + " points, need " +
+              std::to_string(min_rows));
+    return HPSI_ERR_ARG;
+  }
+  const size_t esz = b->dtype == HPSI_C128 ? 16 : 8;
+  if ((reinterpret_cast<uintptr_t>(b->ptr) % 16) != 0 || (size_t(b->ld) * esz) % 16 != 0) {
+    // the stencil gathers 16-byte pieces of each row
+    if (!(b->dtype == HPSI_C64 && b->ld % 2 == 1 && b->ld == 1)) {
+      set_error(std::string(what) + ": rows must start on 16-byte boundaries (ld * element size % 16 == 0)");
+      return HPSI_ERR_ARG;
+    }
+  }
+  (void)m;
+  return HPSI_OK;
+}
+
+// state chunk width of the fused pass for a batch
+int pass_sc(int dtype, long long ld) {
+  const int maxsc = dtype == HPSI_C128 ? 4 : 8;
+  for (int sc = maxsc; sc >= 1; sc >>= 1)
+    if (ld % sc == 0) return sc;
+  return 1;
+}
+
+PassShape default_shape(int dtype, long long ld) {
+  const int sc = pass_sc(dtype, ld);
+  // FP64 keeps 4 rows of 9 running sums per thread (36 doubles), FP32 8 rows
+  return dtype == HPSI_C128 ? PassShape{sc, 16, 16, 4} : PassShape{sc, 16, 16, sc >= 4 ? 8 : 4};
+}
+
+}  // namespace hpsi
+
+using namespace hpsi;
+
+// ===========================================================================
+extern "C" {
+
+const char *hpsi_last_error_string(void) { return t_last_error.c_str(); }
+int64_t hpsi_kernel_launch_count(void) { return g_launches.load(); }
+const char *hpsi_version(void) { return "hpsi 0.1 (sm_100a)"; }
+
+hpsi_status hpsi_profile_enable(int32_t on) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof.clear();
+  g_prof_used = 0;
+  g_prof_on = on != 0;
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_profile_query(const char *label, int64_t *launches, double *total_ms) {
+  if (!label || !launches || !total_ms) return HPSI_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  *launches = 0;
+  *total_ms = 0.0;
+  for (auto &r : g_prof) {
+    if (std::strcmp(r.label, label) != 0) continue;
+    cudaError_t e = cudaEventSynchronize(r.b);
+    if (e != cudaSuccess) {
+      set_error(std::string("hpsi_profile_query: ") + cudaGetErrorString(e));
+      return HPSI_ERR_CUDA;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    *launches += 1;
+    *total_ms += ms;
+  }
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_mesh_create(const hpsi_mesh_desc *d, hpsi_mesh **out) {
+  if (!d || !out || !d->lxyz || d->np < 1 || d->np_part < d->np) {
+    set_error("hpsi_mesh_create: bad descriptor");
+    return HPSI_ERR_ARG;
+  }
+  if (d->order < 1 || d->order > 4) {
+    set_error("hpsi_mesh_create: stencil order must be 1..4");
+    return HPSI_ERR_UNSUPPORTED;
+  }
+  if (d->periodic && !d->per_inner && d->np_part > d->np) {
+    set_error("hpsi_mesh_create: periodic mesh without per_inner");
+    return HPSI_ERR_ARG;
+  }
+  const int np = d->np, npp = d->np_part, HAL = 4;
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = d->lxyz[a];
+    hi[a] = d->lxyz[a];
+  }
+  for (int i = 0; i < np; ++i)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], d->lxyz[3 * i + a]);
+      hi[a] = std::max(hi[a], d->lxyz[3 * i + a]);
+    }
+  CellBox B;
+  B.halo = HAL;
+  B.nxo = hi[0] - lo[0] + 1;
+  B.nyo = hi[1] - lo[1] + 1;
+  B.nzo = hi[2] - lo[2] + 1;
+  B.NX = (B.nxo + 31) / 32 * 32 + 2 * HAL;
+  B.NY = (B.nyo + 31) / 32 * 32 + 2 * HAL;
+  B.NZ = B.nzo + 2 * HAL;
+  for (int a = 0; a < 3; ++a) {
+    B.lo[a] = lo[a] - HAL;
+    B.h[a] = d->spacing[a];
+  }
+  const long long ncell = (long long)B.NX * B.NY * B.NZ;
+  if (ncell > (1LL << 31) - 1 || (long long)npp * 4096 > (1LL << 62)) {
+    set_error("hpsi_mesh_create: mesh too large");
+    return HPSI_ERR_UNSUPPORTED;
+  }
+  std::vector<int> cell_row(ncell, -1), cell_of_row(npp);
+  for (int i = 0; i < npp; ++i) {
+    const int x = d->lxyz[3 * i] - B.lo[0], y = d->lxyz[3 * i + 1] - B.lo[1], z = d->lxyz[3 * i + 2] - B.lo[2];
+    if (x < 0 || y < 0 || z < 0 || x >= B.NX || y >= B.NY || z >= B.NZ) {
+      set_error("hpsi_mesh_create: boundary point " + std::to_string(i) +
+                " is farther than 4 cells from the inner points");
+      return HPSI_ERR_INDEX;
+    }
+    const long long c = ((long long)z * B.NY + y) * B.NX + x;
+    if (cell_row[c] != -1) {
+      set_error("hpsi_mesh_create: duplicate point " + std::to_string(i));
+      return HPSI_ERR_INDEX;
+    }
+    cell_row[c] = i;
+    cell_of_row[i] = int(c);
+  }
+  // every star neighbour (half-width = order) of an inner point must exist
+  const int ord = d->order;
+  for (int i = 0; i < np; ++i) {
+    const long long c = cell_of_row[i];
+    const long long strides[3] = {1, B.NX, (long long)B.NX * B.NY};
+    for (int a = 0; a < 3; ++a)
+      for (int s = -ord; s <= ord; ++s) {
+        if (!s) continue;
+        if (cell_row[c + s * strides[a]] < 0) {
+          set_error("hpsi_mesh_create: stencil of inner point " + std::to_string(i) + " leaves the mesh");
+          return HPSI_ERR_INDEX;
+        }
+      }
+  }
+  std::vector<int> src_zero(ncell), src_per;
+  for (long long c = 0; c < ncell; ++c) src_zero[c] = (cell_row[c] >= 0 && cell_row[c] < np) ? cell_row[c] : -1;
+  std::vector<int> per;
+  if (d->periodic) {
+    per.assign(d->per_inner, d->per_inner + (npp - np));
+    for (int b = 0; b < npp - np; ++b)
+      if (per[b] < 0 || per[b] >= np) {
+        set_error("hpsi_mesh_create: per_inner[" + std::to_string(b) + "] is not an inner point");
+        return HPSI_ERR_INDEX;
+      }
+    src_per = src_zero;
+    for (int b = 0; b < npp - np; ++b) src_per[cell_of_row[np + b]] = per[b];
+  }
+  hpsi_mesh *m = new hpsi_mesh();
+  m->np = np;
+  m->np_part = npp;
+  m->order = ord;
+  m->periodic = d->periodic ? 1 : 0;
+  m->box = B;
+  m->per_inner_h = per;
+  m->cell_of_row_h = cell_of_row;
+  cudaGetDevice(&m->device);
+  cudaDeviceGetAttribute(&m->num_sms, cudaDevAttrMultiProcessorCount, m->device);
+  hpsi_status s = HPSI_OK;
+  auto up = [&](int **dp, const std::vector<int> &h) {
+    if (s != HPSI_OK) return;
+    s = dev_alloc(reinterpret_cast<void **>(dp), h.size() * sizeof(int));
+    if (s == HPSI_OK && !h.empty()) {
+      cudaError_t e = cudaMemcpy(*dp, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        set_error(std::string("hpsi_mesh_create: ") + cudaGetErrorString(e));
+        s = HPSI_ERR_CUDA;
+      }
+    }
+  };
+  up(&m->d_cell_row, cell_row);
+  up(&m->d_src_raw, cell_row);
+  up(&m->d_src_zero, src_zero);
+  up(&m->d_cell_of_row, cell_of_row);
+  if (m->periodic) {
+    up(&m->d_src_per, src_per);
+    up(&m->d_per_inner, per);
+  }
+  if (s != HPSI_OK) {
+    hpsi_mesh_destroy(m);
+    return s;
+  }
+  *out = m;
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_mesh_destroy(hpsi_mesh *m) {
+  if (!m) return HPSI_OK;
+  dev_free(m->d_cell_row);
+  dev_free(m->d_src_raw);
+  dev_free(m->d_src_zero);
+  dev_free(m->d_src_per);
+  dev_free(m->d_per_inner);
+  dev_free(m->d_cell_of_row);
+  m->scratch.release();
+  m->scratch2.release();
+  m->stage_in.release();
+  m->stage_out.release();
+  delete m;
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_mesh_info(const hpsi_mesh *m, int32_t dims[6]) {
+  if (!m || !dims) return HPSI_ERR_ARG;
+  dims[0] = m->box.NX;
+  dims[1] = m->box.NY;
+  dims[2] = m->box.NZ;
+  dims[3] = m->box.nxo;
+  dims[4] = m->box.nyo;
+  dims[5] = m->box.nzo;
+  return HPSI_OK;
+}
+
+// ---------------------------------------------------------------------------
+hpsi_status hpsi_hamiltonian_create(hpsi_mesh *mesh, hpsi_hamiltonian **out) {
+  if (!mesh || !out) return HPSI_ERR_ARG;
+  hpsi_hamiltonian *h = new hpsi_hamiltonian();
+  h->mesh = mesh;
+  *out = h;
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
+  if (!h) return HPSI_OK;
+  dev_free(h->d_vcell);
+  dev_free(h->d_phase);
+  dev_free(h->d_phase_f);
+  dev_free(h->d_src_phase);
+  h->proj_free();
+  for (auto &w : h->u) w.release();
+  h->projbuf.release();
+  h->obsbuf.release();
+  h->small.release();
+  delete h;
+  return HPSI_OK;
+}
+
+void hpsi_hamiltonian::proj_free() {
+  dev_free(d_mat);
+  dev_free(d_proj_row);
+  dev_free(d_map);
+  dev_free(d_pt);
+  dev_free(d_pt_f);
+  dev_free(d_scal);
+  dev_free(d_scal_f);
+  dev_free(d_kb_ptr);
+  dev_free(d_kb_ent);
+  d_mat = nullptr;
+  d_proj_row = d_map = d_kb_ptr = nullptr;
+  d_pt = d_scal = nullptr;
+  d_pt_f = d_scal_f = nullptr;
+  d_kb_ent = nullptr;
+  nmat = 0;
+  nprojections = 0;
+  max_nproj = 0;
+}
+
+hpsi_status hpsi_hamiltonian_set_kinetic(hpsi_hamiltonian *h, int32_t W, const int32_t *points, const double *w,
+                                         double factor) {
+  if (!h || !points || !w || W < 1) return HPSI_ERR_ARG;
+  for (int k = 0; k < 9; ++k) h->wx[k] = h->wy[k] = h->wz[k] = 0.0;
+  int ncenter = 0;
+  for (int j = 0; j < W; ++j) {
+    const int dx = points[3 * j], dy = points[3 * j + 1], dz = points[3 * j + 2];
+    const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+    if (nz > 1 || std::abs(dx) > 4 || std::abs(dy) > 4 || std::abs(dz) > 4 ||
+        std::max({std::abs(dx), std::abs(dy), std::abs(dz)}) > h->mesh->order) {
+      set_error("hpsi_hamiltonian_set_kinetic: only star stencils within the mesh order are supported");
+      return HPSI_ERR_UNSUPPORTED;
+    }
+    const double wf = w[j] * factor;  // the reference multiplies op%w by the factor (nl_operator_inc.F90:72-80)
+    if (nz == 0) {
+      h->wx[4] += wf;
+      ++ncenter;
+    } else if (dx)
+      h->wx[dx + 4] += wf;
+    else if (dy)
+      h->wy[dy + 4] += wf;
+    else
+      h->wz[dz + 4] += wf;
+  }
+  if (ncenter != 1) {
+    set_error("hpsi_hamiltonian_set_kinetic: the stencil must contain the centre exactly once");
+    return HPSI_ERR_ARG;
+  }
+  h->have_kinetic = true;
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_hamiltonian_set_vloc(hpsi_hamiltonian *h, const double *v) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_mesh *m = h->mesh;
+  const long long ncell = (long long)m->box.NX * m->box.NY * m->box.NZ;
+  if (!v) {
+    dev_free(h->d_vcell);
+    h->d_vcell = nullptr;
+    return HPSI_OK;
+  }
+  for (int i = 0; i < m->np; ++i)
+    if (!std::isfinite(v[i])) {
+      set_error("hpsi_hamiltonian_set_vloc: non-finite potential at point " + std::to_string(i));
+      return HPSI_ERR_NONFINITE;
+    }
+  if (!h->d_vcell) {
+    hpsi_status s = dev_alloc(reinterpret_cast<void **>(&h->d_vcell), ncell * sizeof(double));
+    if (s) return s;
+  }
+  HPSI_TRY_CUDA(cudaMemset(h->d_vcell, 0, ncell * sizeof(double)));
+  double *dv = nullptr;
+  hpsi_status s = dev_alloc(reinterpret_cast<void **>(&dv), size_t(m->np) * sizeof(double));
+  if (s) return s;
+  cudaMemcpy(dv, v, size_t(m->np) * sizeof(double), cudaMemcpyHostToDevice);
+  scatter_cells_kernel<<<(m->np + 255) / 256, 256>>>(dv, m->d_cell_of_row, m->np, h->d_vcell);
+  g_launches++;
+  cudaError_t e = cudaDeviceSynchronize();
+  dev_free(dv);
+  if (e != cudaSuccess) {
+    set_error(std::string("hpsi_hamiltonian_set_vloc: ") + cudaGetErrorString(e));
+    return HPSI_ERR_CUDA;
+  }
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_hamiltonian_set_field(hpsi_hamiltonian *h, const double pol[3], double amplitude) {
+  if (!h || !pol) return HPSI_ERR_ARG;
+  for (int a = 0; a < 3; ++a) {
+    h->pol[a] = pol[a];
+    h->fld[a] = pol[a] * amplitude;
+  }
+  h->have_pol = true;
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_hamiltonian_set_phase_corr(hpsi_hamiltonian *h, const double *pc) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_mesh *m = h->mesh;
+  dev_free(h->d_phase);
+  dev_free(h->d_phase_f);
+  dev_free(h->d_src_phase);
+  h->d_phase = nullptr;
+  h->d_phase_f = nullptr;
+  h->d_src_phase = nullptr;
+  if (!pc) return HPSI_OK;
+  if (!m->periodic) {
+    set_error("hpsi_hamiltonian_set_phase_corr: mesh is not periodic");
+    return HPSI_ERR_STATE;
+  }
+  const int nb = m->np_part - m->np;
+  std::vector<float> pf(2 * size_t(nb));
+  for (size_t i = 0; i < pf.size(); ++i) pf[i] = float(pc[i]);
+  // encoded load map: boundary cell -> -(b + 2)
+  const long long ncell = (long long)m->box.NX * m->box.NY * m->box.NZ;
+  std::vector<int> enc(ncell);
+  HPSI_TRY_CUDA(cudaMemcpy(enc.data(), m->d_src_zero, ncell * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int b = 0; b < nb; ++b) enc[m->cell_of_row_h[m->np + b]] = -(b + 2);
+  hpsi_status s = dev_alloc(reinterpret_cast<void **>(&h->d_phase), 2 * size_t(nb) * sizeof(double));
+  if (!s) s = dev_alloc(reinterpret_cast<void **>(&h->d_phase_f), 2 * size_t(nb) * sizeof(float));
+  if (!s) s = dev_alloc(reinterpret_cast<void **>(&h->d_src_phase), ncell * sizeof(int));
+  if (s) return s;
+  HPSI_TRY_CUDA(cudaMemcpy(h->d_phase, pc, 2 * size_t(nb) * sizeof(double), cudaMemcpyHostToDevice));
+  HPSI_TRY_CUDA(cudaMemcpy(h->d_phase_f, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  HPSI_TRY_CUDA(cudaMemcpy(h->d_src_phase, enc.data(), ncell * sizeof(int), cudaMemcpyHostToDevice));
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, const int32_t *npoints,
+                                            const int32_t *nprojs, const int32_t *map, const double *matrices,
+                                            const double *scal) {
+  if (!h || nmat < 0) return HPSI_ERR_ARG;
+  h->proj_free();
+  if (nmat == 0) return HPSI_OK;
+  if (!npoints || !nprojs || !map || !matrices || !scal) return HPSI_ERR_ARG;
+  hpsi_mesh *m = h->mesh;
+  std::vector<int4> mat(nmat);
+  std::vector<int> prow(nmat);
+  long long npts_tot = 0, nval = 0;
+  int nproj_tot = 0, maxp = 0;
+  for (int i = 0; i < nmat; ++i) {
+    if (npoints[i] < 0 || nprojs[i] < 1) {
+      set_error("hpsi_hamiltonian_set_projectors: bad matrix size");
+      return HPSI_ERR_ARG;
+    }
+    mat[i] = make_int4(npoints[i], nprojs[i], int(npts_tot), int(nval));
+    prow[i] = nproj_tot;
+    npts_tot += npoints[i];
+    nval += (long long)npoints[i] * nprojs[i];
+    nproj_tot += nprojs[i];
+    maxp = std::max(maxp, int(nprojs[i]));
+  }
+  if (nval > (1LL << 31) - 1) return HPSI_ERR_UNSUPPORTED;
+  std::vector<double> pt(nval);
+  std::vector<float> ptf(nval), scf(nproj_tot);
+  std::vector<int> cnt(m->np + 1, 0);
+  for (int i = 0; i < nmat; ++i) {
+    const int n = npoints[i], q = nprojs[i];
+    const double *src = matrices + mat[i].w;
+    for (int k = 0; k < n; ++k) {
+      const int row = map[mat[i].z + k];
+      if (row < 0 || row >= m->np) {
+        set_error("hpsi_hamiltonian_set_projectors: map entry " + std::to_string(mat[i].z + k) +
+                  " is not an inner point");
+        return HPSI_ERR_INDEX;
+      }
+      cnt[row + 1]++;
+      for (int j = 0; j < q; ++j) {
+        pt[mat[i].w + (long long)k * q + j] = src[(long long)j * n + k];
+        ptf[mat[i].w + (long long)k * q + j] = float(src[(long long)j * n + k]);
+      }
+    }
+  }
+  for (int i = 0; i < nproj_tot; ++i) scf[i] = float(scal[i]);
+  for (int r = 0; r < m->np; ++r) cnt[r + 1] += cnt[r];
+  std::vector<int4> ent(npts_tot);
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+  for (int i = 0; i < nmat; ++i)
+    for (int k = 0; k < npoints[i]; ++k) {
+      const int row = map[mat[i].z + k];
+      ent[fill[row]++] = make_int4(mat[i].w + k * nprojs[i], prow[i], nprojs[i], 0);
+    }
+  hpsi_status s = HPSI_OK;
+  auto up = [&](void **dp, const void *src, size_t bytes) {
+    if (s) return;
+    s = dev_alloc(dp, bytes);
+    if (!s && bytes) {
+      cudaError_t e = cudaMemcpy(*dp, src, bytes, cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        set_error(cudaGetErrorString(e));
+        s = HPSI_ERR_CUDA;
+      }
+    }
+  };
+  up(reinterpret_cast<void **>(&h->d_mat), mat.data(), mat.size() * sizeof(int4));
+  up(reinterpret_cast<void **>(&h->d_proj_row), prow.data(), prow.size() * sizeof(int));
+  up(reinterpret_cast<void **>(&h->d_map), map, size_t(npts_tot) * sizeof(int));
+  up(reinterpret_cast<void **>(&h->d_pt), pt.data(), pt.size() * sizeof(double));
+  up(reinterpret_cast<void **>(&h->d_pt_f), ptf.data(), ptf.size() * sizeof(float));
+  up(reinterpret_cast<void **>(&h->d_scal), scal, size_t(nproj_tot) * sizeof(double));
+  up(reinterpret_cast<void **>(&h->d_scal_f), scf.data(), scf.size() * sizeof(float));
+  up(reinterpret_cast<void **>(&h->d_kb_ptr), cnt.data(), cnt.size() * sizeof(int));
+  up(reinterpret_cast<void **>(&h->d_kb_ent), ent.data(), ent.size() * sizeof(int4));
+  if (s) {
+    h->proj_free();
+    return s;
+  }
+  h->nmat = nmat;
+  h->nprojections = nproj_tot;
+  h->max_nproj = maxp;
+  return HPSI_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+namespace hpsi {
+
+// Build the pass arguments shared by apply and Taylor passes.
+void base_pass_args(const hpsi_hamiltonian *h, int terms, const int *src_map, PassArgs &a) {
+  const hpsi_mesh *m = h->mesh;
+  std::memset(&a, 0, sizeof(a));
+  a.box = m->box;
+  a.cell_src = src_map;
+  a.cell_row = m->d_cell_row;
+  a.per_inner = m->d_per_inner;
+  a.np = m->np;
+  if ((terms & HPSI_TERM_KINETIC) && h->have_kinetic) {
+    std::memcpy(a.wx, h->wx, sizeof(a.wx));
+    std::memcpy(a.wy, h->wy, sizeof(a.wy));
+    std::memcpy(a.wz, h->wz, sizeof(a.wz));
+  }
+  if (terms & HPSI_TERM_LOCAL_POTENTIAL) {
+    a.v_cell = h->d_vcell;
+    for (int k = 0; k < 3; ++k) a.fld[k] = h->fld[k];
+  }
+  a.obs_pol[0] = 0.0;
+  a.obs_pol[1] = 0.0;
+  a.obs_pol[2] = 1.0;
+  if (h->have_pol)
+    for (int k = 0; k < 3; ++k) a.obs_pol[k] = h->pol[k];
+}
+
+template <typename T>
+hpsi_status run_bra(hpsi_hamiltonian *h, const T *psi, long long ld, T *proj, cudaStream_t st) {
+  ProjArgs p;
+  p.nmat = h->nmat;
+  p.max_nproj = h->max_nproj;
+  p.mat = h->d_mat;
+  p.proj_row = h->d_proj_row;
+  p.map = h->d_map;
+  p.pt = sizeof(T) == 8 ? static_cast<const void *>(h->d_pt) : static_cast<const void *>(h->d_pt_f);
+  p.scal = sizeof(T) == 8 ? static_cast<const void *>(h->d_scal) : static_cast<const void *>(h->d_scal_f);
+  p.psi = psi;
+  p.psi_ld = ld;
+  p.proj = proj;
+  p.proj_ld = ld;
+  ProfScope prof(sizeof(T) == 8 ? "bra_fp64" : "bra_fp32", st);
+  return launch_bra<T>(p, h->use_tensor_bra, st);
+}
+
+// One fused pass.  in: rows to stencil; out: result rows; psi0 for Horner.
+template <typename T>
+hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T *in, long long in_ld, T *out,
+                     long long out_ld, long long ld, int mode, const T *psi0, long long psi0_ld, double a_re,
+                     double a_im, double *obs_partial, int *ncta_out, cudaStream_t st) {
+  PassArgs a;
+  base_pass_args(h, terms, src_map, a);
+  if (h->mesh->periodic && h->d_src_phase && src_map == h->d_src_phase)
+    a.phase_corr = sizeof(T) == 8 ? static_cast<const void *>(h->d_phase) : static_cast<const void *>(h->d_phase_f);
+  a.in = in;
+  a.in_ld = in_ld;
+  a.out = out;
+  a.out_ld = out_ld;
+  a.mode = mode;
+  a.psi0 = psi0;
+  a.psi0_ld = psi0_ld;
+  a.a_re = a_re;
+  a.a_im = a_im;
+  const bool nl = (terms & HPSI_TERM_NON_LOCAL_POTENTIAL) && h->nmat > 0;
+  if (nl) {
+    const size_t pbytes = size_t(h->nprojections) * ld * 2 * sizeof(T);
+    hpsi_status s = h->projbuf.ensure(pbytes);
+    if (s) return s;
+    s = run_bra<T>(h, in, in_ld, static_cast<T *>(h->projbuf.ptr), st);
+    if (s) return s;
+    a.kb_ptr = h->d_kb_ptr;
+    a.kb_ent = h->d_kb_ent;
+    a.kb_pt = sizeof(T) == 8 ? static_cast<const void *>(h->d_pt) : static_cast<const void *>(h->d_pt_f);
+    a.proj = h->projbuf.ptr;
+    a.proj_ld = in_ld;
+  }
+  const PassShape shape = default_shape(sizeof(T) == 8 ? HPSI_C128 : HPSI_C64, ld);
+  pass_geometry(a, shape, int(ld), h->mesh->num_sms);
+  if (obs_partial) {
+    a.obs = obs_partial;
+    a.obs_ld = int(ld);
+  }
+  if (ncta_out) *ncta_out = pass_ncta_xyz(a);
+  ProfScope prof(sizeof(T) == 8 ? "pass_fp64" : "pass_fp32", st);
+  return launch_pass<T>(a, shape, st);
+}
+
+const int *load_map(const hpsi_hamiltonian *h, int set_bc) {
+  const hpsi_mesh *m = h->mesh;
+  if (!set_bc) return m->d_src_raw;
+  if (m->periodic) return h->d_src_phase ? h->d_src_phase : m->d_src_per;
+  return m->d_src_zero;
+}
+
+// size of the observables partial buffer for a pass over ld states
+size_t obs_partial_bytes(const hpsi_hamiltonian *h, long long ld) {
+  PassArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.box = h->mesh->box;
+  const PassShape shape = default_shape(HPSI_C128, ld);
+  pass_geometry(a, shape, int(ld), h->mesh->num_sms);
+  const PassShape shape32 = default_shape(HPSI_C64, ld);
+  PassArgs b = a;
+  pass_geometry(b, shape32, int(ld), h->mesh->num_sms);
+  const long long n = std::max(pass_ncta_xyz(a), pass_ncta_xyz(b));
+  return size_t(n) * ld * 6 * sizeof(double);
+}
+
+template <typename T>
+hpsi_status apply_h_dev(hpsi_hamiltonian *h, const T *psi, long long ld, T *hpsi, long long ldo, int terms,
+                        int set_bc, cudaStream_t st) {
+  return run_pass<T>(h, terms, load_map(h, set_bc), psi, ld, hpsi, ldo, ld, PASS_APPLY, nullptr, 0, 0.0, 0.0,
+                     nullptr, nullptr, st);
+}
+
+// Horner form of the order-K Taylor polynomial, K fused passes.
+template <typename T>
+hpsi_status taylor_dev(hpsi_hamiltonian *h, T *psi, long long ld, int nst, double dt_re, double dt_im, int order,
+                       double *obs_dev, cudaStream_t st) {
+  hpsi_mesh *m = h->mesh;
+  const size_t ubytes = size_t(m->np) * ld * 2 * sizeof(T);
+  for (auto &w : h->u) {
+    hpsi_status s = w.ensure(ubytes);
+    if (s) return s;
+  }
+  double *obs_partial = nullptr;
+  if (obs_dev) {
+    hpsi_status s = h->obsbuf.ensure(obs_partial_bytes(h, ld));
+    if (s) return s;
+    obs_partial = static_cast<double *>(h->obsbuf.ptr);
+  }
+  const int *map = load_map(h, 1);
+  T *u0 = static_cast<T *>(h->u[0].ptr), *u1 = static_cast<T *>(h->u[1].ptr);
+  const T *in = psi;
+  long long in_ld = ld;
+  int ncta = 0;
+  for (int k = order; k >= 1; --k) {
+    // a_k = -i dt / k
+    const double are = dt_im / k, aim = -dt_re / k;
+    T *out = (k == 1 && order > 1) ? psi : ((order - k) % 2 == 0 ? u0 : u1);
+    const long long out_ld = (out == psi) ? ld : ld;
+    hpsi_status s = run_pass<T>(h, HPSI_TERM_ALL, map, in, in_ld, out, out_ld, ld, PASS_HORNER, psi, ld, are, aim,
+                                k == order ? obs_partial : nullptr, k == order ? &ncta : nullptr, st);
+    if (s) return s;
+    in = out;
+    in_ld = out_ld;
+  }
+  if (order == 1) {
+    const long long n = (long long)m->np * nst;
+    copy_rows_kernel<T><<<unsigned((n + 255) / 256), 256, 0, st>>>(u0, ld, psi, ld, m->np, nst);
+    HPSI_CHECK_LAUNCH();
+  }
+  if (obs_dev) {
+    hpsi_status s = launch_obs_finalize(obs_partial, ncta, int(ld), nst, m->box.h[0] * m->box.h[1] * m->box.h[2],
+                                        obs_dev, st);
+    if (s) return s;
+  }
+  return HPSI_OK;
+}
+
+template hpsi_status apply_h_dev<double>(hpsi_hamiltonian *, const double *, long long, double *, long long, int, int,
+                                         cudaStream_t);
+template hpsi_status apply_h_dev<float>(hpsi_hamiltonian *, const float *, long long, float *, long long, int, int,
+                                        cudaStream_t);
+template hpsi_status taylor_dev<double>(hpsi_hamiltonian *, double *, long long, int, double, double, int, double *,
+                                        cudaStream_t);
+template hpsi_status taylor_dev<float>(hpsi_hamiltonian *, float *, long long, int, double, double, int, double *,
+                                       cudaStream_t);
+
+// Host-pointer staging: copy a host batch into a device workspace.
+hpsi_status stage_batch(Workspace &ws, const hpsi_batch *b, int rows, bool copy_in, cudaStream_t st, void **dev) {
+  const size_t esz = b->dtype == HPSI_C128 ? 16 : 8;
+  const size_t bytes = size_t(rows) * b->ld * esz;
+  hpsi_status s = ws.ensure(bytes);
+  if (s) return s;
+  if (copy_in) HPSI_TRY_CUDA(cudaMemcpyAsync(ws.ptr, b->ptr, bytes, cudaMemcpyHostToDevice, st));
+  *dev = ws.ptr;
+  return HPSI_OK;
+}
+
+}  // namespace hpsi
+
+extern "C" {
+
+hpsi_status hpsi_apply_h(hpsi_hamiltonian *h, const hpsi_batch *psi, hpsi_batch *hpsi, int32_t terms,
+                         int32_t set_bc, void *stream) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_mesh *m = h->mesh;
+  hpsi_status s = check_batch(m, psi, m->np_part, "hpsi_apply_h(psi)");
+  if (!s) s = check_batch(m, hpsi, m->np, "hpsi_apply_h(hpsi)");
+  if (s) return s;
+  if (psi->dtype != hpsi->dtype || psi->nst != hpsi->nst) {
+    set_error("hpsi_apply_h: psi and hpsi differ in dtype or nst");
+    return HPSI_ERR_ARG;
+  }
+  if ((terms & HPSI_TERM_KINETIC) && !h->have_kinetic) {
+    set_error("hpsi_apply_h: kinetic weights not set");
+    return HPSI_ERR_STATE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool din = is_device_ptr(psi->ptr), dout = is_device_ptr(hpsi->ptr);
+  const void *pin = psi->ptr;
+  void *pout = hpsi->ptr;
+  long long ldi = psi->ld, ldo = hpsi->ld;
+  if (!din) {
+    void *d;
+    s = stage_batch(m->stage_in, psi, m->np_part, true, st, &d);
+    if (s) return s;
+    pin = d;
+  }
+  if (!dout) {
+    void *d;
+    s = stage_batch(m->stage_out, hpsi, m->np, false, st, &d);
+    if (s) return s;
+    pout = d;
+  }
+  if (psi->dtype == HPSI_C128)
+    s = apply_h_dev<double>(h, static_cast<const double *>(pin), ldi, static_cast<double *>(pout), ldo, terms, set_bc,
+                            st);
+  else
+    s = apply_h_dev<float>(h, static_cast<const float *>(pin), ldi, static_cast<float *>(pout), ldo, terms, set_bc,
+                           st);
+  if (s) return s;
+  if (!dout) {
+    const size_t esz = hpsi->dtype == HPSI_C128 ? 16 : 8;
+    HPSI_TRY_CUDA(cudaMemcpyAsync(hpsi->ptr, pout, size_t(m->np) * ldo * esz, cudaMemcpyDeviceToHost, st));
+  }
+  if (!din || !dout) HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_boundaries_set(hpsi_hamiltonian *h, hpsi_batch *psi, void *stream) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_mesh *m = h->mesh;
+  hpsi_status s = check_batch(m, psi, m->np_part, "hpsi_boundaries_set");
+  if (s) return s;
+  if (!is_device_ptr(psi->ptr)) {
+    set_error("hpsi_boundaries_set: device batch expected");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nb = m->np_part - m->np;
+  if (nb == 0) return HPSI_OK;
+  const long long n = (long long)nb * psi->ld;
+  if (psi->dtype == HPSI_C128)
+    boundaries_kernel<double><<<unsigned((n + 255) / 256), 256, 0, st>>>(
+        static_cast<double *>(psi->ptr), psi->ld, m->np, nb, m->d_per_inner, h->d_phase, m->periodic);
+  else
+    boundaries_kernel<float><<<unsigned((n + 255) / 256), 256, 0, st>>>(
+        static_cast<float *>(psi->ptr), psi->ld, m->np, nb, m->d_per_inner, h->d_phase_f, m->periodic);
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_taylor_step(hpsi_hamiltonian *h, hpsi_batch *psi, double dt_re, double dt_im, int32_t order,
+                             double *energy, double *dipole, double *norm2, void *stream) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_mesh *m = h->mesh;
+  hpsi_status s = check_batch(m, psi, m->np, "hpsi_taylor_step");
+  if (s) return s;
+  if (order < 1 || order > 32) {
+    set_error("hpsi_taylor_step: order must be 1..32");
+    return HPSI_ERR_ARG;
+  }
+  if (!h->have_kinetic) {
+    set_error("hpsi_taylor_step: kinetic weights not set");
+    return HPSI_ERR_STATE;
+  }
+  if (!std::isfinite(dt_re) || !std::isfinite(dt_im)) return HPSI_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool want_obs = energy || dipole || norm2;
+  double *obs_dev = nullptr;
+  if (want_obs) {
+    s = h->small.ensure(3 * size_t(psi->nst) * sizeof(double));
+    if (s) return s;
+    obs_dev = static_cast<double *>(h->small.ptr);
+  }
+  const bool dev = is_device_ptr(psi->ptr);
+  void *p = psi->ptr;
+  if (!dev) {
+    s = stage_batch(m->stage_in, psi, m->np, true, st, &p);
+    if (s) return s;
+  }
+  if (psi->dtype == HPSI_C128)
+    s = taylor_dev<double>(h, static_cast<double *>(p), psi->ld, psi->nst, dt_re, dt_im, order, obs_dev, st);
+  else
+    s = taylor_dev<float>(h, static_cast<float *>(p), psi->ld, psi->nst, dt_re, dt_im, order, obs_dev, st);
+  if (s) return s;
+  if (!dev) {
+    const size_t esz = psi->dtype == HPSI_C128 ? 16 : 8;
+    HPSI_TRY_CUDA(cudaMemcpyAsync(psi->ptr, p, size_t(m->np) * psi->ld * esz, cudaMemcpyDeviceToHost, st));
+  }
+  if (want_obs) {
+    std::vector<double> hv(3 * size_t(psi->nst));
+    HPSI_TRY_CUDA(cudaMemcpyAsync(hv.data(), obs_dev, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+    bool finite = true;
+    for (double x : hv) finite = finite && std::isfinite(x);
+    const int n = psi->nst;
+    if (energy) std::memcpy(energy, hv.data(), n * sizeof(double));
+    if (norm2) std::memcpy(norm2, hv.data() + n, n * sizeof(double));
+    if (dipole) std::memcpy(dipole, hv.data() + 2 * n, n * sizeof(double));
+    if (!finite) {
+      set_error("hpsi_taylor_step: non-finite observable (NaN/Inf in the batch)");
+      return HPSI_ERR_NONFINITE;
+    }
+  } else if (!dev) {
+    HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  }
+  return HPSI_OK;
+}
+
+// ---------------------------------------------------------------------------
+hpsi_status hpsi_nrm2(hpsi_mesh *m, const hpsi_batch *psi, double *out, void *stream) {
+  if (!m || !out) return HPSI_ERR_ARG;
+  hpsi_status s = check_batch(m, psi, m->np, "hpsi_nrm2");
+  if (s) return s;
+  if (!is_device_ptr(psi->ptr)) {
+    set_error("hpsi_nrm2: device batch expected");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nblk = reduce_blocks(m->np);
+  const size_t pbytes = size_t(nblk) * psi->nst * 4 * sizeof(double);
+  s = m->scratch.ensure(pbytes + 2 * size_t(psi->nst) * sizeof(double));
+  if (s) return s;
+  double *partial = static_cast<double *>(m->scratch.ptr);
+  double *res = partial + size_t(nblk) * psi->nst * 4;
+  const double dv = m->box.h[0] * m->box.h[1] * m->box.h[2];
+  if (psi->dtype == HPSI_C128)
+    s = launch_state_sum<double>(0, static_cast<const double *>(psi->ptr), psi->ld, nullptr, 0, m->np, psi->nst,
+                                 partial, nblk, dv, 1, res, st);
+  else
+    s = launch_state_sum<float>(0, static_cast<const float *>(psi->ptr), psi->ld, nullptr, 0, m->np, psi->nst,
+                                partial, nblk, dv, 1, res, st);
+  if (s) return s;
+  std::vector<double> hv(2 * size_t(psi->nst));
+  HPSI_TRY_CUDA(cudaMemcpyAsync(hv.data(), res, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < psi->nst; ++i) out[i] = hv[2 * i];
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_dotp_matrix(hpsi_mesh *m, const hpsi_batch *a, const hpsi_batch *b, double *out, void *stream) {
+  if (!m || !out) return HPSI_ERR_ARG;
+  hpsi_status s = check_batch(m, a, m->np, "hpsi_dotp_matrix(a)");
+  if (!s) s = check_batch(m, b, m->np, "hpsi_dotp_matrix(b)");
+  if (s) return s;
+  if (a->dtype != b->dtype || a->nst != b->nst) {
+    set_error("hpsi_dotp_matrix: a and b differ in dtype or nst");
+    return HPSI_ERR_ARG;
+  }
+  if (!is_device_ptr(a->ptr) || !is_device_ptr(b->ptr)) {
+    set_error("hpsi_dotp_matrix: device batches expected");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nst = a->nst, splits = gram_splits(m->np);
+  const size_t pbytes = size_t(splits) * 4 * nst * nst * sizeof(double);
+  s = m->scratch.ensure(pbytes + 2 * size_t(nst) * nst * sizeof(double));
+  if (s) return s;
+  double *partial = static_cast<double *>(m->scratch.ptr);
+  double *S = partial + size_t(splits) * 4 * nst * nst;
+  const double dv = m->box.h[0] * m->box.h[1] * m->box.h[2];
+  if (a->dtype == HPSI_C128)
+    s = launch_gram<double>(static_cast<const double *>(a->ptr), a->ld, static_cast<const double *>(b->ptr), b->ld,
+                            m->np, nst, partial, splits, dv, S, st);
+  else
+    s = launch_gram<float>(static_cast<const float *>(a->ptr), a->ld, static_cast<const float *>(b->ptr), b->ld,
+                           m->np, nst, partial, splits, dv, S, st);
+  if (s) return s;
+  HPSI_TRY_CUDA(cudaMemcpyAsync(out, S, 2 * size_t(nst) * nst * sizeof(double), cudaMemcpyDeviceToHost, st));
+  HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_orthonormalize_cholesky(hpsi_mesh *m, hpsi_batch *psi, void *stream) {
+  if (!m) return HPSI_ERR_ARG;
+  hpsi_status s = check_batch(m, psi, m->np, "hpsi_orthonormalize_cholesky");
+  if (s) return s;
+  if (!is_device_ptr(psi->ptr)) {
+    set_error("hpsi_orthonormalize_cholesky: device batch expected");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nst = psi->nst, splits = gram_splits(m->np);
+  const size_t pbytes = size_t(splits) * 4 * nst * nst * sizeof(double);
+  const size_t mbytes = 2 * size_t(nst) * nst * sizeof(double);
+  s = m->scratch.ensure(pbytes + 3 * mbytes + 16);
+  if (s) return s;
+  double *partial = static_cast<double *>(m->scratch.ptr);
+  double *S = partial + size_t(splits) * 4 * nst * nst;
+  double *U = S + 2 * size_t(nst) * nst;
+  double *Uinv = U + 2 * size_t(nst) * nst;
+  int *err = reinterpret_cast<int *>(Uinv + 2 * size_t(nst) * nst);
+  HPSI_TRY_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  const double dv = m->box.h[0] * m->box.h[1] * m->box.h[2];
+  if (psi->dtype == HPSI_C128)
+    s = launch_gram<double>(static_cast<const double *>(psi->ptr), psi->ld, static_cast<const double *>(psi->ptr),
+                            psi->ld, m->np, nst, partial, splits, dv, S, st);
+  else
+    s = launch_gram<float>(static_cast<const float *>(psi->ptr), psi->ld, static_cast<const float *>(psi->ptr),
+                           psi->ld, m->np, nst, partial, splits, dv, S, st);
+  if (s) return s;
+  s = launch_cholesky_inverse(S, nst, U, Uinv, err, st);
+  if (s) return s;
+  int herr = 0;
+  HPSI_TRY_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  if (herr) {
+    set_error("hpsi_orthonormalize_cholesky: overlap matrix is not positive definite");
+    return HPSI_ERR_ARG;
+  }
+  if (psi->dtype == HPSI_C128)
+    s = launch_trsm_apply<double>(static_cast<double *>(psi->ptr), psi->ld, m->np, nst, Uinv, st);
+  else
+    s = launch_trsm_apply<float>(static_cast<float *>(psi->ptr), psi->ld, m->np, nst, Uinv, st);
+  return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+// Handle layouts behind the opaque C types of hpsi.h.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace hpsi {
+
+hpsi_status dev_alloc(void **p, size_t bytes);
+void dev_free(void *p);
+bool is_device_ptr(const void *p);
+
+// Times the kernels launched in its scope on `st` when profiling is enabled.
+class ProfScope {
+ public:
+  ProfScope(const char *label, cudaStream_t st);
+  ~ProfScope();
+
+ private:
+  cudaStream_t st_;
+  long idx_ = -1;
+};
+
+// Grow-only device buffer owned by a handle.
+struct Workspace {
+  void *ptr = nullptr;
+  size_t size = 0;
+  hpsi_status ensure(size_t bytes);
+  void release();
+};
+
+}  // namespace hpsi
+
+struct hpsi_mesh {
+  int np = 0, np_part = 0, order = 4, periodic = 0;
+  hpsi::CellBox box{};
+  std::vector<int> per_inner_h;
+  std::vector<int> cell_of_row_h;
+  int *d_cell_row = nullptr;   // own row of each cell, -1 outside the mesh
+  int *d_src_raw = nullptr;    // load map: every mesh point as stored
+  int *d_src_zero = nullptr;   // load map: zero boundary condition
+  int *d_src_per = nullptr;    // load map: periodic images
+  int *d_per_inner = nullptr;
+  int *d_cell_of_row = nullptr;
+  int device = 0, num_sms = 148;
+  hpsi::Workspace scratch, scratch2, stage_in, stage_out;
+};
+
+struct hpsi_hamiltonian {
+  hpsi_mesh *mesh = nullptr;
+  bool have_kinetic = false;
+  double wx[9] = {0}, wy[9] = {0}, wz[9] = {0};
+  double *d_vcell = nullptr;
+  double fld[3] = {0, 0, 0};
+  double pol[3] = {0, 0, 1};
+  bool have_pol = false;
+  double *d_phase = nullptr;
+  float *d_phase_f = nullptr;
+  int *d_src_phase = nullptr;
+  // KB projectors
+  int nmat = 0, nprojections = 0, max_nproj = 0;
+  int4 *d_mat = nullptr;
+  int *d_proj_row = nullptr, *d_map = nullptr;
+  double *d_pt = nullptr, *d_scal = nullptr;
+  float *d_pt_f = nullptr, *d_scal_f = nullptr;
+  int *d_kb_ptr = nullptr;
+  int4 *d_kb_ent = nullptr;
+  bool use_tensor_bra = true;
+  // workspaces
+  hpsi::Workspace u[2], projbuf, obsbuf, small;
+  void proj_free();
+};

@@ -1,0 +1,164 @@
+// Kleinman-Bylander projector "bra": projections of a batch on the projector
+// spheres, the step X(hamiltonian_elec_base_nlocal_start) performs on the CPU
+// as a gather of the sphere points followed by a real GEMM
+// (src/hamiltonian/hamiltonian_elec_base_inc.F90:650-780):
+//   proj[row0(m) + j][s] = scal[j] * sum_k P_m[k][j] * psi[map_m[k]][s].
+// The matching "ket" (scatter-add of P * proj) is folded into the stencil
+// pass epilogue, so no scatter kernel and no write races exist.
+//
+// FP64: the contraction runs on the FP64 tensor cores (DMMA,
+// mma.sync.m8n8k4.f64): M = 8 real lanes per warp, N = 8 projectors per
+// tile, K = 4 sphere points per step, with the gathered rows and the
+// projector block staged in shared memory by cp.async.  FP32 uses the SIMT
+// kernel below (also used as the FP64 cross-check).
+#include "projector.cuh"
+
+namespace hpsi {
+
+namespace {
+
+constexpr int KB = 32;     // sphere points per staged block
+constexpr int LANES = 32;  // real lanes per CTA (16 complex states)
+constexpr int APAD = 40;   // padded row length of the staged psi block (doubles)
+constexpr int NMAX = 16;   // projectors per matrix served by the DMMA kernel
+
+__device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// grid: (nmat, ld2 / LANES); block: 128 threads (4 warps x 8 lanes each)
+__global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
+  __shared__ __align__(16) double sA[2][KB][APAD];
+  __shared__ __align__(16) double sB[2][KB][NMAX];
+  const int m = blockIdx.x;
+  const int l0 = blockIdx.y * LANES;
+  const int4 md = p.mat[m];  // npoints, nproj, map_off, pt_off
+  const int npts = md.x, npr = md.y;
+  const int *map = p.map + md.z;
+  const double *pt = static_cast<const double *>(p.pt) + md.w;
+  const double *psi = static_cast<const double *>(p.psi);
+  const long long ld2 = 2 * p.psi_ld;
+  const int tid = threadIdx.x, warp = tid >> 5, ln = tid & 31;
+
+  auto stage = [&](int k0, int b) {
+    // psi rows: KB points x 32 lanes = KB*8 copies of 16 bytes
+    for (int i = tid; i < KB * 8; i += 128) {
+      const int k = i >> 3, part = i & 7;
+      double *d = &sA[b][k][part * 4];
+      if (k0 + k < npts) {
+        const int row = __ldg(map + k0 + k);
+        const double *g = psi + row * ld2 + l0 + part * 4;
+        cp_async16(d, g);
+        cp_async16(d + 2, g + 2);
+      } else {
+        d[0] = d[1] = d[2] = d[3] = 0.0;
+      }
+    }
+    for (int i = tid; i < KB * NMAX; i += 128) {
+      const int k = i / NMAX, j = i % NMAX;
+      sB[b][k][j] = (k0 + k < npts && j < npr) ? __ldg(pt + (long long)(k0 + k) * npr + j) : 0.0;
+    }
+  };
+
+  double c0[2] = {0.0, 0.0}, c1[2] = {0.0, 0.0};
+  const int nblk = (npts + KB - 1) / KB;
+  stage(0, 0);
+  cp_async_commit();
+  for (int blk = 0; blk < nblk; ++blk) {
+    const int b = blk & 1;
+    if (blk + 1 < nblk) stage((blk + 1) * KB, b ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < KB; kk += 4) {
+      const double a = sA[b][kk + (ln & 3)][warp * 8 + (ln >> 2)];
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        const double bb = sB[b][kk + (ln & 3)][nt * 8 + (ln >> 2)];
+        dmma_m8n8k4(c0[nt], c1[nt], a, bb);
+      }
+    }
+    __syncthreads();
+  }
+  // C fragment: row (lane) = ln >> 2, cols (projectors) = (ln & 3) * 2 + {0,1}
+  const int lane = l0 + warp * 8 + (ln >> 2);
+  const double *scal = static_cast<const double *>(p.scal) + p.proj_row[m];
+  double *out = static_cast<double *>(p.proj) + (long long)p.proj_row[m] * 2 * p.proj_ld;
+#pragma unroll
+  for (int nt = 0; nt < 2; ++nt) {
+    const int j0 = nt * 8 + (ln & 3) * 2;
+    if (j0 < npr) out[(long long)j0 * 2 * p.proj_ld + lane] = c0[nt] * scal[j0];
+    if (j0 + 1 < npr) out[(long long)(j0 + 1) * 2 * p.proj_ld + lane] = c1[nt] * scal[j0 + 1];
+  }
+}
+
+// SIMT bra: grid (nmat, ceil(ld2/32)); block 128 = 32 lanes x 4 point groups
+template <typename T>
+__global__ void __launch_bounds__(128) bra_simt_kernel(const ProjArgs p) {
+  constexpr int MAXP = 32;
+  __shared__ T red[4][MAXP][32];
+  const int m = blockIdx.x;
+  const int ln = threadIdx.x & 31, grp = threadIdx.x >> 5;
+  const long long ld2 = 2 * p.psi_ld;
+  const int lane = blockIdx.y * 32 + ln;
+  const int4 md = p.mat[m];
+  const int npts = md.x, npr = md.y;
+  const int *map = p.map + md.z;
+  const T *pt = static_cast<const T *>(p.pt) + md.w;
+  const T *psi = static_cast<const T *>(p.psi);
+  T acc[MAXP];
+#pragma unroll
+  for (int j = 0; j < MAXP; ++j) acc[j] = T(0);
+  if (lane < ld2) {
+    for (int k = grp; k < npts; k += 4) {
+      const T x = psi[__ldg(map + k) * ld2 + lane];
+      const T *pk = pt + (long long)k * npr;
+#pragma unroll
+      for (int j = 0; j < MAXP; ++j)
+        if (j < npr) acc[j] += pk[j] * x;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < MAXP; ++j) red[grp][j][ln] = acc[j];
+  __syncthreads();
+  if (grp == 0 && lane < ld2) {
+    const T *scal = static_cast<const T *>(p.scal) + p.proj_row[m];
+    T *out = static_cast<T *>(p.proj) + (long long)p.proj_row[m] * 2 * p.proj_ld;
+    for (int j = 0; j < npr; ++j) {
+      const T s = red[0][j][ln] + red[1][j][ln] + red[2][j][ln] + red[3][j][ln];
+      out[(long long)j * 2 * p.proj_ld + lane] = s * scal[j];
+    }
+  }
+}
+
+}  // namespace
+
+template <typename T>
+hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, cudaStream_t st) {
+  if (p.nmat == 0) return HPSI_OK;
+  const long long ld2 = 2 * p.psi_ld;
+  if constexpr (sizeof(T) == 8) {
+    if (use_tensor && p.max_nproj <= NMAX && ld2 % LANES == 0) {
+      dim3 grid(p.nmat, unsigned(ld2 / LANES));
+      bra_dmma_kernel<<<grid, 128, 0, st>>>(p);
+      HPSI_CHECK_LAUNCH();
+      return HPSI_OK;
+    }
+  }
+  if (p.max_nproj > 32) {
+    set_error("projector matrices with more than 32 projectors are not supported");
+    return HPSI_ERR_UNSUPPORTED;
+  }
+  dim3 grid(p.nmat, unsigned((ld2 + 31) / 32));
+  bra_simt_kernel<T><<<grid, 128, 0, st>>>(p);
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+
+template hpsi_status launch_bra<double>(const ProjArgs &, bool, cudaStream_t);
+template hpsi_status launch_bra<float>(const ProjArgs &, bool, cudaStream_t);
+
+}  // namespace hpsi

@@ -1,0 +1,72 @@
+// Fused H.psi pass: star stencil + local potential + KB ket + Taylor/Horner
+// epilogue + FP64 observables, over a packed (state-fastest) batch in the
+// host's mesh point order.
+#pragma once
+
+#include "common.cuh"
+
+namespace hpsi {
+
+enum PassMode : int {
+  PASS_APPLY = 0,   // out = H in
+  PASS_HORNER = 1,  // out = psi0 + a * (H in)
+};
+
+struct PassArgs {
+  CellBox box;
+  const int *cell_src;    // per cell: source row to load, -1 zero, <= -2 periodic+phase
+  const int *cell_row;    // per cell: own row (inner < np, boundary >= np) or -1
+  const int *per_inner;   // boundary b -> inner image row (for encoded cells)
+  const void *phase_corr; // complex (np_part - np), storage type of the batch
+  int np;
+
+  const void *in;         // stencil input batch
+  long long in_ld;        // complex numbers per row
+  void *out;
+  long long out_ld;
+  const void *psi0;       // Horner: the untouched psi (pointwise term)
+  long long psi0_ld;
+  int mode;
+  double a_re, a_im;      // Horner coefficient
+
+  // per-axis weights, index d+4 for offset d; wx[4] holds the whole centre
+  // weight, wy[4] = wz[4] = 0
+  double wx[9], wy[9], wz[9];
+  const double *v_cell;   // local potential in cell layout, or null
+  double fld[3];          // laser: v += (fld . r), r = (cell + lo) * h
+  const double *fld_scale_dev;  // optional device scalar multiplying fld
+
+  // KB ket folded into the epilogue
+  const int *kb_ptr;      // np + 1
+  const int4 *kb_ent;     // {offset of the point's projector row, projection row, nproj, 0}
+  const void *kb_pt;      // projector values, projector index fastest per point
+  const void *proj;       // projections, complex [nprojections][proj_ld]
+  long long proj_ld;
+
+  // per-state observables of `in`: energy, norm, dipole partials
+  double *obs;            // [ncta_xyz][obs_ld][3][2] (Kahan sum, compensation)
+  int obs_ld;
+  double obs_pol[3];      // dipole direction
+
+  int zb;                 // output planes per CTA
+  int tiles_x, tiles_y, zblocks, chunks;
+  int *err_flag;          // device error word (index checks), may be null
+};
+
+// Kernel variant chosen for a pass.
+struct PassShape {
+  int sc;   // complex states per CTA
+  int tx, ty, ry;
+};
+
+// Launch the fused pass for a storage type (double -> FP64, float -> FP32).
+template <typename T>
+hpsi_status launch_pass(PassArgs a, const PassShape &shape, cudaStream_t st);
+
+// Number of CTAs along (tile, zblock) for the observables partial buffer.
+inline int pass_ncta_xyz(const PassArgs &a) { return a.tiles_x * a.tiles_y * a.zblocks; }
+
+// Choose tiles/zblocks for a shape on a box (host helper).
+void pass_geometry(PassArgs &a, const PassShape &s, int ld, int num_sms);
+
+}  // namespace hpsi

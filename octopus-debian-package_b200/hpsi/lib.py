@@ -1,0 +1,302 @@
+"""ctypes binding of libhpsi.so (the C ABI declared in include/hpsi.h).
+
+This is the Python host's counterpart of the Fortran ``bind(C)`` interface a
+maintainer adds to Octopus: the same entry points, the same argument meaning,
+and errors raised from the library's status codes.  Batches are torch tensors
+(device memory, streams) or numpy arrays (host memory, staged by the
+library).  There is no CPU fallback: if the shared library is missing the
+import fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libhpsi.so")
+
+HPSI_C128 = 0
+HPSI_C64 = 1
+TERM_KINETIC = 1
+TERM_LOCAL_POTENTIAL = 2
+TERM_NON_LOCAL_POTENTIAL = 4
+TERM_ALL = 0x7FFFFFFF
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_INDEX", 3: "ERR_NONFINITE", 4: "ERR_CUDA", 5: "ERR_TIMEOUT",
+          6: "ERR_STATE", 7: "ERR_NOMEM", 8: "ERR_RUNAWAY", 9: "ERR_UNSUPPORTED"}
+
+
+class HpsiError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("np", C.c_int32), ("np_part", C.c_int32), ("lxyz", C.POINTER(C.c_int32)),
+                ("spacing", C.c_double * 3), ("order", C.c_int32), ("periodic", C.c_int32),
+                ("per_inner", C.POINTER(C.c_int32))]
+
+
+class Batch(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("ld", C.c_int64), ("nst", C.c_int32), ("npts", C.c_int32),
+                ("dtype", C.c_int32)]
+
+
+_lib = None
+
+# declared entry points: name -> (restype, argtypes)
+SIGNATURES = {
+    "hpsi_mesh_create": (C.c_int32, [C.POINTER(MeshDesc), C.POINTER(C.c_void_p)]),
+    "hpsi_mesh_destroy": (C.c_int32, [C.c_void_p]),
+    "hpsi_mesh_info": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "hpsi_hamiltonian_create": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "hpsi_hamiltonian_destroy": (C.c_int32, [C.c_void_p]),
+    "hpsi_hamiltonian_set_kinetic": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
+                                                 C.POINTER(C.c_double), C.c_double]),
+    "hpsi_hamiltonian_set_vloc": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "hpsi_hamiltonian_set_field": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.c_double]),
+    "hpsi_hamiltonian_set_phase_corr": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "hpsi_hamiltonian_set_projectors": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
+                                                    C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "hpsi_apply_h": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_int32, C.c_int32,
+                                 C.c_void_p]),
+    "hpsi_boundaries_set": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_void_p]),
+    "hpsi_taylor_step": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_double, C.c_double, C.c_int32,
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                     C.c_void_p]),
+    "hpsi_nrm2": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_dotp_matrix": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(C.c_double),
+                                     C.c_void_p]),
+    "hpsi_orthonormalize_cholesky": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_void_p]),
+    "hpsi_last_error_string": (C.c_char_p, []),
+    "hpsi_kernel_launch_count": (C.c_int64, []),
+    "hpsi_version": (C.c_char_p, []),
+    "hpsi_profile_enable": (C.c_int32, [C.c_int32]),
+    "hpsi_profile_query": (C.c_int32, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
+}
+
+
+def load():
+    """Load libhpsi.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} not built (run `make` in {PKG})")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(status: int):
+    if status != 0:
+        raise HpsiError(status, load().hpsi_last_error_string().decode())
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except Exception:  # pragma: no cover
+            pass
+        return None
+    return C.c_void_p(getattr(stream, "cuda_stream", stream))
+
+
+def as_batch(x, npts=None, nst=None) -> Batch:
+    """Describe a packed batch: a (npts, ld) complex torch tensor or numpy array."""
+    b = Batch()
+    try:
+        import torch
+        is_t = isinstance(x, torch.Tensor)
+    except ImportError:  # pragma: no cover
+        is_t = False
+    if is_t:
+        if x.dim() != 2 or not x.is_contiguous():
+            raise ValueError("batch must be a contiguous (npts, ld) tensor")
+        if x.dtype == torch.complex128:
+            b.dtype = HPSI_C128
+        elif x.dtype == torch.complex64:
+            b.dtype = HPSI_C64
+        else:
+            raise ValueError("batch dtype must be complex128 or complex64")
+        b.ptr = x.data_ptr()
+    else:
+        x = np.asarray(x)
+        if x.ndim != 2 or not x.flags.c_contiguous:
+            raise ValueError("batch must be a C-contiguous (npts, ld) array")
+        b.dtype = {np.dtype(np.complex128): HPSI_C128, np.dtype(np.complex64): HPSI_C64}[x.dtype]
+        b.ptr = x.ctypes.data
+    b.ld = x.shape[1]
+    b.npts = x.shape[0] if npts is None else npts
+    b.nst = x.shape[1] if nst is None else nst
+    return b
+
+
+class DeviceMesh:
+    """hpsi_mesh handle built from a host :class:`hpsi.mesh.Mesh`."""
+
+    def __init__(self, mesh, order: int = 4):
+        L = load()
+        self.mesh = mesh
+        self._lxyz = np.ascontiguousarray(mesh.lxyz.astype(np.int32))
+        d = MeshDesc()
+        d.np = mesh.np
+        d.np_part = mesh.np_part
+        d.lxyz = _ip(self._lxyz)
+        for a in range(3):
+            d.spacing[a] = float(mesh.spacing[a])
+        d.order = order
+        d.periodic = 1 if mesh.periodic else 0
+        self._per = None
+        if mesh.periodic:
+            self._per = np.ascontiguousarray(mesh.per_inner.astype(np.int32))
+            d.per_inner = _ip(self._per)
+        h = C.c_void_p()
+        check(L.hpsi_mesh_create(C.byref(d), C.byref(h)))
+        self.handle = h
+
+    def info(self):
+        dims = (C.c_int32 * 6)()
+        check(load().hpsi_mesh_info(self.handle, dims))
+        return list(dims)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().hpsi_mesh_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # reductions (mesh_batch_* of the reference)
+    def nrm2(self, psi, nst=None, stream=None) -> np.ndarray:
+        b = as_batch(psi, nst=nst)
+        out = np.zeros(b.nst)
+        check(load().hpsi_nrm2(self.handle, C.byref(b), _dp(out), _stream_ptr(stream)))
+        return out
+
+    def dotp_matrix(self, a, b, nst=None, stream=None) -> np.ndarray:
+        ba, bb = as_batch(a, nst=nst), as_batch(b, nst=nst)
+        out = np.zeros((ba.nst, ba.nst), dtype=np.complex128)
+        check(load().hpsi_dotp_matrix(self.handle, C.byref(ba), C.byref(bb), _dp(out.view(np.float64)),
+                                      _stream_ptr(stream)))
+        return out
+
+    def orthonormalize_cholesky(self, psi, nst=None, stream=None):
+        b = as_batch(psi, nst=nst)
+        check(load().hpsi_orthonormalize_cholesky(self.handle, C.byref(b), _stream_ptr(stream)))
+
+
+class Hamiltonian:
+    """hpsi_hamiltonian handle: kinetic weights, local potential, KB projectors."""
+
+    def __init__(self, dmesh: DeviceMesh, weights, points, v=None, projectors=None, factor=-0.5):
+        L = load()
+        self.dmesh = dmesh
+        h = C.c_void_p()
+        check(L.hpsi_hamiltonian_create(dmesh.handle, C.byref(h)))
+        self.handle = h
+        pts = np.ascontiguousarray(np.asarray(points, dtype=np.int32))
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+        check(L.hpsi_hamiltonian_set_kinetic(h, len(w), _ip(pts), _dp(w), C.c_double(factor)))
+        if v is not None:
+            self.set_vloc(v)
+        if projectors is not None:
+            self.set_projectors(projectors.maps, projectors.mats, projectors.scals)
+
+    def set_vloc(self, v):
+        v = np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+        check(load().hpsi_hamiltonian_set_vloc(self.handle, _dp(v)))
+
+    def set_field(self, pol, amplitude: float):
+        p = np.ascontiguousarray(np.asarray(pol, dtype=np.float64))
+        check(load().hpsi_hamiltonian_set_field(self.handle, _dp(p), C.c_double(amplitude)))
+
+    def set_phase_corr(self, phase_corr):
+        if phase_corr is None:
+            check(load().hpsi_hamiltonian_set_phase_corr(self.handle, None))
+            return
+        pc = np.ascontiguousarray(np.asarray(phase_corr, dtype=np.complex128))
+        check(load().hpsi_hamiltonian_set_phase_corr(self.handle, _dp(pc.view(np.float64))))
+
+    def set_projectors(self, maps, mats, scals):
+        npts = np.asarray([len(m) for m in maps], dtype=np.int32)
+        nproj = np.asarray([m.shape[1] for m in mats], dtype=np.int32)
+        mp = np.ascontiguousarray(np.concatenate(maps).astype(np.int32))
+        mt = np.ascontiguousarray(np.concatenate([np.asarray(m, dtype=np.float64).T.ravel() for m in mats]))
+        sc = np.ascontiguousarray(np.concatenate(scals).astype(np.float64))
+        check(load().hpsi_hamiltonian_set_projectors(self.handle, len(maps), _ip(npts), _ip(nproj), _ip(mp),
+                                                     _dp(mt), _dp(sc)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().hpsi_hamiltonian_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # X(hamiltonian_elec_apply_batch)
+    def apply(self, psi, hpsi, nst=None, terms=TERM_ALL, set_bc=True, stream=None):
+        bi = as_batch(psi, nst=nst)
+        bo = as_batch(hpsi, nst=nst)
+        check(load().hpsi_apply_h(self.handle, C.byref(bi), C.byref(bo), terms, 1 if set_bc else 0,
+                                  _stream_ptr(stream)))
+
+    def boundaries_set(self, psi, nst=None, stream=None):
+        b = as_batch(psi, nst=nst)
+        check(load().hpsi_boundaries_set(self.handle, C.byref(b), _stream_ptr(stream)))
+
+    # Taylor branch of exponential_apply_batch
+    def taylor_step(self, psi, dt, order=4, nst=None, observables=False, stream=None):
+        b = as_batch(psi, nst=nst)
+        dt = complex(dt)
+        if observables:
+            e, d, n = np.zeros(b.nst), np.zeros(b.nst), np.zeros(b.nst)
+            check(load().hpsi_taylor_step(self.handle, C.byref(b), dt.real, dt.imag, order, _dp(e), _dp(d),
+                                          _dp(n), _stream_ptr(stream)))
+            return e, d, n
+        check(load().hpsi_taylor_step(self.handle, C.byref(b), dt.real, dt.imag, order, None, None, None,
+                                      _stream_ptr(stream)))
+        return None
+
+
+def launch_count() -> int:
+    return int(load().hpsi_kernel_launch_count())
+
+
+def profile_enable(on: bool = True):
+    check(load().hpsi_profile_enable(1 if on else 0))
+
+
+def profile_query(label: str):
+    """(launches, total device ms) of one kernel label since profile_enable."""
+    n = C.c_int64()
+    ms = C.c_double()
+    check(load().hpsi_profile_query(label.encode(), C.byref(n), C.byref(ms)))
+    return int(n.value), float(ms.value)
