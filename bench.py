@@ -261,6 +261,7 @@ def main():
     launches = lib.launch_count() - n0
     npass, pass_ms = lib.profile_query("pass_fp64")
     nbra, bra_ms = lib.profile_query("bra_fp64")
+    nket, ket_ms = lib.profile_query("ket_fp64")
     lib.profile_enable(False)
     ms_step = ms / args.steps
     value = world * m.np * nst * args.steps / (ms / 1e3) / 1e9
@@ -318,10 +319,11 @@ def main():
                     "d2h_bytes_per_step": int(m.np * nst * S)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "pass_fp64 (fused stencil + vpsi + KB ket)",
+                         "kernel": "pass_fp64 (fused stencil + local potential)",
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": pass_avg_ms},
             "kernels": {"pass_fp64": {"launches": npass, "ms": pass_ms},
-                        "bra_fp64": {"launches": nbra, "ms": bra_ms}},
+                        "bra_fp64": {"launches": nbra, "ms": bra_ms},
+                        "ket_fp64": {"launches": nket, "ms": ket_ms}},
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "extra": {

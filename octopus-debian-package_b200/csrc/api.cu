@@ -184,8 +184,8 @@ int pass_sc(int dtype, long long ld) {
 
 PassShape default_shape(int dtype, long long ld) {
   const int sc = pass_sc(dtype, ld);
-  // FP64 keeps 4 rows of 9 running sums per thread (36 doubles), FP32 8 rows
-  return dtype == HPSI_C128 ? PassShape{sc, 16, 16, 4} : PassShape{sc, 16, 16, sc >= 4 ? 8 : 4};
+  // a thread keeps RY rows of 9 complex running sums: FP64 2 rows, FP32 4
+  return dtype == HPSI_C128 ? PassShape{sc, 16, 16, 2} : PassShape{sc, 16, 16, 4};
 }
 
 }  // namespace hpsi
@@ -312,6 +312,18 @@ hpsi_status hpsi_mesh_create(const hpsi_mesh_desc *d, hpsi_mesh **out) {
     for (int b = 0; b < npp - np; ++b) src_per[cell_of_row[np + b]] = per[b];
   }
   hpsi_mesh *m = new hpsi_mesh();
+  m->tiles_x = (B.nxo + PASS_TILE - 1) / PASS_TILE;
+  m->tiles_y = (B.nyo + PASS_TILE - 1) / PASS_TILE;
+  m->tile_z.assign(size_t(m->tiles_x) * m->tiles_y, make_int2(1 << 30, -1));
+  for (int i = 0; i < np; ++i) {
+    const int c = cell_of_row[i];
+    const int x = c % B.NX, y = (c / B.NX) % B.NY, z = c / (B.NX * B.NY);
+    int2 &t = m->tile_z[size_t((y - HAL) / PASS_TILE) * m->tiles_x + (x - HAL) / PASS_TILE];
+    t.x = std::min(t.x, z);
+    t.y = std::max(t.y, z);
+  }
+  for (auto &t : m->tile_z)
+    if (t.y >= 0) m->column_planes += t.y - t.x + 1;
   m->np = np;
   m->np_part = npp;
   m->order = ord;
@@ -359,6 +371,7 @@ hpsi_status hpsi_mesh_destroy(hpsi_mesh *m) {
   dev_free(m->d_cell_of_row);
   m->scratch.release();
   m->scratch2.release();
+  for (auto &kv : m->items) dev_free(kv.second.first);
   m->stage_in.release();
   m->stage_out.release();
   delete m;
@@ -394,7 +407,9 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   h->proj_free();
   for (auto &w : h->u) w.release();
   h->projbuf.release();
+  h->bra_partial.release();
   h->obsbuf.release();
+  h->ketobs.release();
   h->small.release();
   delete h;
   return HPSI_OK;
@@ -408,10 +423,13 @@ void hpsi_hamiltonian::proj_free() {
   dev_free(d_pt_f);
   dev_free(d_scal);
   dev_free(d_scal_f);
-  dev_free(d_kb_ptr);
+  dev_free(d_krows);
+  dev_free(d_kptr);
   dev_free(d_kb_ent);
   d_mat = nullptr;
-  d_proj_row = d_map = d_kb_ptr = nullptr;
+  d_proj_row = d_map = d_krows = d_kptr = nullptr;
+  nk = 0;
+  min_npoints = 0;
   d_pt = d_scal = nullptr;
   d_pt_f = d_scal_f = nullptr;
   d_kb_ent = nullptr;
@@ -582,6 +600,15 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, c
       const int row = map[mat[i].z + k];
       ent[fill[row]++] = make_int4(mat[i].w + k * nprojs[i], prow[i], nprojs[i], 0);
     }
+  // compress to the covered rows (entries stay in matrix order per row)
+  std::vector<int> krows, kptr(1, 0);
+  for (int r = 0; r < m->np; ++r)
+    if (cnt[r + 1] > cnt[r]) {
+      krows.push_back(r);
+      kptr.push_back(cnt[r + 1]);
+    }
+  int minp = 1 << 30;
+  for (int i = 0; i < nmat; ++i) minp = std::min(minp, int(npoints[i]));
   hpsi_status s = HPSI_OK;
   auto up = [&](void **dp, const void *src, size_t bytes) {
     if (s) return;
@@ -601,7 +628,8 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, c
   up(reinterpret_cast<void **>(&h->d_pt_f), ptf.data(), ptf.size() * sizeof(float));
   up(reinterpret_cast<void **>(&h->d_scal), scal, size_t(nproj_tot) * sizeof(double));
   up(reinterpret_cast<void **>(&h->d_scal_f), scf.data(), scf.size() * sizeof(float));
-  up(reinterpret_cast<void **>(&h->d_kb_ptr), cnt.data(), cnt.size() * sizeof(int));
+  up(reinterpret_cast<void **>(&h->d_krows), krows.data(), krows.size() * sizeof(int));
+  up(reinterpret_cast<void **>(&h->d_kptr), kptr.data(), kptr.size() * sizeof(int));
   up(reinterpret_cast<void **>(&h->d_kb_ent), ent.data(), ent.size() * sizeof(int4));
   if (s) {
     h->proj_free();
@@ -610,6 +638,8 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, c
   h->nmat = nmat;
   h->nprojections = nproj_tot;
   h->max_nproj = maxp;
+  h->nk = int(krows.size());
+  h->min_npoints = minp;
   return HPSI_OK;
 }
 
@@ -617,6 +647,42 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, c
 
 // ===========================================================================
 namespace hpsi {
+
+// z block depth of a pass: the largest depth that still gives about four
+// waves of CTAs (each block re-reads a 4-plane halo above and below).
+int choose_zb(const hpsi_mesh *m, int chunks) {
+  const long long want = 4LL * m->num_sms;
+  const int cands[] = {1 << 20, 96, 64, 48, 32, 24, 16};
+  for (int zb : cands) {
+    long long n = 0;
+    for (auto &t : m->tile_z)
+      if (t.y >= 0) n += (t.y - t.x + zb) / zb;
+    if (n * chunks >= want) return zb;
+  }
+  return 16;
+}
+
+// Work list {tile x, tile y, first plane, end plane} for a z block depth.
+hpsi_status mesh_items(hpsi_mesh *m, int zb, const int4 **items, int *nitems) {
+  auto it = m->items.find(zb);
+  if (it == m->items.end()) {
+    std::vector<int4> v;
+    for (int by = 0; by < m->tiles_y; ++by)
+      for (int bx = 0; bx < m->tiles_x; ++bx) {
+        const int2 t = m->tile_z[size_t(by) * m->tiles_x + bx];
+        if (t.y < 0) continue;
+        for (int z = t.x; z <= t.y; z += zb) v.push_back(make_int4(bx, by, z, std::min(z + zb, t.y + 1)));
+      }
+    int4 *d = nullptr;
+    hpsi_status s = dev_alloc(reinterpret_cast<void **>(&d), std::max<size_t>(1, v.size()) * sizeof(int4));
+    if (s) return s;
+    if (!v.empty()) HPSI_TRY_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    it = m->items.emplace(zb, std::make_pair(d, int(v.size()))).first;
+  }
+  *items = it->second.first;
+  *nitems = it->second.second;
+  return HPSI_OK;
+}
 
 // Build the pass arguments shared by apply and Taylor passes.
 void base_pass_args(const hpsi_hamiltonian *h, int terms, const int *src_map, PassArgs &a) {
@@ -631,6 +697,11 @@ void base_pass_args(const hpsi_hamiltonian *h, int terms, const int *src_map, Pa
     std::memcpy(a.wx, h->wx, sizeof(a.wx));
     std::memcpy(a.wy, h->wy, sizeof(a.wy));
     std::memcpy(a.wz, h->wz, sizeof(a.wz));
+  }
+  for (int k = 0; k < 9; ++k) {
+    a.wxf[k] = float(a.wx[k]);
+    a.wyf[k] = float(a.wy[k]);
+    a.wzf[k] = float(a.wz[k]);
   }
   if (terms & HPSI_TERM_LOCAL_POTENTIAL) {
     a.v_cell = h->d_vcell;
@@ -657,8 +728,39 @@ hpsi_status run_bra(hpsi_hamiltonian *h, const T *psi, long long ld, T *proj, cu
   p.psi_ld = ld;
   p.proj = proj;
   p.proj_ld = ld;
+  p.nprojections = h->nprojections;
+  p.min_npoints = h->min_npoints;
+  const int ksplit = bra_ksplit(p, h->mesh->num_sms);
+  hpsi_status s = h->bra_partial.ensure(size_t(ksplit) * h->nprojections * ld * 2 * sizeof(T));
+  if (s) return s;
+  p.partial = h->bra_partial.ptr;
   ProfScope prof(sizeof(T) == 8 ? "bra_fp64" : "bra_fp32", st);
-  return launch_bra<T>(p, h->use_tensor_bra, st);
+  return launch_bra<T>(p, h->use_tensor_bra, ksplit, st);
+}
+
+template <typename T>
+hpsi_status run_ket(hpsi_hamiltonian *h, const T *proj, long long ld, int nst, T *out, long long out_ld, int mode,
+                    double a_re, double a_im, const T *psi0, long long psi0_ld, double *obs, cudaStream_t st) {
+  KetArgs k;
+  k.nk = h->nk;
+  k.krows = h->d_krows;
+  k.kptr = h->d_kptr;
+  k.ent = h->d_kb_ent;
+  k.pt = sizeof(T) == 8 ? static_cast<const void *>(h->d_pt) : static_cast<const void *>(h->d_pt_f);
+  k.proj = proj;
+  k.proj_ld = ld;
+  k.out = out;
+  k.out_ld = out_ld;
+  k.nst = nst;
+  k.mode = mode;
+  k.a_re = a_re;
+  k.a_im = a_im;
+  k.psi0 = psi0;
+  k.psi0_ld = psi0_ld;
+  k.obs = obs;
+  k.obs_ld = int(ld);
+  ProfScope prof(sizeof(T) == 8 ? "ket_fp64" : "ket_fp32", st);
+  return launch_ket<T>(k, st);
 }
 
 // One fused pass.  in: rows to stencil; out: result rows; psi0 for Horner.
@@ -686,21 +788,35 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
     if (s) return s;
     s = run_bra<T>(h, in, in_ld, static_cast<T *>(h->projbuf.ptr), st);
     if (s) return s;
-    a.kb_ptr = h->d_kb_ptr;
-    a.kb_ent = h->d_kb_ent;
-    a.kb_pt = sizeof(T) == 8 ? static_cast<const void *>(h->d_pt) : static_cast<const void *>(h->d_pt_f);
-    a.proj = h->projbuf.ptr;
-    a.proj_ld = in_ld;
   }
   const PassShape shape = default_shape(sizeof(T) == 8 ? HPSI_C128 : HPSI_C64, ld);
-  pass_geometry(a, shape, int(ld), h->mesh->num_sms);
+  a.chunks = int(ld / shape.sc);
+  a.zb = choose_zb(h->mesh, a.chunks);
+  hpsi_status si = mesh_items(h->mesh, a.zb, &a.items, &a.nitems);
+  if (si) return si;
   if (obs_partial) {
     a.obs = obs_partial;
     a.obs_ld = int(ld);
   }
-  if (ncta_out) *ncta_out = pass_ncta_xyz(a);
-  ProfScope prof(sizeof(T) == 8 ? "pass_fp64" : "pass_fp32", st);
-  return launch_pass<T>(a, shape, st);
+  if (ncta_out) *ncta_out = a.nitems;
+  if (obs_partial && !psi0) a.psi0 = in, a.psi0_ld = in_ld;
+  {
+    ProfScope prof(sizeof(T) == 8 ? "pass_fp64" : "pass_fp32", st);
+    hpsi_status s = launch_pass<T>(a, shape, st);
+    if (s) return s;
+  }
+  if (nl) {
+    double *kobs = nullptr;
+    if (obs_partial) {
+      hpsi_status s = h->ketobs.ensure(size_t(ket_row_blocks(h->nk)) * ld * 2 * sizeof(double));
+      if (s) return s;
+      kobs = static_cast<double *>(h->ketobs.ptr);
+    }
+    hpsi_status s = run_ket<T>(h, static_cast<const T *>(h->projbuf.ptr), ld, int(ld), out, out_ld, mode, a_re, a_im,
+                               static_cast<const T *>(a.psi0), a.psi0_ld, kobs, st);
+    if (s) return s;
+  }
+  return HPSI_OK;
 }
 
 const int *load_map(const hpsi_hamiltonian *h, int set_bc) {
@@ -711,17 +827,16 @@ const int *load_map(const hpsi_hamiltonian *h, int set_bc) {
 }
 
 // size of the observables partial buffer for a pass over ld states
-size_t obs_partial_bytes(const hpsi_hamiltonian *h, long long ld) {
-  PassArgs a;
-  std::memset(&a, 0, sizeof(a));
-  a.box = h->mesh->box;
-  const PassShape shape = default_shape(HPSI_C128, ld);
-  pass_geometry(a, shape, int(ld), h->mesh->num_sms);
-  const PassShape shape32 = default_shape(HPSI_C64, ld);
-  PassArgs b = a;
-  pass_geometry(b, shape32, int(ld), h->mesh->num_sms);
-  const long long n = std::max(pass_ncta_xyz(a), pass_ncta_xyz(b));
-  return size_t(n) * ld * 6 * sizeof(double);
+size_t obs_partial_bytes(hpsi_hamiltonian *h, long long ld) {
+  size_t n = 0;
+  for (int dt : {HPSI_C128, HPSI_C64}) {
+    const PassShape sh = default_shape(dt, ld);
+    const int4 *items;
+    int nitems = 0;
+    if (mesh_items(h->mesh, choose_zb(h->mesh, int(ld / sh.sc)), &items, &nitems) == HPSI_OK)
+      n = std::max(n, size_t(nitems));
+  }
+  return std::max<size_t>(n, 1) * ld * 6 * sizeof(double);
 }
 
 template <typename T>
@@ -769,8 +884,10 @@ hpsi_status taylor_dev(hpsi_hamiltonian *h, T *psi, long long ld, int nst, doubl
     HPSI_CHECK_LAUNCH();
   }
   if (obs_dev) {
+    const bool nl = h->nmat > 0 && h->nk > 0;
     hpsi_status s = launch_obs_finalize(obs_partial, ncta, int(ld), nst, m->box.h[0] * m->box.h[1] * m->box.h[2],
-                                        obs_dev, st);
+                                        nl ? static_cast<const double *>(h->ketobs.ptr) : nullptr,
+                                        nl ? ket_row_blocks(h->nk) : 0, obs_dev, st);
     if (s) return s;
   }
   return HPSI_OK;

@@ -1,6 +1,7 @@
 // Handle layouts behind the opaque C types of hpsi.h.
 #pragma once
 
+#include <map>
 #include <vector>
 
 #include "common.cuh"
@@ -45,6 +46,11 @@ struct hpsi_mesh {
   int *d_cell_of_row = nullptr;
   int device = 0, num_sms = 148;
   hpsi::Workspace scratch, scratch2, stage_in, stage_out;
+  // z range {first, last} (cells) of the inner points of each 16x16 tile column
+  int tiles_x = 0, tiles_y = 0;
+  std::vector<int2> tile_z;
+  long long column_planes = 0;          // sum of the tile z extents
+  std::map<int, std::pair<int4 *, int>> items;  // work list per z block depth
 };
 
 struct hpsi_hamiltonian {
@@ -64,10 +70,12 @@ struct hpsi_hamiltonian {
   int *d_proj_row = nullptr, *d_map = nullptr;
   double *d_pt = nullptr, *d_scal = nullptr;
   float *d_pt_f = nullptr, *d_scal_f = nullptr;
-  int *d_kb_ptr = nullptr;
+  // rows covered by at least one sphere: krows[nk], entries kptr[nk+1] -> kb_ent
+  int nk = 0, min_npoints = 0;
+  int *d_krows = nullptr, *d_kptr = nullptr;
   int4 *d_kb_ent = nullptr;
   bool use_tensor_bra = true;
   // workspaces
-  hpsi::Workspace u[2], projbuf, obsbuf, small;
+  hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small;
   void proj_free();
 };

@@ -3,14 +3,18 @@
 // as a gather of the sphere points followed by a real GEMM
 // (src/hamiltonian/hamiltonian_elec_base_inc.F90:650-780):
 //   proj[row0(m) + j][s] = scal[j] * sum_k P_m[k][j] * psi[map_m[k]][s].
-// The matching "ket" (scatter-add of P * proj) is folded into the stencil
-// pass epilogue, so no scatter kernel and no write races exist.
+// The matching "ket" (add P * proj back onto the covered rows) runs per
+// covered row after the stencil pass: one thread per output element, so no
+// write races and no colouring are needed.
 //
 // FP64: the contraction runs on the FP64 tensor cores (DMMA,
 // mma.sync.m8n8k4.f64): M = 8 real lanes per warp, N = 8 projectors per
 // tile, K = 4 sphere points per step, with the gathered rows and the
 // projector block staged in shared memory by cp.async.  FP32 uses the SIMT
 // kernel below (also used as the FP64 cross-check).
+#include <algorithm>
+#include <type_traits>
+
 #include "projector.cuh"
 
 namespace hpsi {
@@ -28,16 +32,20 @@ __device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, do
                : "d"(a), "d"(b));
 }
 
-// grid: (nmat, ld2 / LANES); block: 128 threads (4 warps x 8 lanes each)
+// grid: (nmat, ld2 / LANES, ksplit); block: 128 threads (4 warps x 8 lanes
+// each).  Split z sums sphere points [z*npts/ksplit, (z+1)*npts/ksplit) into
+// partial[z] (unscaled); bra_reduce_kernel adds the splits and applies scal.
 __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
   __shared__ __align__(16) double sA[2][KB][APAD];
   __shared__ __align__(16) double sB[2][KB][NMAX];
   const int m = blockIdx.x;
   const int l0 = blockIdx.y * LANES;
   const int4 md = p.mat[m];  // npoints, nproj, map_off, pt_off
-  const int npts = md.x, npr = md.y;
-  const int *map = p.map + md.z;
-  const double *pt = static_cast<const double *>(p.pt) + md.w;
+  const int kbeg = int((long long)md.x * blockIdx.z / gridDim.z);
+  const int kend = int((long long)md.x * (blockIdx.z + 1) / gridDim.z);
+  const int npts = kend - kbeg, npr = md.y;
+  const int *map = p.map + md.z + kbeg;
+  const double *pt = static_cast<const double *>(p.pt) + md.w + (long long)kbeg * npr;
   const double *psi = static_cast<const double *>(p.psi);
   const long long ld2 = 2 * p.psi_ld;
   const int tid = threadIdx.x, warp = tid >> 5, ln = tid & 31;
@@ -85,14 +93,27 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
   }
   // C fragment: row (lane) = ln >> 2, cols (projectors) = (ln & 3) * 2 + {0,1}
   const int lane = l0 + warp * 8 + (ln >> 2);
-  const double *scal = static_cast<const double *>(p.scal) + p.proj_row[m];
-  double *out = static_cast<double *>(p.proj) + (long long)p.proj_row[m] * 2 * p.proj_ld;
+  double *out = static_cast<double *>(p.partial) +
+                ((long long)blockIdx.z * p.nprojections + p.proj_row[m]) * 2 * p.proj_ld;
 #pragma unroll
   for (int nt = 0; nt < 2; ++nt) {
     const int j0 = nt * 8 + (ln & 3) * 2;
-    if (j0 < npr) out[(long long)j0 * 2 * p.proj_ld + lane] = c0[nt] * scal[j0];
-    if (j0 + 1 < npr) out[(long long)(j0 + 1) * 2 * p.proj_ld + lane] = c1[nt] * scal[j0 + 1];
+    if (j0 < npr) out[(long long)j0 * 2 * p.proj_ld + lane] = c0[nt];
+    if (j0 + 1 < npr) out[(long long)(j0 + 1) * 2 * p.proj_ld + lane] = c1[nt];
   }
+}
+
+// proj[j][l] = scal[j] * sum_z partial[z][j][l]  (one thread per real lane)
+template <typename T>
+__global__ void bra_reduce_kernel(const ProjArgs p, int ksplit) {
+  const long long n = (long long)p.nprojections * 2 * p.proj_ld;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j = int(i / (2 * p.proj_ld));
+  const T *part = static_cast<const T *>(p.partial);
+  T acc = T(0);
+  for (int z = 0; z < ksplit; ++z) acc += part[(long long)z * n + i];
+  static_cast<T *>(p.proj)[i] = acc * static_cast<const T *>(p.scal)[j];
 }
 
 // SIMT bra: grid (nmat, ceil(ld2/32)); block 128 = 32 lanes x 4 point groups
@@ -136,14 +157,25 @@ __global__ void __launch_bounds__(128) bra_simt_kernel(const ProjArgs p) {
 
 }  // namespace
 
+int bra_ksplit(const ProjArgs &p, int num_sms) {
+  const long long ld2 = 2 * p.psi_ld;
+  const long long base = (long long)p.nmat * ((ld2 + LANES - 1) / LANES);
+  long long k = (4LL * num_sms + base - 1) / base;
+  k = std::min<long long>(k, std::max(1, p.min_npoints / 128));
+  return int(std::max<long long>(1, std::min<long long>(k, 64)));
+}
+
 template <typename T>
-hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, cudaStream_t st) {
+hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStream_t st) {
   if (p.nmat == 0) return HPSI_OK;
   const long long ld2 = 2 * p.psi_ld;
   if constexpr (sizeof(T) == 8) {
     if (use_tensor && p.max_nproj <= NMAX && ld2 % LANES == 0) {
-      dim3 grid(p.nmat, unsigned(ld2 / LANES));
+      dim3 grid(p.nmat, unsigned(ld2 / LANES), ksplit);
       bra_dmma_kernel<<<grid, 128, 0, st>>>(p);
+      HPSI_CHECK_LAUNCH();
+      const long long n = (long long)p.nprojections * ld2;
+      bra_reduce_kernel<T><<<unsigned((n + 255) / 256), 256, 0, st>>>(p, ksplit);
       HPSI_CHECK_LAUNCH();
       return HPSI_OK;
     }
@@ -158,7 +190,90 @@ hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, cudaStream_t st) {
   return HPSI_OK;
 }
 
-template hpsi_status launch_bra<double>(const ProjArgs &, bool, cudaStream_t);
-template hpsi_status launch_bra<float>(const ProjArgs &, bool, cudaStream_t);
+// ---------------------------------------------------------------------------
+// KB ket, one thread per (covered row, complex state): h = sum over the
+// row's (matrix, point) entries of P[point][j] * proj[j], then
+// out[row] += h (apply) or += a * h (Horner pass), and, if requested, the
+// energy partial Re(conj(psi0[row]) h) per state.  Each output element is
+// written by exactly one thread, in a fixed order: no atomics, deterministic.
+namespace {
+template <typename T, typename C2>
+__global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
+  const int s = blockIdx.x * 32 + threadIdx.x;
+  const bool active = s < k.nst;
+  const T *pt = static_cast<const T *>(k.pt);
+  const C2 *proj = static_cast<const C2 *>(k.proj);
+  C2 *out = static_cast<C2 *>(k.out);
+  const C2 *psi0 = static_cast<const C2 *>(k.psi0);
+  Kahan ke = {0, 0};
+  for (int i = blockIdx.y * 8 + threadIdx.y; i < k.nk; i += gridDim.y * 8) {
+    if (!active) continue;
+    const int row = k.krows[i];
+    C2 h;
+    h.x = 0;
+    h.y = 0;
+    for (int e = k.kptr[i]; e < k.kptr[i + 1]; ++e) {
+      const int4 E = __ldg(k.ent + e);
+      const T *pp = pt + E.x;
+      const C2 *pr = proj + (long long)E.y * k.proj_ld + s;
+      for (int j = 0; j < E.z; ++j) {
+        const T w = pp[j];
+        const C2 v = pr[(long long)j * k.proj_ld];
+        h.x += w * v.x;
+        h.y += w * v.y;
+      }
+    }
+    C2 *o = out + (long long)row * k.out_ld + s;
+    C2 y = *o;
+    if (k.mode == 1) {
+      const T ar = T(k.a_re), ai = T(k.a_im);
+      y.x += ar * h.x - ai * h.y;
+      y.y += ar * h.y + ai * h.x;
+    } else {
+      y.x += h.x;
+      y.y += h.y;
+    }
+    *o = y;
+    if (k.obs) {
+      const C2 x = psi0[(long long)row * k.psi0_ld + s];
+      kadd(ke, double(x.x) * double(h.x) + double(x.y) * double(h.y));
+    }
+  }
+  if (k.obs) {
+    __shared__ double red[8][32][2];
+    red[threadIdx.y][threadIdx.x][0] = ke.s;
+    red[threadIdx.y][threadIdx.x][1] = ke.c;
+    __syncthreads();
+    if (threadIdx.y == 0 && active) {
+      Kahan a = {0, 0};
+      for (int y = 0; y < 8; ++y) {
+        kadd(a, red[y][threadIdx.x][0]);
+        a.c += red[y][threadIdx.x][1];
+      }
+      double *o = k.obs + ((long long)blockIdx.y * k.obs_ld + s) * 2;
+      o[0] = a.s;
+      o[1] = a.c;
+    }
+  }
+}
+}  // namespace
+
+int ket_row_blocks(int nk) { return std::max(1, std::min(1024, (nk + 7) / 8)); }
+
+template <typename T>
+hpsi_status launch_ket(const KetArgs &k, cudaStream_t st) {
+  if (k.nk == 0) return HPSI_OK;
+  using C2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  dim3 grid((k.nst + 31) / 32, ket_row_blocks(k.nk));
+  ket_kernel<T, C2><<<grid, dim3(32, 8), 0, st>>>(k);
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+
+template hpsi_status launch_ket<double>(const KetArgs &, cudaStream_t);
+template hpsi_status launch_ket<float>(const KetArgs &, cudaStream_t);
+
+template hpsi_status launch_bra<double>(const ProjArgs &, bool, int, cudaStream_t);
+template hpsi_status launch_bra<float>(const ProjArgs &, bool, int, cudaStream_t);
 
 }  // namespace hpsi

@@ -17,9 +17,36 @@ struct ProjArgs {
   long long psi_ld;
   void *proj;            // projections [nprojections][proj_ld] complex
   long long proj_ld;
+  int nprojections;
+  int min_npoints;       // smallest sphere (bounds the K split)
+  void *partial;         // split-K partials [ksplit][nprojections][proj_ld] complex
 };
 
+struct KetArgs {
+  int nk;                // covered rows
+  const int *krows;      // covered row -> mesh row
+  const int *kptr;       // nk + 1 offsets into ent
+  const int4 *ent;       // {projector value offset, projection row, nproj, 0}
+  const void *pt;        // projector values
+  const void *proj;      // projections [nprojections][proj_ld] complex
+  long long proj_ld;
+  void *out;             // batch receiving the ket
+  long long out_ld;
+  int nst;
+  int mode;              // 0: out += h; 1: out += a * h
+  double a_re, a_im;
+  const void *psi0;      // energy partials: Re(conj(psi0) h)
+  long long psi0_ld;
+  double *obs;           // [ket_row_blocks][obs_ld][2] or null
+  int obs_ld;
+};
+
+int bra_ksplit(const ProjArgs &p, int num_sms);
+int ket_row_blocks(int nk);
+
 template <typename T>
-hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, cudaStream_t st);
+hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStream_t st);
+template <typename T>
+hpsi_status launch_ket(const KetArgs &k, cudaStream_t st);
 
 }  // namespace hpsi

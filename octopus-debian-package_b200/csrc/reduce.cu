@@ -256,7 +256,8 @@ __global__ void __launch_bounds__(256) trsm_apply_kernel(T *psi, long long ld, i
 }
 
 // observables: partial [ncta][ld][3][2] -> out[3][nst] (energy, norm2, dipole) * dv
-__global__ void obs_finalize_kernel(const double *partial, int ncta, int ld, int nst, double dv, double *out) {
+__global__ void obs_finalize_kernel(const double *partial, int ncta, int ld, int nst, double dv,
+                                    const double *ket_partial, int nket, double *out) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nst) return;
   for (int q = 0; q < 3; ++q) {
@@ -266,6 +267,12 @@ __global__ void obs_finalize_kernel(const double *partial, int ncta, int ld, int
       kadd(a, p[0]);
       a.c += p[1];
     }
+    if (q == 0 && ket_partial)
+      for (int c = 0; c < nket; ++c) {
+        const double *p = ket_partial + ((long long)c * ld + s) * 2;
+        kadd(a, p[0]);
+        a.c += p[1];
+      }
     out[q * nst + s] = (a.s + a.c) * dv;
   }
 }
@@ -330,9 +337,9 @@ hpsi_status launch_trsm_apply(T *psi, long long ld, int np, int nst, const doubl
   return HPSI_OK;
 }
 
-hpsi_status launch_obs_finalize(const double *partial, int ncta, int ld, int nst, double dv, double *out,
-                                cudaStream_t st) {
-  obs_finalize_kernel<<<(nst + 127) / 128, 128, 0, st>>>(partial, ncta, ld, nst, dv, out);
+hpsi_status launch_obs_finalize(const double *partial, int ncta, int ld, int nst, double dv,
+                                const double *ket_partial, int nket, double *out, cudaStream_t st) {
+  obs_finalize_kernel<<<(nst + 127) / 128, 128, 0, st>>>(partial, ncta, ld, nst, dv, ket_partial, nket, out);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
 }

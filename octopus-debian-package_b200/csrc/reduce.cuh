@@ -25,8 +25,9 @@ hpsi_status launch_cholesky_inverse(const double *S, int nst, double *U, double 
 template <typename T>
 hpsi_status launch_trsm_apply(T *psi, long long ld, int np, int nst, const double *Uinv, cudaStream_t st);
 
-// partial [ncta][ld][3][2] -> out[3][nst] = (energy, norm2, dipole) * dv
-hpsi_status launch_obs_finalize(const double *partial, int ncta, int ld, int nst, double dv, double *out,
-                                cudaStream_t st);
+// partial [ncta][ld][3][2] -> out[3][nst] = (energy, norm2, dipole) * dv;
+// ket_partial [nket][ld][2] (may be null) adds the KB part of the energy
+hpsi_status launch_obs_finalize(const double *partial, int ncta, int ld, int nst, double dv,
+                                const double *ket_partial, int nket, double *out, cudaStream_t st);
 
 }  // namespace hpsi

@@ -9,8 +9,9 @@
 // one x column and one real lane, and keeps 9 running sums per cell: when
 // plane p arrives it adds w_z(p - z) * psi(p) to the sums of outputs
 // z = p-4..p+4 and the x/y arms plus the centre (w_c + v) to output p.  The
-// sum of output p-4 is then complete and is written out after the KB ket
-// term and, for a Taylor pass, the Horner update psi0 + a * H u.
+// sum of output p-4 is then complete and is written out (for a Taylor pass
+// after the Horner update psi0 + a * H u).  The KB ket is added by the
+// separate row kernel in projector.cu.
 //
 // Reference semantics: X(nl_operator_operate_batch)
 // (src/grid/nl_operator_inc.F90:21-130) with weights op%w * (-1/2),
@@ -20,6 +21,7 @@
 // order than the reference's (rounding differences at the 1e-16 level).
 #include <algorithm>
 #include <cstdio>
+#include <type_traits>
 
 #include "stencil.cuh"
 
@@ -62,72 +64,106 @@ __device__ __forceinline__ void zero_n(void *d) {
     *reinterpret_cast<float *>(d) = 0.f;
 }
 
+// complex number of the storage type and its multiply-add by a real weight
+template <typename T>
+struct Cx;
+template <>
+struct Cx<double> {
+  using type = double2;
+};
+template <>
+struct Cx<float> {
+  using type = float2;
+};
+__device__ __forceinline__ double2 cfma(double w, double2 x, double2 a) {
+  return make_double2(fma(w, x.x, a.x), fma(w, x.y, a.y));
+}
+__device__ __forceinline__ float2 cfma(float w, float2 x, float2 a) {
+  return __ffma2_rn(make_float2(w, w), x, a);  // packed FP32 FMA (sm_100)
+}
+template <typename T>
+__device__ __forceinline__ const T *wsel(const double *d, const float *f);
+template <>
+__device__ __forceinline__ const double *wsel<double>(const double *d, const float *) {
+  return d;
+}
+template <>
+__device__ __forceinline__ const float *wsel<float>(const double *, const float *f) {
+  return f;
+}
+template <typename C2>
+__device__ __forceinline__ C2 czero() {
+  C2 z;
+  z.x = 0;
+  z.y = 0;
+  return z;
+}
+
 template <typename T, int SC, int TX, int TY, int RY, int NBUF>
 struct PassLayout {
-  static constexpr int L = 2 * SC;
+  using C2 = typename Cx<T>::type;
   static constexpr int HAL = 4;
   static constexpr int HX = TX + 2 * HAL, HY = TY + 2 * HAL;
-  static constexpr int NT = L * TX * (TY / RY);
-  static constexpr int PLANE = HY * HX * L;  // T elements of one halo plane
-  static constexpr int INNER = TY * TX * L;  // T elements of one interior plane
-  static constexpr int RING = 8;             // row ring (>= NBUF + 4)
-  static constexpr int MAPS = 4;             // map ring (>= NBUF + 1)
+  static constexpr int NT = SC * TX * (TY / RY);
+  static constexpr int PLANE = HY * HX * SC;  // complex numbers of one halo plane
+  static constexpr int INNER = TY * TX * SC;  // complex numbers of one interior plane
+  static constexpr int RING = 8;              // row ring (>= NBUF + 4)
+  static constexpr int MAPS = 4;              // map ring (>= NBUF + 1)
   // byte offsets of the shared-memory regions
   static constexpr size_t off_planes = 0;
-  static constexpr size_t off_psi0 = off_planes + size_t(NBUF) * PLANE * sizeof(T);
-  static constexpr size_t off_v = off_psi0 + size_t(NBUF) * INNER * sizeof(T);
+  static constexpr size_t off_psi0 = off_planes + size_t(NBUF) * PLANE * sizeof(C2);
+  static constexpr size_t off_v = off_psi0 + size_t(NBUF) * INNER * sizeof(C2);
   static constexpr size_t off_rows = off_v + size_t(NBUF) * TY * TX * sizeof(double);
   static constexpr size_t off_maps = off_rows + size_t(RING) * TY * TX * sizeof(int);
   static constexpr size_t bytes = off_maps + size_t(MAPS) * HY * HX * sizeof(int);
 };
 
+// Each thread owns one complex state (re and im together) of RY consecutive
+// y cells of one x column; a warp reads whole contiguous cell chunks.
 template <typename T, int SC, int TX, int TY, int RY, int NBUF>
-__global__ void __launch_bounds__(2 * SC * TX * (TY / RY), 1)
+__global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
     pass_kernel(const PassArgs p) {
   using LY = PassLayout<T, SC, TX, TY, RY, NBUF>;
-  constexpr int L = LY::L, HAL = LY::HAL, HX = LY::HX, HY = LY::HY, NT = LY::NT;
+  using C2 = typename LY::C2;
+  constexpr int HAL = LY::HAL, HX = LY::HX, HY = LY::HY, NT = LY::NT;
   constexpr int PLANE = LY::PLANE, INNER = LY::INNER, RING = LY::RING, MAPS = LY::MAPS;
-  constexpr int CELLB = L * int(sizeof(T));     // bytes per cell chunk
+  constexpr int CELLB = SC * int(sizeof(C2));   // bytes per cell chunk
   constexpr int COPYB = CELLB >= 16 ? 16 : CELLB;
   constexpr int CPC = CELLB / COPYB;            // copies per cell
-  constexpr int COPYE = COPYB / int(sizeof(T)); // T elements per copy
+  constexpr int COPYC = COPYB / int(sizeof(T)); // T elements per copy
   static_assert(NBUF + 4 <= RING && NBUF + 1 <= MAPS, "ring too small");
-  static_assert((HX * 4) % 16 == 0 && (TX * 4) % 16 == 0, "tile rows must be 16-byte multiples");
 
   extern __shared__ __align__(16) unsigned char smem[];
-  T *planes = reinterpret_cast<T *>(smem + LY::off_planes);
-  T *psi0ring = reinterpret_cast<T *>(smem + LY::off_psi0);
+  C2 *planes = reinterpret_cast<C2 *>(smem + LY::off_planes);
+  C2 *psi0ring = reinterpret_cast<C2 *>(smem + LY::off_psi0);
   double *vring = reinterpret_cast<double *>(smem + LY::off_v);
   int *rowring = reinterpret_cast<int *>(smem + LY::off_rows);
   int *mapring = reinterpret_cast<int *>(smem + LY::off_maps);
 
   const int tid = threadIdx.x;
-  const int lane = tid % L;
-  const int tx = (tid / L) % TX;
-  const int tyg = tid / (L * TX);
-  // chunks of the same tile are adjacent in launch order, so they run
-  // together and share each row's DRAM lines, the cell maps and v in L2
+  const int cs = tid % SC;              // complex state within the chunk
+  const int tx = (tid / SC) % TX;
+  const int tyg = tid / (SC * TX);
+  // one work item = one tile column over a z range that holds inner points;
+  // the chunks of an item are adjacent in launch order, so they run together
+  // and share each row's DRAM lines, the cell maps and v in L2
   const int chunk = blockIdx.x % p.chunks;
-  const int rest = blockIdx.x / p.chunks;
-  const int ntiles = p.tiles_x * p.tiles_y;
-  const int tile = rest % ntiles, zblk = rest / ntiles;
-  const int bx = tile % p.tiles_x, by = tile / p.tiles_x;
+  const int item = blockIdx.x / p.chunks;
+  const int4 it = p.items[item];
   const CellBox &B = p.box;
-  const int cx0 = HAL + bx * TX, cy0 = HAL + by * TY;
-  const int zs = HAL + zblk * p.zb;
-  const int ze = min(zs + p.zb, HAL + B.nzo);
+  const int cx0 = HAL + it.x * TX, cy0 = HAL + it.y * TY;
+  const int zs = it.z, ze = it.w;
   const long long planeN = (long long)B.NX * B.NY;
   const int zbeg = zs - HAL, zend = ze + HAL;  // planes [zbeg, zend)
 
   const T *in = static_cast<const T *>(p.in);
   const long long in_ld2 = 2 * p.in_ld;
-  const int s_off = chunk * L;
+  const int s_off = chunk * SC * 2;  // T offset of this chunk within a row
   const T *psi0 = static_cast<const T *>(p.psi0);
   const long long psi0_ld2 = 2 * p.psi0_ld;
   const bool need_x0 = psi0 != nullptr;
 
   // ---- asynchronous loaders -------------------------------------------------
-  // halo-plane cell map of plane q (HY rows of HX ints, 16-byte pieces)
   auto load_map = [&](int q) {
     int *dst = mapring + (q & (MAPS - 1)) * HY * HX;
     const int *src = p.cell_src + q * planeN + (long long)(cy0 - HAL) * B.NX + (cx0 - HAL);
@@ -137,29 +173,28 @@ __global__ void __launch_bounds__(2 * SC * TX * (TY / RY), 1)
       cp_async16(dst + hy * HX + part * 4, src + (long long)hy * B.NX + part * 4);
     }
   };
-  // gathered halo plane q (map already resident), interior v and rows of q,
-  // and the pointwise psi0 values of the plane q - 4 emitted later
   auto load_plane = [&](int q) {
     const int buf = q % NBUF;
-    T *dst = planes + buf * PLANE;
+    T *dst = reinterpret_cast<T *>(planes + buf * PLANE);
     const int *map = mapring + (q & (MAPS - 1)) * HY * HX;
-    for (int i = tid; i < HY * HX * CPC; i += NT) {
-      const int cell = i / CPC, part = i - cell * CPC;
+    // thread t always copies piece t % CPC of its cells (coalesced: the CPC
+    // pieces of a cell chunk are adjacent threads)
+    for (int cell = tid / CPC, part = tid % CPC; cell < HY * HX; cell += NT / CPC) {
       const int src = map[cell];
-      T *d = dst + cell * L + part * COPYE;
+      T *d = dst + cell * SC * 2 + part * COPYC;
       if (src >= 0) {
-        cp_async_n<COPYB>(d, in + src * in_ld2 + s_off + part * COPYE);
+        cp_async_n<COPYB>(d, in + src * in_ld2 + s_off + part * COPYC);
       } else if (src == -1) {
         zero_n<COPYB>(d);
       } else {
         // periodic image times the Bloch phase correction
         const int b = -(src + 2);
         const int irow = __ldg(p.per_inner + b);
-        const T *g = in + irow * in_ld2 + s_off + part * COPYE;
+        const T *g = in + irow * in_ld2 + s_off + part * COPYC;
         const T pr = static_cast<const T *>(p.phase_corr)[2 * b];
         const T pi = static_cast<const T *>(p.phase_corr)[2 * b + 1];
 #pragma unroll
-        for (int e = 0; e < COPYE; e += 2) {
+        for (int e = 0; e < COPYC; e += 2) {
           const T xr = g[e], xi = g[e + 1];
           d[e] = xr * pr - xi * pi;
           d[e + 1] = xr * pi + xi * pr;
@@ -183,36 +218,31 @@ __global__ void __launch_bounds__(2 * SC * TX * (TY / RY), 1)
     const int qo = q - HAL;
     if (need_x0 && qo >= zs) {
       const int *ro = rowring + (qo & (RING - 1)) * TY * TX;
-      T *x0d = psi0ring + buf * INNER;
-      for (int i = tid; i < TY * TX * CPC; i += NT) {
-        const int cell = i / CPC, part = i - cell * CPC;
-        const int row = ro[cell];
-        T *d = x0d + cell * L + part * COPYE;
-        if (row >= 0 && row < p.np)
-          cp_async_n<COPYB>(d, psi0 + row * psi0_ld2 + s_off + part * COPYE);
+      T *x0d = reinterpret_cast<T *>(psi0ring + buf * INNER);
+      for (int cell = tid / CPC, part = tid % CPC; cell < TY * TX; cell += NT / CPC) {
+        const int rv = ro[cell];
+        const int row = rv & 0x3fffffff;  // bit 30 flags rows with KB entries
+        if (rv >= 0 && row < p.np)
+          cp_async_n<COPYB>(x0d + cell * SC * 2 + part * COPYC, psi0 + row * psi0_ld2 + s_off + part * COPYC);
       }
     }
   };
 
   // ---- weights and field ---------------------------------------------------
-  T w_x[9], w_y[9], w_z[9];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    w_x[k] = static_cast<T>(p.wx[k]);
-    w_y[k] = static_cast<T>(p.wy[k]);
-    w_z[k] = static_cast<T>(p.wz[k]);
-  }
-  double fscale = p.fld_scale_dev ? *p.fld_scale_dev : 1.0;
+  // weights are read straight from the kernel parameters (constant bank),
+  // so they cost no registers
+  const T *w_x = wsel<T>(p.wx, p.wxf), *w_y = wsel<T>(p.wy, p.wyf), *w_z = wsel<T>(p.wz, p.wzf);
+  const double fscale = p.fld_scale_dev ? *p.fld_scale_dev : 1.0;
   const double fx = p.fld[0] * fscale * B.h[0], fy = p.fld[1] * fscale * B.h[1],
                fz = p.fld[2] * fscale * B.h[2];
   const bool obs_on = p.obs != nullptr;
   const double px = p.obs_pol[0] * B.h[0], py = p.obs_pol[1] * B.h[1], pzc = p.obs_pol[2] * B.h[2];
 
-  T acc[RY][9];
+  C2 acc[RY][9];
 #pragma unroll
   for (int r = 0; r < RY; ++r)
 #pragma unroll
-    for (int k = 0; k < 9; ++k) acc[r][k] = T(0);
+    for (int k = 0; k < 9; ++k) acc[r][k] = czero<C2>();
 
   Kahan ke = {0, 0}, kn = {0, 0}, kd = {0, 0};
 
@@ -237,12 +267,14 @@ __global__ void __launch_bounds__(2 * SC * TX * (TY / RY), 1)
     cp_async_commit();
   }
 
-  T *out = static_cast<T *>(p.out);
-  const long long out_ld2 = 2 * p.out_ld;
-  const T *kb_pt = static_cast<const T *>(p.kb_pt);
-  const T *projv = static_cast<const T *>(p.proj);
-  const long long proj_ld2 = 2 * p.proj_ld;
+  C2 *out = static_cast<C2 *>(p.out);
+  const long long out_ldc = p.out_ld;
+  const double xr = double(cx0 + tx + B.lo[0]);
+  const int cidx = chunk * SC + cs;  // complex column of this thread in a row
+  const T are = static_cast<T>(p.a_re), aim = static_cast<T>(p.a_im);
+  const bool horner = p.mode == PASS_HORNER;
 
+  int ring = 0;
 #pragma unroll 1
   for (int pz = zbeg; pz < zend; ++pz) {
     cp_async_wait<NBUF - 2>();
@@ -254,86 +286,96 @@ __global__ void __launch_bounds__(2 * SC * TX * (TY / RY), 1)
       cp_async_commit();
     }
     const int buf = pz % NBUF;
-    const T *P = planes + buf * PLANE;
+    const C2 *P = planes + buf * PLANE;
     const double *vd = vring + buf * TY * TX;
-
-    // y window of this thread's column
-    T col[RY + 8];
-#pragma unroll
-    for (int i = 0; i < RY + 8; ++i) col[i] = P[((tyg * RY + i) * HX + tx + HAL) * L + lane];
-
-    const double xr = double(cx0 + tx + B.lo[0]);
     const double zr = double(pz + B.lo[2]);
+
+    // Slot (j + K) % 9 of acc holds the running sum of output plane pz - 4 + j
+    // with K = (pz - zbeg) % 9, so the ring never moves; the slot of the
+    // completed output pz - 4 is handed to the epilogue and cleared.
+    C2 done[RY];
+    auto compute = [&](auto Kc) {
+      constexpr int K = decltype(Kc)::value;
+      // y arms, streamed down the column: value i feeds row r with weight
+      // w_y[i - r]; the centre (i - r == 4) carries w_c + v and the z arms
+      C2 xy[RY];
 #pragma unroll
-    for (int r = 0; r < RY; ++r) {
-      const T c = col[r + 4];
+      for (int r = 0; r < RY; ++r) xy[r] = czero<C2>();
 #pragma unroll
-      for (int k = 0; k < 9; ++k)
-        if (k != 4) acc[r][k] += w_z[8 - k] * c;
-      T s = acc[r][4];
+      for (int i = 0; i < RY + 8; ++i) {
+        const C2 val = P[((tyg * RY + i) * HX + tx + HAL) * SC + cs];
 #pragma unroll
-      for (int d = -4; d <= 4; ++d)
-        if (d != 0) s += w_y[d + 4] * col[r + 4 + d];
-      const T *rp = P + ((tyg * RY + r + HAL) * HX + tx + HAL) * L + lane;
+        for (int r = 0; r < RY; ++r) {
+          const int d = i - r;  // 0..8, offset d - 4
+          if (d < 0 || d > 8) continue;
+          if (d != 4) {
+            xy[r] = cfma(w_y[d], val, xy[r]);
+          } else {
+            const int ty = tyg * RY + r;
+            const double yr = double(cy0 + ty + B.lo[1]);
+            const double vv = vd[ty * TX + tx] + fx * xr + fy * yr + fz * zr;
+            xy[r] = cfma(w_x[4] + static_cast<T>(vv), val, xy[r]);
 #pragma unroll
-      for (int d = -4; d <= 4; ++d)
-        if (d != 0) s += w_x[d + 4] * rp[d * L];
-      const int ty = tyg * RY + r;
-      const double yr = double(cy0 + ty + B.lo[1]);
-      const double vv = vd[ty * TX + tx] + fx * xr + fy * yr + fz * zr;
-      s += (w_x[4] + static_cast<T>(vv)) * c;
-      acc[r][4] = s;
+            for (int j = 0; j < 9; ++j)
+              if (j != 4) acc[r][(j + K) % 9] = cfma(w_z[8 - j], val, acc[r][(j + K) % 9]);
+          }
+        }
+      }
+      // x arms
+#pragma unroll
+      for (int r = 0; r < RY; ++r) {
+        const C2 *rp = P + ((tyg * RY + r + HAL) * HX + tx + HAL) * SC + cs;
+#pragma unroll
+        for (int d = -4; d <= 4; ++d)
+          if (d != 0) xy[r] = cfma(w_x[d + 4], rp[d * SC], xy[r]);
+        acc[r][(4 + K) % 9].x += xy[r].x;
+        acc[r][(4 + K) % 9].y += xy[r].y;
+        done[r] = acc[r][K];
+        acc[r][K] = czero<C2>();
+      }
+    };
+    switch (ring) {
+      case 0: compute(std::integral_constant<int, 0>{}); break;
+      case 1: compute(std::integral_constant<int, 1>{}); break;
+      case 2: compute(std::integral_constant<int, 2>{}); break;
+      case 3: compute(std::integral_constant<int, 3>{}); break;
+      case 4: compute(std::integral_constant<int, 4>{}); break;
+      case 5: compute(std::integral_constant<int, 5>{}); break;
+      case 6: compute(std::integral_constant<int, 6>{}); break;
+      case 7: compute(std::integral_constant<int, 7>{}); break;
+      default: compute(std::integral_constant<int, 8>{}); break;
     }
+    ring = ring == 8 ? 0 : ring + 1;
 
     // ---- epilogue: outputs of plane zo = pz - 4 are complete ---------------
     const int zo = pz - HAL;
     if (zo >= zs) {
       const int *ro = rowring + (zo & (RING - 1)) * TY * TX;
-      const T *x0s = psi0ring + buf * INNER;
+      const C2 *x0s = psi0ring + buf * INNER;
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
         const int ty = tyg * RY + r;
         const int rowv = ro[ty * TX + tx];
-        const int row = (rowv >= 0 && rowv < p.np) ? rowv : -1;
-        T h = acc[r][0];
-        if (row >= 0 && p.kb_ptr) {
-          const int e0 = __ldg(p.kb_ptr + row), e1 = __ldg(p.kb_ptr + row + 1);
-          for (int e = e0; e < e1; ++e) {
-            const int4 E = __ldg(p.kb_ent + e);
-            const T *pt = kb_pt + E.x;
-            const T *pr = projv + (long long)E.y * proj_ld2 + s_off + lane;
-            for (int j = 0; j < E.z; ++j) h += pt[j] * pr[j * proj_ld2];
-          }
-        }
-        const T partner = __shfl_xor_sync(0xffffffffu, h, 1);
-        const T x0 = need_x0 ? x0s[(ty * TX + tx) * L + lane] : T(0);
-        if (obs_on && row >= 0) {
-          const double xd = double(x0);
-          const double rr = px * xr + py * double(cy0 + ty + B.lo[1]) + pzc * double(zo + B.lo[2]);
-          kadd(ke, xd * double(h));
-          kadd(kn, xd * xd);
-          kadd(kd, xd * xd * rr);
-        }
+        const int rr0 = rowv & 0x3fffffff;
+        const int row = (rowv >= 0 && rr0 < p.np) ? rr0 : -1;
+        const C2 h = done[r];
         if (row >= 0) {
-          T val;
-          if (p.mode == PASS_HORNER) {
-            const T are = static_cast<T>(p.a_re), aim = static_cast<T>(p.a_im);
-            if ((lane & 1) == 0)
-              val = x0 + are * h - aim * partner;  // real part
-            else
-              val = x0 + are * h + aim * partner;  // imaginary part
-          } else {
-            val = h;
+          const C2 x0 = need_x0 ? x0s[(ty * TX + tx) * SC + cs] : czero<C2>();
+          if (obs_on) {
+            const double rr = px * xr + py * double(cy0 + ty + B.lo[1]) + pzc * double(zo + B.lo[2]);
+            const double n2 = double(x0.x) * double(x0.x) + double(x0.y) * double(x0.y);
+            kadd(ke, double(x0.x) * double(h.x) + double(x0.y) * double(h.y));
+            kadd(kn, n2);
+            kadd(kd, n2 * rr);
           }
-          out[row * out_ld2 + s_off + lane] = val;
+          C2 val = h;
+          if (horner) {
+            val.x = x0.x + are * h.x - aim * h.y;
+            val.y = x0.y + are * h.y + aim * h.x;
+          }
+          out[row * out_ldc + cidx] = val;
         }
       }
-    }
-#pragma unroll
-    for (int r = 0; r < RY; ++r) {
-#pragma unroll
-      for (int k = 0; k < 8; ++k) acc[r][k] = acc[r][k + 1];
-      acc[r][8] = T(0);
     }
   }
   cp_async_wait<0>();
@@ -349,19 +391,15 @@ __global__ void __launch_bounds__(2 * SC * TX * (TY / RY), 1)
     red[tid * 6 + 5] = kd.c;
     __syncthreads();
     if (tid < SC) {
-      const int s = tid;
       Kahan a[3] = {{0, 0}, {0, 0}, {0, 0}};
-      for (int t = 0; t < NT; ++t) {
-        const int ln = t % L;
-        if ((ln >> 1) != s) continue;
+      for (int t = tid; t < NT; t += SC) {
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
           kadd(a[q], red[t * 6 + 2 * q]);
           a[q].c += red[t * 6 + 2 * q + 1];
         }
       }
-      const int cta = tile + ntiles * zblk;
-      double *o = p.obs + ((long long)cta * p.obs_ld + chunk * SC + s) * 6;
+      double *o = p.obs + ((long long)item * p.obs_ld + chunk * SC + tid) * 6;
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         o[2 * q] = a[q].s;
@@ -383,7 +421,7 @@ hpsi_status launch_variant(const PassArgs &a, cudaStream_t st) {
     HPSI_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
     attr_set = true;
   }
-  const unsigned nblocks = unsigned(a.tiles_x) * a.tiles_y * a.zblocks * a.chunks;
+  const unsigned nblocks = unsigned(a.nitems) * a.chunks;
   kern<<<nblocks, LY::NT, bytes, st>>>(a);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
@@ -391,41 +429,27 @@ hpsi_status launch_variant(const PassArgs &a, cudaStream_t st) {
 
 }  // namespace
 
-void pass_geometry(PassArgs &a, const PassShape &s, int ld, int num_sms) {
-  const CellBox &B = a.box;
-  a.tiles_x = (B.nxo + s.tx - 1) / s.tx;
-  a.tiles_y = (B.nyo + s.ty - 1) / s.ty;
-  a.chunks = ld / s.sc;
-  // z blocks: enough CTAs for ~4 waves while keeping the z halo overhead small
-  const long long base = (long long)a.tiles_x * a.tiles_y * a.chunks;
-  int zb = B.nzo;
-  const long long want = 4LL * num_sms;
-  while (zb > 16 && base * ((B.nzo + zb - 1) / zb) < want) zb = (zb + 1) / 2;
-  a.zb = zb;
-  a.zblocks = (B.nzo + zb - 1) / zb;
-}
-
-template <typename T, int TX, int TY, int RY>
-hpsi_status launch_sc(const PassArgs &a, int sc, cudaStream_t st) {
-  switch (sc) {
-    case 1:
-      return launch_variant<T, 1, TX, TY, RY>(a, st);
-    case 2:
-      return launch_variant<T, 2, TX, TY, RY>(a, st);
-    case 4:
-      return launch_variant<T, 4, TX, TY, RY>(a, st);
-    case 8:
-      if constexpr (sizeof(T) == 4) return launch_variant<T, 8, TX, TY, RY>(a, st);
-      break;
-  }
-  set_error("launch_pass: no kernel variant for this state chunk");
-  return HPSI_ERR_UNSUPPORTED;
-}
-
+// Instantiated variants (tile 16 x 16 cells): FP64 threads keep RY = 2 rows of
+// 9 complex running sums, FP32 threads RY = 4.
 template <typename T>
 hpsi_status launch_pass(PassArgs a, const PassShape &s, cudaStream_t st) {
-  if (s.tx == 16 && s.ty == 16 && s.ry == 4) return launch_sc<T, 16, 16, 4>(a, s.sc, st);
-  if (s.tx == 16 && s.ty == 16 && s.ry == 8) return launch_sc<T, 16, 16, 8>(a, s.sc, st);
+  if (a.nitems == 0) return HPSI_OK;
+  if (s.tx == 16 && s.ty == 16) {
+    if constexpr (sizeof(T) == 8) {
+      if (s.ry == 2) {
+        if (s.sc == 4) return launch_variant<T, 4, 16, 16, 2>(a, st);
+        if (s.sc == 2) return launch_variant<T, 2, 16, 16, 2>(a, st);
+        if (s.sc == 1) return launch_variant<T, 1, 16, 16, 2>(a, st);
+      }
+    } else {
+      if (s.ry == 4) {
+        if (s.sc == 8) return launch_variant<T, 8, 16, 16, 4>(a, st);
+        if (s.sc == 4) return launch_variant<T, 4, 16, 16, 4>(a, st);
+        if (s.sc == 2) return launch_variant<T, 2, 16, 16, 4>(a, st);
+        if (s.sc == 1) return launch_variant<T, 1, 16, 16, 4>(a, st);
+      }
+    }
+  }
   set_error("launch_pass: no kernel variant for this shape");
   return HPSI_ERR_UNSUPPORTED;
 }

@@ -32,25 +32,20 @@ struct PassArgs {
   // per-axis weights, index d+4 for offset d; wx[4] holds the whole centre
   // weight, wy[4] = wz[4] = 0
   double wx[9], wy[9], wz[9];
+  float wxf[9], wyf[9], wzf[9];  // the same weights rounded to FP32
   const double *v_cell;   // local potential in cell layout, or null
   double fld[3];          // laser: v += (fld . r), r = (cell + lo) * h
   const double *fld_scale_dev;  // optional device scalar multiplying fld
-
-  // KB ket folded into the epilogue
-  const int *kb_ptr;      // np + 1
-  const int4 *kb_ent;     // {offset of the point's projector row, projection row, nproj, 0}
-  const void *kb_pt;      // projector values, projector index fastest per point
-  const void *proj;       // projections, complex [nprojections][proj_ld]
-  long long proj_ld;
 
   // per-state observables of `in`: energy, norm, dipole partials
   double *obs;            // [ncta_xyz][obs_ld][3][2] (Kahan sum, compensation)
   int obs_ld;
   double obs_pol[3];      // dipole direction
 
-  int zb;                 // output planes per CTA
-  int tiles_x, tiles_y, zblocks, chunks;
-  int *err_flag;          // device error word (index checks), may be null
+  const int4 *items;      // work items {tile x, tile y, first plane, end plane}
+  int nitems;
+  int chunks;             // state chunks per item (ld / SC)
+  int zb;                 // output planes per item (at most)
 };
 
 // Kernel variant chosen for a pass.
@@ -63,10 +58,7 @@ struct PassShape {
 template <typename T>
 hpsi_status launch_pass(PassArgs a, const PassShape &shape, cudaStream_t st);
 
-// Number of CTAs along (tile, zblock) for the observables partial buffer.
-inline int pass_ncta_xyz(const PassArgs &a) { return a.tiles_x * a.tiles_y * a.zblocks; }
-
-// Choose tiles/zblocks for a shape on a box (host helper).
-void pass_geometry(PassArgs &a, const PassShape &s, int ld, int num_sms);
+// Tile edge (cells) of every pass kernel variant.
+constexpr int PASS_TILE = 16;
 
 }  // namespace hpsi
