@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -185,7 +186,19 @@ int pass_sc(int dtype, long long ld) {
 PassShape default_shape(int dtype, long long ld) {
   const int sc = pass_sc(dtype, ld);
   // a thread keeps RY rows of 9 complex running sums: FP64 2 rows, FP32 4
-  return dtype == HPSI_C128 ? PassShape{sc, 16, 16, 2} : PassShape{sc, 16, 16, 4};
+  PassShape s = dtype == HPSI_C128 ? PassShape{sc, 16, 16, 2} : PassShape{sc, 16, 16, 4};
+  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb"
+  const char *env = std::getenv(dtype == HPSI_C128 ? "HPSI_PASS_SHAPE64" : "HPSI_PASS_SHAPE32");
+  if (env) {
+    int a = 0, b = 0, c = 0, u = 0;
+    if (std::sscanf(env, "%d,%d,%d,%d", &a, &b, &c, &u) >= 2 && ld % a == 0) {
+      s.sc = a;
+      s.ry = b;
+      s.zb = c;
+      s.unroll = u;
+    }
+  }
+  return s;
 }
 
 }  // namespace hpsi
@@ -791,7 +804,7 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
   }
   const PassShape shape = default_shape(sizeof(T) == 8 ? HPSI_C128 : HPSI_C64, ld);
   a.chunks = int(ld / shape.sc);
-  a.zb = choose_zb(h->mesh, a.chunks);
+  a.zb = shape.zb > 0 ? shape.zb : choose_zb(h->mesh, a.chunks);
   hpsi_status si = mesh_items(h->mesh, a.zb, &a.items, &a.nitems);
   if (si) return si;
   if (obs_partial) {
@@ -833,7 +846,8 @@ size_t obs_partial_bytes(hpsi_hamiltonian *h, long long ld) {
     const PassShape sh = default_shape(dt, ld);
     const int4 *items;
     int nitems = 0;
-    if (mesh_items(h->mesh, choose_zb(h->mesh, int(ld / sh.sc)), &items, &nitems) == HPSI_OK)
+    const int zb = sh.zb > 0 ? sh.zb : choose_zb(h->mesh, int(ld / sh.sc));
+    if (mesh_items(h->mesh, zb, &items, &nitems) == HPSI_OK)
       n = std::max(n, size_t(nitems));
   }
   return std::max<size_t>(n, 1) * ld * 6 * sizeof(double);

@@ -99,39 +99,45 @@ __device__ __forceinline__ C2 czero() {
   return z;
 }
 
-template <typename T, int SC, int TX, int TY, int RY, int NBUF>
+template <typename T, int SC, int TX, int TY, int RY>
 struct PassLayout {
   using C2 = typename Cx<T>::type;
   static constexpr int HAL = 4;
+  static constexpr int NBUF = 3;             // data ring; 3 divides the 9-plane unroll
+  static constexpr int RING = 9;             // row ring (rows live from load to emission)
   static constexpr int HX = TX + 2 * HAL, HY = TY + 2 * HAL;
   static constexpr int NT = SC * TX * (TY / RY);
   static constexpr int PLANE = HY * HX * SC;  // complex numbers of one halo plane
   static constexpr int INNER = TY * TX * SC;  // complex numbers of one interior plane
-  static constexpr int RING = 8;              // row ring (>= NBUF + 4)
-  static constexpr int MAPS = 4;              // map ring (>= NBUF + 1)
-  // byte offsets of the shared-memory regions
   static constexpr size_t off_planes = 0;
   static constexpr size_t off_psi0 = off_planes + size_t(NBUF) * PLANE * sizeof(C2);
   static constexpr size_t off_v = off_psi0 + size_t(NBUF) * INNER * sizeof(C2);
   static constexpr size_t off_rows = off_v + size_t(NBUF) * TY * TX * sizeof(double);
   static constexpr size_t off_maps = off_rows + size_t(RING) * TY * TX * sizeof(int);
-  static constexpr size_t bytes = off_maps + size_t(MAPS) * HY * HX * sizeof(int);
+  static constexpr size_t bytes = off_maps + size_t(NBUF) * HY * HX * sizeof(int);
 };
 
 // Each thread owns one complex state (re and im together) of RY consecutive
-// y cells of one x column; a warp reads whole contiguous cell chunks.
-template <typename T, int SC, int TX, int TY, int RY, int NBUF>
+// y cells of one x column.  The plane loop is unrolled nine times, so every
+// ring position (data, rows, maps, the 9 running sums) is a compile-time
+// constant.  HORNER: out = psi0 + a * H in; OBS: per-state observables of in.
+template <typename T, int SC, int TX, int TY, int RY, bool HORNER, bool OBS>
 __global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
     pass_kernel(const PassArgs p) {
-  using LY = PassLayout<T, SC, TX, TY, RY, NBUF>;
+  using LY = PassLayout<T, SC, TX, TY, RY>;
   using C2 = typename LY::C2;
-  constexpr int HAL = LY::HAL, HX = LY::HX, HY = LY::HY, NT = LY::NT;
-  constexpr int PLANE = LY::PLANE, INNER = LY::INNER, RING = LY::RING, MAPS = LY::MAPS;
+  constexpr int HAL = LY::HAL, HX = LY::HX, HY = LY::HY, NT = LY::NT, NBUF = LY::NBUF, RING = LY::RING;
+  constexpr int PLANE = LY::PLANE, INNER = LY::INNER;
   constexpr int CELLB = SC * int(sizeof(C2));   // bytes per cell chunk
   constexpr int COPYB = CELLB >= 16 ? 16 : CELLB;
   constexpr int CPC = CELLB / COPYB;            // copies per cell
   constexpr int COPYC = COPYB / int(sizeof(T)); // T elements per copy
-  static_assert(NBUF + 4 <= RING && NBUF + 1 <= MAPS, "ring too small");
+  static_assert(NT % CPC == 0, "copy pieces must tile the threads");
+  constexpr int CSTEP = NT / CPC;               // cells per copy round
+  constexpr int HROUNDS = (HY * HX) / CSTEP, HREM = (HY * HX) % CSTEP;
+  constexpr int IROUNDS = (TY * TX) / CSTEP, IREM = (TY * TX) % CSTEP;
+  constexpr int NV = TY * TX / 2, NR = TY * TX / 4, NM = HY * HX / 4;  // 16-byte copies
+  constexpr bool X0 = HORNER || OBS;
 
   extern __shared__ __align__(16) unsigned char smem[];
   C2 *planes = reinterpret_cast<C2 *>(smem + LY::off_planes);
@@ -141,12 +147,11 @@ __global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
   int *mapring = reinterpret_cast<int *>(smem + LY::off_maps);
 
   const int tid = threadIdx.x;
-  const int cs = tid % SC;              // complex state within the chunk
+  const int cs = tid % SC;  // complex state within the chunk
   const int tx = (tid / SC) % TX;
   const int tyg = tid / (SC * TX);
-  // one work item = one tile column over a z range that holds inner points;
-  // the chunks of an item are adjacent in launch order, so they run together
-  // and share each row's DRAM lines, the cell maps and v in L2
+  // the chunks of a work item are adjacent in launch order, so they run
+  // together and share each row's DRAM lines, the cell maps and v in L2
   const int chunk = blockIdx.x % p.chunks;
   const int item = blockIdx.x / p.chunks;
   const int4 it = p.items[item];
@@ -156,87 +161,117 @@ __global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
   const long long planeN = (long long)B.NX * B.NY;
   const int zbeg = zs - HAL, zend = ze + HAL;  // planes [zbeg, zend)
 
-  const T *in = static_cast<const T *>(p.in);
+  // per-thread copy roles (fixed for the whole kernel)
+  const int cell0 = tid / CPC, part = tid % CPC;
+  const T *in_base = static_cast<const T *>(p.in) + chunk * SC * 2 + part * COPYC;
   const long long in_ld2 = 2 * p.in_ld;
-  const int s_off = chunk * SC * 2;  // T offset of this chunk within a row
-  const T *psi0 = static_cast<const T *>(p.psi0);
+  const T *psi0_base = static_cast<const T *>(p.psi0) + chunk * SC * 2 + part * COPYC;
   const long long psi0_ld2 = 2 * p.psi0_ld;
-  const bool need_x0 = psi0 != nullptr;
-
-  // ---- asynchronous loaders -------------------------------------------------
-  auto load_map = [&](int q) {
-    int *dst = mapring + (q & (MAPS - 1)) * HY * HX;
-    const int *src = p.cell_src + q * planeN + (long long)(cy0 - HAL) * B.NX + (cx0 - HAL);
-    constexpr int PER_ROW = HX / 4;
-    for (int i = tid; i < HY * PER_ROW; i += NT) {
-      const int hy = i / PER_ROW, part = i - hy * PER_ROW;
-      cp_async16(dst + hy * HX + part * 4, src + (long long)hy * B.NX + part * 4);
-    }
-  };
-  auto load_plane = [&](int q) {
-    const int buf = q % NBUF;
-    T *dst = reinterpret_cast<T *>(planes + buf * PLANE);
-    const int *map = mapring + (q & (MAPS - 1)) * HY * HX;
-    // thread t always copies piece t % CPC of its cells (coalesced: the CPC
-    // pieces of a cell chunk are adjacent threads)
-    for (int cell = tid / CPC, part = tid % CPC; cell < HY * HX; cell += NT / CPC) {
-      const int src = map[cell];
-      T *d = dst + cell * SC * 2 + part * COPYC;
-      if (src >= 0) {
-        cp_async_n<COPYB>(d, in + src * in_ld2 + s_off + part * COPYC);
-      } else if (src == -1) {
-        zero_n<COPYB>(d);
-      } else {
-        // periodic image times the Bloch phase correction
-        const int b = -(src + 2);
-        const int irow = __ldg(p.per_inner + b);
-        const T *g = in + irow * in_ld2 + s_off + part * COPYC;
-        const T pr = static_cast<const T *>(p.phase_corr)[2 * b];
-        const T pi = static_cast<const T *>(p.phase_corr)[2 * b + 1];
+  // side copies (16-byte pieces): v (NV), rows (NR), maps (NM); a thread does
+  // pieces tid, tid + NT, ... (one round when NT >= NV + NR + NM)
+  constexpr int NSIDE = NV + NR + NM;
+  constexpr int SROUNDS = (NSIDE + NT - 1) / NT;
+  const long long tile0 = (long long)cy0 * B.NX + cx0;
+  int side_dst[SROUNDS], side_kind[SROUNDS];
+  long long side_src[SROUNDS];
 #pragma unroll
-        for (int e = 0; e < COPYC; e += 2) {
-          const T xr = g[e], xi = g[e + 1];
-          d[e] = xr * pr - xi * pi;
-          d[e + 1] = xr * pi + xi * pr;
-        }
-      }
+  for (int k = 0; k < SROUNDS; ++k) {
+    const int i = tid + k * NT;
+    side_kind[k] = 0;
+    side_dst[k] = 0;
+    side_src[k] = 0;
+    if (i < NV) {
+      const int ty = i / (TX / 2), pc = i % (TX / 2);
+      side_kind[k] = 1;
+      side_dst[k] = ty * TX + pc * 2;
+      side_src[k] = tile0 + (long long)ty * B.NX + pc * 2;
+    } else if (i < NV + NR) {
+      const int j = i - NV, ty = j / (TX / 4), pc = j % (TX / 4);
+      side_kind[k] = 2;
+      side_dst[k] = ty * TX + pc * 4;
+      side_src[k] = tile0 + (long long)ty * B.NX + pc * 4;
+    } else if (i < NSIDE) {
+      const int j = i - NV - NR, hy = j / (HX / 4), pc = j % (HX / 4);
+      side_kind[k] = 3;
+      side_dst[k] = hy * HX + pc * 4;
+      side_src[k] = (long long)(cy0 - HAL + hy) * B.NX + (cx0 - HAL) + pc * 4;
     }
-    double *vd = vring + buf * TY * TX;
-    int *rd = rowring + (q & (RING - 1)) * TY * TX;
-    const long long base = q * planeN + (long long)cy0 * B.NX + cx0;
-    for (int i = tid; i < TY * (TX / 2); i += NT) {  // v: 2 doubles per copy
-      const int ty = i / (TX / 2), part = i - ty * (TX / 2);
-      if (p.v_cell)
-        cp_async16(vd + ty * TX + part * 2, p.v_cell + base + (long long)ty * B.NX + part * 2);
-      else
-        *reinterpret_cast<float4 *>(vd + ty * TX + part * 2) = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    for (int i = tid; i < TY * (TX / 4); i += NT) {  // rows: 4 ints per copy
-      const int ty = i / (TX / 4), part = i - ty * (TX / 4);
-      cp_async16(rd + ty * TX + part * 4, p.cell_row + base + (long long)ty * B.NX + part * 4);
-    }
-    const int qo = q - HAL;
-    if (need_x0 && qo >= zs) {
-      const int *ro = rowring + (qo & (RING - 1)) * TY * TX;
-      T *x0d = reinterpret_cast<T *>(psi0ring + buf * INNER);
-      for (int cell = tid / CPC, part = tid % CPC; cell < TY * TX; cell += NT / CPC) {
-        const int rv = ro[cell];
-        const int row = rv & 0x3fffffff;  // bit 30 flags rows with KB entries
-        if (rv >= 0 && row < p.np)
-          cp_async_n<COPYB>(x0d + cell * SC * 2 + part * COPYC, psi0 + row * psi0_ld2 + s_off + part * COPYC);
+  }
+
+  // gather one piece of a halo cell (src: load-map entry)
+  auto gather = [&](int src, T *d) {
+    if (src >= 0) {
+      cp_async_n<COPYB>(d, in_base + src * in_ld2);
+    } else if (src == -1) {
+      zero_n<COPYB>(d);
+    } else {
+      // periodic image times the Bloch phase correction
+      const int b = -(src + 2);
+      const int irow = __ldg(p.per_inner + b);
+      const T *g = in_base + irow * in_ld2;
+      const T pr = static_cast<const T *>(p.phase_corr)[2 * b];
+      const T pi = static_cast<const T *>(p.phase_corr)[2 * b + 1];
+#pragma unroll
+      for (int e = 0; e < COPYC; e += 2) {
+        const T xr = g[e], xi = g[e + 1];
+        d[e] = xr * pr - xi * pi;
+        d[e + 1] = xr * pi + xi * pr;
       }
     }
   };
+  // halo plane q (map in slot MS), v and rows of q, psi0 of plane q - 4
+  auto load_plane = [&](int q, int DB, int RS, int MS, int RS4) {
+    T *dst = reinterpret_cast<T *>(planes + DB * PLANE) + part * COPYC;
+    const int *map = mapring + MS * HY * HX;
+#pragma unroll
+    for (int k = 0; k < HROUNDS; ++k) {
+      const int cell = cell0 + k * CSTEP;
+      gather(map[cell], dst + cell * SC * 2);
+    }
+    if (HREM && cell0 < HREM) {
+      const int cell = cell0 + HROUNDS * CSTEP;
+      gather(map[cell], dst + cell * SC * 2);
+    }
+    const long long qoff = q * planeN;
+#pragma unroll
+    for (int k = 0; k < SROUNDS; ++k) {
+      if (side_kind[k] == 1) {
+        if (p.v_cell)
+          cp_async16(vring + DB * TY * TX + side_dst[k], p.v_cell + qoff + side_src[k]);
+        else
+          *reinterpret_cast<float4 *>(vring + DB * TY * TX + side_dst[k]) = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else if (side_kind[k] == 2) {
+        cp_async16(rowring + RS * TY * TX + side_dst[k], p.cell_row + qoff + side_src[k]);
+      }
+    }
+    if (X0 && q - HAL >= zs) {
+      const int *ro = rowring + RS4 * TY * TX;
+      T *x0d = reinterpret_cast<T *>(psi0ring + DB * INNER) + part * COPYC;
+#pragma unroll
+      for (int k = 0; k <= IROUNDS; ++k) {
+        const int cell = cell0 + k * CSTEP;
+        if (k == IROUNDS && !(IREM && cell0 < IREM)) break;
+        const int row = ro[cell];
+        if (row >= 0 && row < p.np) cp_async_n<COPYB>(x0d + cell * SC * 2, psi0_base + row * psi0_ld2);
+      }
+    }
+  };
+  auto load_map = [&](int q, int MS) {
+#pragma unroll
+    for (int k = 0; k < SROUNDS; ++k)
+      if (side_kind[k] == 3) cp_async16(mapring + MS * HY * HX + side_dst[k], p.cell_src + q * planeN + side_src[k]);
+  };
 
-  // ---- weights and field ---------------------------------------------------
-  // weights are read straight from the kernel parameters (constant bank),
-  // so they cost no registers
+  // ---- weights, field, observables -------------------------------------------
   const T *w_x = wsel<T>(p.wx, p.wxf), *w_y = wsel<T>(p.wy, p.wyf), *w_z = wsel<T>(p.wz, p.wzf);
   const double fscale = p.fld_scale_dev ? *p.fld_scale_dev : 1.0;
-  const double fx = p.fld[0] * fscale * B.h[0], fy = p.fld[1] * fscale * B.h[1],
-               fz = p.fld[2] * fscale * B.h[2];
-  const bool obs_on = p.obs != nullptr;
-  const double px = p.obs_pol[0] * B.h[0], py = p.obs_pol[1] * B.h[1], pzc = p.obs_pol[2] * B.h[2];
+  const double fz = p.fld[2] * fscale * B.h[2];
+  double fxy[RY];
+#pragma unroll
+  for (int r = 0; r < RY; ++r)
+    fxy[r] = fscale * (p.fld[0] * B.h[0] * double(cx0 + tx + B.lo[0]) +
+                       p.fld[1] * B.h[1] * double(cy0 + tyg * RY + r + B.lo[1]));
+  Kahan ke = {0, 0}, kn = {0, 0}, kd = {0, 0};
 
   C2 acc[RY][9];
 #pragma unroll
@@ -244,143 +279,131 @@ __global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
 #pragma unroll
     for (int k = 0; k < 9; ++k) acc[r][k] = czero<C2>();
 
-  Kahan ke = {0, 0}, kn = {0, 0}, kd = {0, 0};
-
-  // ---- prologue: maps of the first NBUF-1 planes synchronously, then the
-  // groups G(q) = {plane q, map of plane q+NBUF-1} for those planes
-#pragma unroll 1
-  for (int k = 0; k < NBUF - 1; ++k) {
-    const int q = zbeg + k;
-    if (q >= zend) break;
-    int *dst = mapring + (q & (MAPS - 1)) * HY * HX;
-    for (int i = tid; i < HY * HX; i += NT) {
-      const int hy = i / HX, hx = i - hy * HX;
-      dst[i] = __ldg(p.cell_src + q * planeN + (long long)(cy0 - HAL + hy) * B.NX + cx0 - HAL + hx);
-    }
+  // ---- prologue ---------------------------------------------------------------
+  // maps of planes zbeg, zbeg+1 synchronously (slots 0, 1), then the planes
+  // themselves with the maps of zbeg+2, zbeg+3 (slots 2, 0)
+  for (int i = tid; i < 2 * HY * HX; i += NT) {
+    const int k = i / (HY * HX), c = i - k * (HY * HX);
+    const int hy = c / HX, hx = c - hy * HX;
+    const int q = min(zbeg + k, zend - 1);
+    mapring[k * HY * HX + c] = __ldg(p.cell_src + q * planeN + (long long)(cy0 - HAL + hy) * B.NX + cx0 - HAL + hx);
   }
   __syncthreads();
-#pragma unroll 1
-  for (int k = 0; k < NBUF - 1; ++k) {
-    const int q = zbeg + k;
-    if (q < zend) load_plane(q);
-    if (q + NBUF - 1 < zend) load_map(q + NBUF - 1);
-    cp_async_commit();
-  }
+  load_plane(zbeg, 0, 0, 0, 0);
+  if (zbeg + 2 < zend) load_map(zbeg + 2, 2);
+  cp_async_commit();
+  __syncthreads();  // everyone has read map slot 0 before it is refilled
+  if (zbeg + 1 < zend) load_plane(zbeg + 1, 1, 1, 1, 0);
+  if (zbeg + 3 < zend) load_map(zbeg + 3, 0);
+  cp_async_commit();
 
   C2 *out = static_cast<C2 *>(p.out);
   const long long out_ldc = p.out_ld;
-  const double xr = double(cx0 + tx + B.lo[0]);
   const int cidx = chunk * SC + cs;  // complex column of this thread in a row
   const T are = static_cast<T>(p.a_re), aim = static_cast<T>(p.a_im);
-  const bool horner = p.mode == PASS_HORNER;
+  const double xr = double(cx0 + tx + B.lo[0]);
 
-  int ring = 0;
-#pragma unroll 1
-  for (int pz = zbeg; pz < zend; ++pz) {
-    cp_async_wait<NBUF - 2>();
+  // one plane; K = (pz - zbeg) % 9 makes every ring index static
+  auto plane = [&](auto Kc, int pz) {
+    constexpr int K = decltype(Kc)::value;
+    constexpr int DB = K % NBUF;                       // data / v / psi0 buffer of pz
+    cp_async_wait<1>();
     __syncthreads();
-    {
-      const int q = pz + NBUF - 1;
-      if (q < zend) load_plane(q);
-      if (q + NBUF - 1 < zend) load_map(q + NBUF - 1);
-      cp_async_commit();
-    }
-    const int buf = pz % NBUF;
-    const C2 *P = planes + buf * PLANE;
-    const double *vd = vring + buf * TY * TX;
-    const double zr = double(pz + B.lo[2]);
+    if (pz + 2 < zend) load_plane(pz + 2, (K + 2) % NBUF, (K + 2) % RING, (K + 2) % NBUF, (K + 7) % RING);
+    if (pz + 4 < zend) load_map(pz + 4, (K + 1) % NBUF);
+    cp_async_commit();
 
-    // Slot (j + K) % 9 of acc holds the running sum of output plane pz - 4 + j
-    // with K = (pz - zbeg) % 9, so the ring never moves; the slot of the
-    // completed output pz - 4 is handed to the epilogue and cleared.
-    C2 done[RY];
-    auto compute = [&](auto Kc) {
-      constexpr int K = decltype(Kc)::value;
-      // y arms, streamed down the column: value i feeds row r with weight
-      // w_y[i - r]; the centre (i - r == 4) carries w_c + v and the z arms
-      C2 xy[RY];
+    const C2 *P = planes + DB * PLANE;
+    const double *vd = vring + DB * TY * TX;
+    const double vz = fz * double(pz + B.lo[2]);
+
+    // y arms streamed down the column (value i feeds row r with w_y[i - r]),
+    // the centre carries w_c + v and the z arms; x arms after
+    C2 ya[RY], yb[RY], xa[RY], xb[RY];
 #pragma unroll
-      for (int r = 0; r < RY; ++r) xy[r] = czero<C2>();
+    for (int r = 0; r < RY; ++r) ya[r] = yb[r] = xa[r] = xb[r] = czero<C2>();
 #pragma unroll
-      for (int i = 0; i < RY + 8; ++i) {
-        const C2 val = P[((tyg * RY + i) * HX + tx + HAL) * SC + cs];
-#pragma unroll
-        for (int r = 0; r < RY; ++r) {
-          const int d = i - r;  // 0..8, offset d - 4
-          if (d < 0 || d > 8) continue;
-          if (d != 4) {
-            xy[r] = cfma(w_y[d], val, xy[r]);
-          } else {
-            const int ty = tyg * RY + r;
-            const double yr = double(cy0 + ty + B.lo[1]);
-            const double vv = vd[ty * TX + tx] + fx * xr + fy * yr + fz * zr;
-            xy[r] = cfma(w_x[4] + static_cast<T>(vv), val, xy[r]);
-#pragma unroll
-            for (int j = 0; j < 9; ++j)
-              if (j != 4) acc[r][(j + K) % 9] = cfma(w_z[8 - j], val, acc[r][(j + K) % 9]);
-          }
-        }
-      }
-      // x arms
+    for (int i = 0; i < RY + 8; ++i) {
+      const C2 val = P[((tyg * RY + i) * HX + tx + HAL) * SC + cs];
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
-        const C2 *rp = P + ((tyg * RY + r + HAL) * HX + tx + HAL) * SC + cs;
+        const int d = i - r;
+        if (d < 0 || d > 8) continue;
+        if (d < 4) {
+          ya[r] = cfma(w_y[d], val, ya[r]);
+        } else if (d > 4) {
+          yb[r] = cfma(w_y[d], val, yb[r]);
+        } else {
+          const double vv = vd[(tyg * RY + r) * TX + tx] + fxy[r] + vz;
+          xa[r] = cfma(w_x[4] + static_cast<T>(vv), val, xa[r]);
 #pragma unroll
-        for (int d = -4; d <= 4; ++d)
-          if (d != 0) xy[r] = cfma(w_x[d + 4], rp[d * SC], xy[r]);
-        acc[r][(4 + K) % 9].x += xy[r].x;
-        acc[r][(4 + K) % 9].y += xy[r].y;
-        done[r] = acc[r][K];
-        acc[r][K] = czero<C2>();
+          for (int j = 0; j < 9; ++j)
+            if (j != 4) acc[r][(j + K) % 9] = cfma(w_z[8 - j], val, acc[r][(j + K) % 9]);
+        }
       }
-    };
-    switch (ring) {
-      case 0: compute(std::integral_constant<int, 0>{}); break;
-      case 1: compute(std::integral_constant<int, 1>{}); break;
-      case 2: compute(std::integral_constant<int, 2>{}); break;
-      case 3: compute(std::integral_constant<int, 3>{}); break;
-      case 4: compute(std::integral_constant<int, 4>{}); break;
-      case 5: compute(std::integral_constant<int, 5>{}); break;
-      case 6: compute(std::integral_constant<int, 6>{}); break;
-      case 7: compute(std::integral_constant<int, 7>{}); break;
-      default: compute(std::integral_constant<int, 8>{}); break;
     }
-    ring = ring == 8 ? 0 : ring + 1;
+    C2 done[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+      const C2 *rp = P + ((tyg * RY + r + HAL) * HX + tx + HAL) * SC + cs;
+#pragma unroll
+      for (int d = -4; d <= -1; ++d) xa[r] = cfma(w_x[d + 4], rp[d * SC], xa[r]);
+#pragma unroll
+      for (int d = 1; d <= 4; ++d) xb[r] = cfma(w_x[d + 4], rp[d * SC], xb[r]);
+      C2 &a4 = acc[r][(4 + K) % 9];
+      a4.x += (ya[r].x + yb[r].x) + (xa[r].x + xb[r].x);
+      a4.y += (ya[r].y + yb[r].y) + (xa[r].y + xb[r].y);
+      done[r] = acc[r][K];
+      acc[r][K] = czero<C2>();
+    }
 
-    // ---- epilogue: outputs of plane zo = pz - 4 are complete ---------------
+    // ---- outputs of plane zo = pz - 4 are complete ----------------------------
     const int zo = pz - HAL;
     if (zo >= zs) {
-      const int *ro = rowring + (zo & (RING - 1)) * TY * TX;
-      const C2 *x0s = psi0ring + buf * INNER;
+      const int *ro = rowring + ((K + 5) % RING) * TY * TX;
+      const C2 *x0s = psi0ring + DB * INNER;
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
         const int ty = tyg * RY + r;
-        const int rowv = ro[ty * TX + tx];
-        const int rr0 = rowv & 0x3fffffff;
-        const int row = (rowv >= 0 && rr0 < p.np) ? rr0 : -1;
+        const int row = ro[ty * TX + tx];
+        if (row < 0 || row >= p.np) continue;
         const C2 h = done[r];
-        if (row >= 0) {
-          const C2 x0 = need_x0 ? x0s[(ty * TX + tx) * SC + cs] : czero<C2>();
-          if (obs_on) {
-            const double rr = px * xr + py * double(cy0 + ty + B.lo[1]) + pzc * double(zo + B.lo[2]);
+        C2 val = h;
+        if constexpr (X0) {
+          const C2 x0 = x0s[(ty * TX + tx) * SC + cs];
+          if constexpr (OBS) {
+            const double rr = p.obs_pol[0] * B.h[0] * xr + p.obs_pol[1] * B.h[1] * double(cy0 + ty + B.lo[1]) +
+                              p.obs_pol[2] * B.h[2] * double(zo + B.lo[2]);
             const double n2 = double(x0.x) * double(x0.x) + double(x0.y) * double(x0.y);
             kadd(ke, double(x0.x) * double(h.x) + double(x0.y) * double(h.y));
             kadd(kn, n2);
             kadd(kd, n2 * rr);
           }
-          C2 val = h;
-          if (horner) {
+          if constexpr (HORNER) {
             val.x = x0.x + are * h.x - aim * h.y;
             val.y = x0.y + are * h.y + aim * h.x;
           }
-          out[row * out_ldc + cidx] = val;
         }
+        out[row * out_ldc + cidx] = val;
       }
     }
+  };
+
+#pragma unroll 1
+  for (int pz = zbeg; pz < zend; pz += 9) {
+    plane(std::integral_constant<int, 0>{}, pz);
+    if (pz + 1 < zend) plane(std::integral_constant<int, 1>{}, pz + 1);
+    if (pz + 2 < zend) plane(std::integral_constant<int, 2>{}, pz + 2);
+    if (pz + 3 < zend) plane(std::integral_constant<int, 3>{}, pz + 3);
+    if (pz + 4 < zend) plane(std::integral_constant<int, 4>{}, pz + 4);
+    if (pz + 5 < zend) plane(std::integral_constant<int, 5>{}, pz + 5);
+    if (pz + 6 < zend) plane(std::integral_constant<int, 6>{}, pz + 6);
+    if (pz + 7 < zend) plane(std::integral_constant<int, 7>{}, pz + 7);
+    if (pz + 8 < zend) plane(std::integral_constant<int, 8>{}, pz + 8);
   }
   cp_async_wait<0>();
 
-  if (obs_on) {
+  if constexpr (OBS) {
     __syncthreads();
     double *red = reinterpret_cast<double *>(smem);  // NT x 6 doubles
     red[tid * 6 + 0] = ke.s;
@@ -409,13 +432,12 @@ __global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
   }
 }
 
-template <typename T, int SC, int TX, int TY, int RY>
-hpsi_status launch_variant(const PassArgs &a, cudaStream_t st) {
-  constexpr int NBUF = 3;
-  using LY = PassLayout<T, SC, TX, TY, RY, NBUF>;
+template <typename T, int SC, int TX, int TY, int RY, bool HORNER, bool OBS>
+hpsi_status launch_mode(const PassArgs &a, cudaStream_t st) {
+  using LY = PassLayout<T, SC, TX, TY, RY>;
   const size_t red = size_t(LY::NT) * 6 * sizeof(double);
   const size_t bytes = std::max(LY::bytes, red);
-  auto kern = pass_kernel<T, SC, TX, TY, RY, NBUF>;
+  auto kern = pass_kernel<T, SC, TX, TY, RY, HORNER, OBS>;
   static bool attr_set = false;
   if (!attr_set) {
     HPSI_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
@@ -425,6 +447,15 @@ hpsi_status launch_variant(const PassArgs &a, cudaStream_t st) {
   kern<<<nblocks, LY::NT, bytes, st>>>(a);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
+}
+
+template <typename T, int SC, int TX, int TY, int RY, bool UNR = false>
+hpsi_status launch_variant(const PassArgs &a, cudaStream_t st) {
+  const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr;
+  if (horner && obs) return launch_mode<T, SC, TX, TY, RY, true, true>(a, st);
+  if (horner) return launch_mode<T, SC, TX, TY, RY, true, false>(a, st);
+  if (obs) return launch_mode<T, SC, TX, TY, RY, false, true>(a, st);
+  return launch_mode<T, SC, TX, TY, RY, false, false>(a, st);
 }
 
 }  // namespace

@@ -52,6 +52,8 @@ struct PassArgs {
 struct PassShape {
   int sc;   // complex states per CTA
   int tx, ty, ry;
+  int zb = 0;  // output planes per work item (0: chosen from the wave count)
+  int unroll = 0;  // 1: nine-plane unrolled ring, 0: switch-selected ring
 };
 
 // Launch the fused pass for a storage type (double -> FP64, float -> FP32).
