@@ -187,6 +187,24 @@ hpsi_status hpsi_dotp_matrix(hpsi_mesh *mesh, const hpsi_batch *a,
 hpsi_status hpsi_orthonormalize_cholesky(hpsi_mesh *mesh, hpsi_batch *psi,
                                          void *stream);
 
+/* Allocation-free variant of hpsi_nrm2 (no counterpart in the reference).
+ * For callers that must not make the library allocate device memory at this
+ * point (an application that owns the whole device-memory budget or pool, or
+ * a per-step loop that may not reach the allocator): it takes np and the
+ * volume element directly, needs no mesh handle and calls neither cudaMalloc
+ * nor cudaFree.  Its partial sums live in one fixed device array of the
+ * library (about 1 MiB, held by every GPU that loads the library until the
+ * process exits), so at most HPSI_NOALLOC_MAX_STATES states are accepted;
+ * larger batches get HPSI_ERR_ARG.  The first call on a device looks up that
+ * array's device address and should come before any stream capture.  All
+ * calls on a device share the array and it keeps the last call's contents:
+ * calls that overlap on the GPU (for example on two streams) race and must be
+ * ordered by the caller.  `out` (nst doubles) may be host or device memory;
+ * with host memory the call waits for the stream. */
+#define HPSI_NOALLOC_MAX_STATES 256
+hpsi_status hpsi_nrm2_noalloc(int32_t np, double vol_pp, const hpsi_batch *psi,
+                              double *out, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Library-wide controls and diagnostics. */
 const char *hpsi_last_error_string(void);

@@ -76,6 +76,8 @@ SIGNATURES = {
     "hpsi_last_error_string": (C.c_char_p, []),
     "hpsi_kernel_launch_count": (C.c_int64, []),
     "hpsi_version": (C.c_char_p, []),
+    "hpsi_nrm2_noalloc": (C.c_int32, [C.c_int32, C.c_double, C.POINTER(Batch), C.POINTER(C.c_double),
+                                      C.c_void_p]),
     "hpsi_profile_enable": (C.c_int32, [C.c_int32]),
     "hpsi_profile_query": (C.c_int32, [C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
 }
@@ -284,6 +286,14 @@ class Hamiltonian:
         check(load().hpsi_taylor_step(self.handle, C.byref(b), dt.real, dt.imag, order, None, None, None,
                                       _stream_ptr(stream)))
         return None
+
+
+def nrm2_noalloc(np_inner: int, vol_pp: float, psi, nst=None, stream=None) -> np.ndarray:
+    """State norms through the allocation-free entry point (host result)."""
+    b = as_batch(psi, nst=nst)
+    out = np.zeros(b.nst)
+    check(load().hpsi_nrm2_noalloc(int(np_inner), float(vol_pp), C.byref(b), _dp(out), _stream_ptr(stream)))
+    return out
 
 
 def launch_count() -> int:
