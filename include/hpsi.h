@@ -172,6 +172,31 @@ hpsi_status hpsi_taylor_step(hpsi_hamiltonian *ham, hpsi_batch *psi, double dt_r
                              double *dipole, double *norm2, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* Time propagation with exponential-midpoint steps
+ * (TDPropagator = exp_mid, src/td/propagator_expmid.F90:52-100, driven by
+ * td_run, src/td/td.F90:546-631) under a frozen local potential and a
+ * length-gauge laser E(t) pol.r with E(t) = E0 sin^2(pi t/T) cos(omega t) on
+ * [0, T] (zero outside).  Step n applies the order-`order` Taylor exponential
+ * of H(t0 + (n + 1/2) dt).  Per-step FP64 observables of psi(t_n) under
+ * H(t_n), summed over the states (host arrays of nsteps, any may be NULL):
+ *   energy[n] = sum_i <psi_i|H(t_n)|psi_i>, dipole[n] = sum_i <psi_i|pol.r|psi_i>,
+ *   norm2[n] = sum_i <psi_i|psi_i>.
+ * use_graph != 0 captures one step (all passes and the observable reduction)
+ * in a CUDA graph and replays it nsteps times; the field amplitude of each
+ * step comes from a device table, so one graph serves every step.  Returns
+ * HPSI_ERR_RUNAWAY if the norm grows by more than 1e-3 relative (the Taylor
+ * series diverges for too large dt), HPSI_ERR_NONFINITE on NaN/Inf. */
+typedef struct {
+  double E0, omega, T;  /* amplitude, frequency, envelope length (a.u.) */
+  double pol[3];        /* polarisation (also the dipole direction) */
+} hpsi_laser;
+
+hpsi_status hpsi_td_propagate(hpsi_hamiltonian *ham, hpsi_batch *psi, int32_t nsteps,
+                              double dt, int32_t order, const hpsi_laser *laser,
+                              double t0, int32_t use_graph, double *energy,
+                              double *dipole, double *norm2, void *stream);
+
+/* ------------------------------------------------------------------ */
 /* FP64 reductions over the np inner points (dV = vol_pp), results in host
  * arrays:
  *   hpsi_nrm2        out[nst]      X(mesh_batch_nrm2), src/grid/mesh_batch_inc.F90:970-1167

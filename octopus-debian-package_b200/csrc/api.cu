@@ -47,6 +47,11 @@ cudaEvent_t prof_event() {
 ProfScope::ProfScope(const char *label, cudaStream_t st) : st_(st) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   if (!g_prof_on || g_prof.size() >= (1u << 20)) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return;  // no timing events inside a graph capture
+  }
   ProfRec r{label, prof_event(), prof_event()};
   cudaEventRecord(r.a, st);
   g_prof.push_back(r);
@@ -423,6 +428,9 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   h->bra_partial.release();
   h->obsbuf.release();
   h->ketobs.release();
+  h->tdbuf.release();
+  if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
+  if (h->capture_event) cudaEventDestroy(h->capture_event);
   h->small.release();
   delete h;
   return HPSI_OK;
@@ -719,6 +727,7 @@ void base_pass_args(const hpsi_hamiltonian *h, int terms, const int *src_map, Pa
   if (terms & HPSI_TERM_LOCAL_POTENTIAL) {
     a.v_cell = h->d_vcell;
     for (int k = 0; k < 3; ++k) a.fld[k] = h->fld[k];
+    a.fld_scale_dev = h->fld_scale_dev;
   }
   a.obs_pol[0] = 0.0;
   a.obs_pol[1] = 0.0;
@@ -851,6 +860,39 @@ size_t obs_partial_bytes(hpsi_hamiltonian *h, long long ld) {
       n = std::max(n, size_t(nitems));
   }
   return std::max<size_t>(n, 1) * ld * 6 * sizeof(double);
+}
+
+// Allocate every workspace a Taylor step touches (so that a step can be
+// captured in a CUDA graph without allocating).
+hpsi_status prepare_taylor_workspaces(hpsi_hamiltonian *h, long long ld, size_t elem, bool obs) {
+  hpsi_mesh *m = h->mesh;
+  const size_t ubytes = size_t(m->np) * ld * 2 * elem;
+  for (auto &w : h->u) {
+    hpsi_status s = w.ensure(ubytes);
+    if (s) return s;
+  }
+  if (obs) {
+    hpsi_status s = h->obsbuf.ensure(obs_partial_bytes(h, ld));
+    if (s) return s;
+    s = h->small.ensure(3 * size_t(ld) * sizeof(double));
+    if (s) return s;
+  }
+  if (h->nmat > 0) {
+    hpsi_status s = h->projbuf.ensure(size_t(h->nprojections) * ld * 2 * elem);
+    if (s) return s;
+    ProjArgs p;
+    std::memset(&p, 0, sizeof(p));
+    p.nmat = h->nmat;
+    p.psi_ld = ld;
+    p.min_npoints = h->min_npoints;
+    s = h->bra_partial.ensure(size_t(bra_ksplit(p, m->num_sms)) * h->nprojections * ld * 2 * elem);
+    if (s) return s;
+    if (obs) {
+      s = h->ketobs.ensure(size_t(ket_row_blocks(h->nk)) * ld * 2 * sizeof(double));
+      if (s) return s;
+    }
+  }
+  return HPSI_OK;
 }
 
 template <typename T>

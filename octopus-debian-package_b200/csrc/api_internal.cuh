@@ -75,7 +75,10 @@ struct hpsi_hamiltonian {
   int *d_krows = nullptr, *d_kptr = nullptr;
   int4 *d_kb_ent = nullptr;
   bool use_tensor_bra = true;
+  const double *fld_scale_dev = nullptr;  // set while a TD run replays steps
+  cudaStream_t capture_stream = nullptr;  // graph capture / replay stream of TD runs
+  cudaEvent_t capture_event = nullptr;
   // workspaces
-  hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small;
+  hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small, tdbuf;
   void proj_free();
 };

@@ -41,6 +41,10 @@ class MeshDesc(C.Structure):
                 ("per_inner", C.POINTER(C.c_int32))]
 
 
+class Laser(C.Structure):
+    _fields_ = [("E0", C.c_double), ("omega", C.c_double), ("T", C.c_double), ("pol", C.c_double * 3)]
+
+
 class Batch(C.Structure):
     _fields_ = [("ptr", C.c_void_p), ("ld", C.c_int64), ("nst", C.c_int32), ("npts", C.c_int32),
                 ("dtype", C.c_int32)]
@@ -69,6 +73,9 @@ SIGNATURES = {
     "hpsi_taylor_step": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_double, C.c_double, C.c_int32,
                                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                      C.c_void_p]),
+    "hpsi_td_propagate": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
+                                      C.POINTER(Laser), C.c_double, C.c_int32, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_nrm2": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_dotp_matrix": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(C.c_double),
                                      C.c_void_p]),
@@ -251,6 +258,19 @@ class Hamiltonian:
         sc = np.ascontiguousarray(np.concatenate(scals).astype(np.float64))
         check(load().hpsi_hamiltonian_set_projectors(self.handle, len(maps), _ip(npts), _ip(nproj), _ip(mp),
                                                      _dp(mt), _dp(sc)))
+
+    # exponential-midpoint time propagation (td_run with TDPropagator = exp_mid)
+    def td_propagate(self, psi, nsteps, dt, order=4, E0=0.0, omega=0.0, T=0.0, pol=(0.0, 0.0, 1.0), t0=0.0,
+                     graph=True, nst=None, stream=None):
+        b = as_batch(psi, nst=nst)
+        las = Laser()
+        las.E0, las.omega, las.T = float(E0), float(omega), float(T)
+        for a in range(3):
+            las.pol[a] = float(pol[a])
+        e, d, n = np.zeros(nsteps), np.zeros(nsteps), np.zeros(nsteps)
+        check(load().hpsi_td_propagate(self.handle, C.byref(b), int(nsteps), float(dt), int(order), C.byref(las),
+                                       float(t0), 1 if graph else 0, _dp(e), _dp(d), _dp(n), _stream_ptr(stream)))
+        return e, d, n
 
     def close(self):
         if getattr(self, "handle", None):

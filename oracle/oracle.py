@@ -219,6 +219,42 @@ class Hamiltonian:
 
 
 # ---------------------------------------------------------------------------
+# time propagation (exponential midpoint, td_run / exponential_midpoint)
+def laser_field(E0, omega, T, t):
+    """E0 sin^2(pi t/T) cos(omega t) on [0, T], zero outside."""
+    if t < 0 or t > T or T <= 0:
+        return 0.0
+    return E0 * np.sin(np.pi * t / T) ** 2 * np.cos(omega * t)
+
+
+def td_propagate(H, v0, psi, nsteps, dt, E0, omega, T, pol=(0.0, 0.0, 1.0), order=4, t0=0.0):
+    """Exponential-midpoint propagation with the laser folded into v
+    (src/td/propagator_expmid.F90:52-100, src/hamiltonian/hamiltonian_elec.F90:1028).
+
+    Returns (psi_final (np, nst), energy[n], dipole[n], norm2[n]) where the
+    observables are those of psi(t_n) under H(t_n), summed over the states."""
+    m = H.mesh
+    r = m.x[: m.np] @ np.asarray(pol, dtype=np.float64)
+    x = np.array(psi, dtype=np.complex128, copy=True)
+    E, D, N = [], [], []
+    dv = m.vol_pp
+    for n in range(nsteps):
+        tn = t0 + n * dt
+        H.v[:] = v0 + laser_field(E0, omega, T, tn) * r
+        h = H.apply(x)
+        a = x[: m.np]
+        E.append(dv * float(np.sum(np.real(a.conj() * h))))
+        D.append(dv * float(np.sum(np.abs(a) ** 2 * r[:, None])))
+        N.append(dv * float(np.sum(np.abs(a) ** 2)))
+        H.v[:] = v0 + laser_field(E0, omega, T, tn + 0.5 * dt) * r
+        y = H.taylor(x, dt, order=order)
+        x = np.zeros_like(x)
+        x[: m.np] = y
+    H.v[:] = v0
+    return x[: m.np], np.array(E), np.array(D), np.array(N)
+
+
+# ---------------------------------------------------------------------------
 # dense FP64 pieces
 def mesh_batch_nrm2(mesh, psi):
     a = np.asarray(psi)[: mesh.np]
