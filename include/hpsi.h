@@ -197,6 +197,33 @@ hpsi_status hpsi_td_propagate(hpsi_hamiltonian *ham, hpsi_batch *psi, int32_t ns
                               double *dipole, double *norm2, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* Independent systems advanced together (no reference counterpart: the
+ * reference loops over state blocks on the host,
+ * propagation_ops_elec_fuse_density_exp_apply, src/td/propagation_ops_elec.F90:261-333).
+ * A group holds nsys Hamiltonians (borrowed, uneven meshes and state counts).
+ * hpsi_group_taylor_steps applies nsteps order-`order` Taylor steps (real dt)
+ * to psis[s] (device batches, one per system, one storage type): per Horner
+ * pass, the KB bras of all systems, one persistent stencil launch over a
+ * (system, tile column + z block, state chunk) work list sorted by cost
+ * (up to 48 systems per launch), and the KB kets.  use_graph != 0 captures one
+ * step in a CUDA graph and replays it. */
+typedef struct hpsi_group hpsi_group;
+hpsi_status hpsi_group_create(int32_t nsys, hpsi_hamiltonian *const *hams,
+                              hpsi_group **out);
+hpsi_status hpsi_group_destroy(hpsi_group *group);
+hpsi_status hpsi_group_taylor_steps(hpsi_group *group, hpsi_batch *psis,
+                                    int32_t nsteps, double dt, int32_t order,
+                                    int32_t use_graph, void *stream);
+
+/* Autotuner: times the candidate shapes of the fused stencil pass (state chunk
+ * width, z block depth) on scratch batches of width ld and storage dtype and
+ * keeps the fastest for this Hamiltonian's later calls with that width.
+ * shape_out (optional): {state chunk, rows per thread, z block, tile edge};
+ * ms_out: time of one pass with that shape. */
+hpsi_status hpsi_autotune(hpsi_hamiltonian *ham, int32_t dtype, int64_t ld,
+                          int32_t shape_out[4], double *ms_out, void *stream);
+
+/* ------------------------------------------------------------------ */
 /* FP64 reductions over the np inner points (dV = vol_pp), results in host
  * arrays:
  *   hpsi_nrm2        out[nst]      X(mesh_batch_nrm2), src/grid/mesh_batch_inc.F90:970-1167

@@ -785,12 +785,19 @@ hpsi_status run_ket(hpsi_hamiltonian *h, const T *proj, long long ld, int nst, T
   return launch_ket<T>(k, st);
 }
 
-// One fused pass.  in: rows to stencil; out: result rows; psi0 for Horner.
+// Shape of the fused pass for a batch: the autotuned one when it matches.
+PassShape pass_shape(const hpsi_hamiltonian *h, int dtype, long long ld) {
+  const auto &t = h->tuned[dtype == HPSI_C128 ? 0 : 1];
+  if (t.ld == ld && !std::getenv(dtype == HPSI_C128 ? "HPSI_PASS_SHAPE64" : "HPSI_PASS_SHAPE32")) return t.shape;
+  return default_shape(dtype, ld);
+}
+
+// Arguments of one fused pass (no launch).  in: rows to stencil; out: result
+// rows; psi0: pointwise term of a Horner pass.
 template <typename T>
-hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T *in, long long in_ld, T *out,
-                     long long out_ld, long long ld, int mode, const T *psi0, long long psi0_ld, double a_re,
-                     double a_im, double *obs_partial, int *ncta_out, cudaStream_t st) {
-  PassArgs a;
+hpsi_status build_pass_args(hpsi_hamiltonian *h, int terms, const int *src_map, const T *in, long long in_ld, T *out,
+                            long long out_ld, long long ld, int mode, const T *psi0, long long psi0_ld, double a_re,
+                            double a_im, const PassShape &shape, PassArgs &a) {
   base_pass_args(h, terms, src_map, a);
   if (h->mesh->periodic && h->d_src_phase && src_map == h->d_src_phase)
     a.phase_corr = sizeof(T) == 8 ? static_cast<const void *>(h->d_phase) : static_cast<const void *>(h->d_phase_f);
@@ -803,6 +810,21 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
   a.psi0_ld = psi0_ld;
   a.a_re = a_re;
   a.a_im = a_im;
+  a.chunks = int(ld / shape.sc);
+  a.zb = shape.zb > 0 ? shape.zb : choose_zb(h->mesh, a.chunks);
+  return mesh_items(h->mesh, a.zb, &a.items, &a.nitems);
+}
+
+// One fused pass with its KB bra before and ket after.
+template <typename T>
+hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T *in, long long in_ld, T *out,
+                     long long out_ld, long long ld, int mode, const T *psi0, long long psi0_ld, double a_re,
+                     double a_im, double *obs_partial, int *ncta_out, cudaStream_t st) {
+  PassArgs a;
+  const PassShape shape = pass_shape(h, sizeof(T) == 8 ? HPSI_C128 : HPSI_C64, ld);
+  hpsi_status si = build_pass_args<T>(h, terms, src_map, in, in_ld, out, out_ld, ld, mode, psi0, psi0_ld, a_re,
+                                      a_im, shape, a);
+  if (si) return si;
   const bool nl = (terms & HPSI_TERM_NON_LOCAL_POTENTIAL) && h->nmat > 0;
   if (nl) {
     const size_t pbytes = size_t(h->nprojections) * ld * 2 * sizeof(T);
@@ -811,11 +833,6 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
     s = run_bra<T>(h, in, in_ld, static_cast<T *>(h->projbuf.ptr), st);
     if (s) return s;
   }
-  const PassShape shape = default_shape(sizeof(T) == 8 ? HPSI_C128 : HPSI_C64, ld);
-  a.chunks = int(ld / shape.sc);
-  a.zb = shape.zb > 0 ? shape.zb : choose_zb(h->mesh, a.chunks);
-  hpsi_status si = mesh_items(h->mesh, a.zb, &a.items, &a.nitems);
-  if (si) return si;
   if (obs_partial) {
     a.obs = obs_partial;
     a.obs_ld = int(ld);
@@ -841,6 +858,19 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
   return HPSI_OK;
 }
 
+template hpsi_status build_pass_args<double>(hpsi_hamiltonian *, int, const int *, const double *, long long,
+                                             double *, long long, long long, int, const double *, long long, double,
+                                             double, const PassShape &, PassArgs &);
+template hpsi_status build_pass_args<float>(hpsi_hamiltonian *, int, const int *, const float *, long long, float *,
+                                            long long, long long, int, const float *, long long, double, double,
+                                            const PassShape &, PassArgs &);
+template hpsi_status run_bra<double>(hpsi_hamiltonian *, const double *, long long, double *, cudaStream_t);
+template hpsi_status run_bra<float>(hpsi_hamiltonian *, const float *, long long, float *, cudaStream_t);
+template hpsi_status run_ket<double>(hpsi_hamiltonian *, const double *, long long, int, double *, long long, int,
+                                     double, double, const double *, long long, double *, cudaStream_t);
+template hpsi_status run_ket<float>(hpsi_hamiltonian *, const float *, long long, int, float *, long long, int,
+                                    double, double, const float *, long long, double *, cudaStream_t);
+
 const int *load_map(const hpsi_hamiltonian *h, int set_bc) {
   const hpsi_mesh *m = h->mesh;
   if (!set_bc) return m->d_src_raw;
@@ -852,7 +882,7 @@ const int *load_map(const hpsi_hamiltonian *h, int set_bc) {
 size_t obs_partial_bytes(hpsi_hamiltonian *h, long long ld) {
   size_t n = 0;
   for (int dt : {HPSI_C128, HPSI_C64}) {
-    const PassShape sh = default_shape(dt, ld);
+    const PassShape sh = pass_shape(h, dt, ld);
     const int4 *items;
     int nitems = 0;
     const int zb = sh.zb > 0 ? sh.zb : choose_zb(h->mesh, int(ld / sh.sc));

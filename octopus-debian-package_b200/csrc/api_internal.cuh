@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "stencil.cuh"
 
 namespace hpsi {
 
@@ -75,6 +76,12 @@ struct hpsi_hamiltonian {
   int *d_krows = nullptr, *d_kptr = nullptr;
   int4 *d_kb_ent = nullptr;
   bool use_tensor_bra = true;
+  // autotuned pass shape per storage type (valid for batches of width ld)
+  struct Tuned {
+    long long ld = -1;
+    hpsi::PassShape shape{};
+    double ms = 0.0;
+  } tuned[2];
   const double *fld_scale_dev = nullptr;  // set while a TD run replays steps
   cudaStream_t capture_stream = nullptr;  // graph capture / replay stream of TD runs
   cudaEvent_t capture_event = nullptr;

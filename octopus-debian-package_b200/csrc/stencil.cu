@@ -122,8 +122,8 @@ struct PassLayout {
 // ring position (data, rows, maps, the 9 running sums) is a compile-time
 // constant.  HORNER: out = psi0 + a * H in; OBS: per-state observables of in.
 template <typename T, int SC, int TX, int TY, int RY, bool HORNER, bool OBS>
-__global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
-    pass_kernel(const PassArgs p) {
+__device__ __forceinline__ void pass_body(const PassArgs &p, const int item, const int chunk,
+                                          unsigned char *smem) {
   using LY = PassLayout<T, SC, TX, TY, RY>;
   using C2 = typename LY::C2;
   constexpr int HAL = LY::HAL, HX = LY::HX, HY = LY::HY, NT = LY::NT, NBUF = LY::NBUF, RING = LY::RING;
@@ -139,7 +139,6 @@ __global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
   constexpr int NV = TY * TX / 2, NR = TY * TX / 4, NM = HY * HX / 4;  // 16-byte copies
   constexpr bool X0 = HORNER || OBS;
 
-  extern __shared__ __align__(16) unsigned char smem[];
   C2 *planes = reinterpret_cast<C2 *>(smem + LY::off_planes);
   C2 *psi0ring = reinterpret_cast<C2 *>(smem + LY::off_psi0);
   double *vring = reinterpret_cast<double *>(smem + LY::off_v);
@@ -150,10 +149,6 @@ __global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
   const int cs = tid % SC;  // complex state within the chunk
   const int tx = (tid / SC) % TX;
   const int tyg = tid / (SC * TX);
-  // the chunks of a work item are adjacent in launch order, so they run
-  // together and share each row's DRAM lines, the cell maps and v in L2
-  const int chunk = blockIdx.x % p.chunks;
-  const int item = blockIdx.x / p.chunks;
   const int4 it = p.items[item];
   const CellBox &B = p.box;
   const int cx0 = HAL + it.x * TX, cy0 = HAL + it.y * TY;
@@ -432,6 +427,32 @@ __global__ void __launch_bounds__(SC * TX * (TY / RY), 1)
   }
 }
 
+// One system: the chunks of a work item are adjacent in launch order, so they
+// run together and share each row's DRAM lines, the cell maps and v in L2.
+template <typename T, int SC, int TX, int TY, int RY, bool HORNER, bool OBS>
+__global__ void __launch_bounds__(SC * TX * (TY / RY), 1) pass_kernel(const __grid_constant__ PassArgs p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  pass_body<T, SC, TX, TY, RY, HORNER, OBS>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem);
+}
+
+// Many systems in one persistent launch: each CTA takes (system, item,
+// chunk) units from a list sorted by cost until it is exhausted.
+template <typename T, int SC, int TX, int TY, int RY, bool HORNER>
+__global__ void __launch_bounds__(SC * TX * (TY / RY), 1) pass_group_kernel(const __grid_constant__ GroupArgs g) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int unit_s;
+  for (;;) {
+    if (threadIdx.x == 0) unit_s = atomicAdd(g.counter, 1);
+    __syncthreads();
+    const int u = unit_s;
+    __syncthreads();
+    if (u >= g.nunits) break;
+    const int4 U = g.units[u];  // {system, item, chunk, -}
+    pass_body<T, SC, TX, TY, RY, HORNER, false>(g.sys[U.x], U.y, U.z, smem);
+    __syncthreads();
+  }
+}
+
 template <typename T, int SC, int TX, int TY, int RY, bool HORNER, bool OBS>
 hpsi_status launch_mode(const PassArgs &a, cudaStream_t st) {
   using LY = PassLayout<T, SC, TX, TY, RY>;
@@ -485,6 +506,51 @@ hpsi_status launch_pass(PassArgs a, const PassShape &s, cudaStream_t st) {
   return HPSI_ERR_UNSUPPORTED;
 }
 
+template <typename T, int SC, int RY>
+hpsi_status launch_group_v(const GroupArgs &g, int grid, cudaStream_t st) {
+  using LY = PassLayout<T, SC, 16, 16, RY>;
+  const size_t bytes = LY::bytes;
+  if (g.sys[0].mode == PASS_HORNER) {
+    auto kern = pass_group_kernel<T, SC, 16, 16, RY, true>;
+    static bool set = false;
+    if (!set) {
+      HPSI_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+      set = true;
+    }
+    kern<<<grid, LY::NT, bytes, st>>>(g);
+  } else {
+    auto kern = pass_group_kernel<T, SC, 16, 16, RY, false>;
+    static bool set = false;
+    if (!set) {
+      HPSI_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+      set = true;
+    }
+    kern<<<grid, LY::NT, bytes, st>>>(g);
+  }
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+
+template <typename T>
+hpsi_status launch_pass_group(const GroupArgs &g, int sc, int num_sms, cudaStream_t st) {
+  if (g.nunits == 0) return HPSI_OK;
+  const int grid = std::min(g.nunits, num_sms);
+  if constexpr (sizeof(T) == 8) {
+    if (sc == 4) return launch_group_v<T, 4, 2>(g, grid, st);
+    if (sc == 2) return launch_group_v<T, 2, 2>(g, grid, st);
+    if (sc == 1) return launch_group_v<T, 1, 2>(g, grid, st);
+  } else {
+    if (sc == 8) return launch_group_v<T, 8, 4>(g, grid, st);
+    if (sc == 4) return launch_group_v<T, 4, 4>(g, grid, st);
+    if (sc == 2) return launch_group_v<T, 2, 4>(g, grid, st);
+    if (sc == 1) return launch_group_v<T, 1, 4>(g, grid, st);
+  }
+  set_error("launch_pass_group: no kernel variant for this state chunk");
+  return HPSI_ERR_UNSUPPORTED;
+}
+
+template hpsi_status launch_pass_group<double>(const GroupArgs &, int, int, cudaStream_t);
+template hpsi_status launch_pass_group<float>(const GroupArgs &, int, int, cudaStream_t);
 template hpsi_status launch_pass<double>(PassArgs, const PassShape &, cudaStream_t);
 template hpsi_status launch_pass<float>(PassArgs, const PassShape &, cudaStream_t);
 

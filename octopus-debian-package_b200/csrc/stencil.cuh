@@ -63,4 +63,18 @@ hpsi_status launch_pass(PassArgs a, const PassShape &shape, cudaStream_t st);
 // Tile edge (cells) of every pass kernel variant.
 constexpr int PASS_TILE = 16;
 
+// Systems of one grouped launch (their arguments travel as kernel parameters).
+constexpr int GROUP_MAX = 48;
+struct GroupArgs {
+  PassArgs sys[GROUP_MAX];
+  const int4 *units;   // {system, item, chunk, -}, most expensive first
+  int nunits;
+  int *counter;        // zeroed before every launch
+};
+
+// One persistent launch of the fused pass over several systems (no
+// observables); sc must be a valid chunk for every system.
+template <typename T>
+hpsi_status launch_pass_group(const GroupArgs &g, int sc, int num_sms, cudaStream_t st);
+
 }  // namespace hpsi

@@ -76,6 +76,12 @@ SIGNATURES = {
     "hpsi_td_propagate": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
                                       C.POINTER(Laser), C.c_double, C.c_int32, C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_group_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "hpsi_group_destroy": (C.c_int32, [C.c_void_p]),
+    "hpsi_group_taylor_steps": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
+                                            C.c_int32, C.c_void_p]),
+    "hpsi_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                  C.c_void_p]),
     "hpsi_nrm2": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_dotp_matrix": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(C.c_double),
                                      C.c_void_p]),
@@ -259,6 +265,14 @@ class Hamiltonian:
         check(load().hpsi_hamiltonian_set_projectors(self.handle, len(maps), _ip(npts), _ip(nproj), _ip(mp),
                                                      _dp(mt), _dp(sc)))
 
+    def autotune(self, dtype=HPSI_C128, ld=32, stream=None):
+        """Pick the fastest pass shape for batches of width ld; returns
+        ({sc, ry, zb, tile}, ms)."""
+        shp = (C.c_int32 * 4)()
+        ms = C.c_double()
+        check(load().hpsi_autotune(self.handle, int(dtype), int(ld), shp, C.byref(ms), _stream_ptr(stream)))
+        return dict(sc=shp[0], ry=shp[1], zb=shp[2], tile=shp[3]), float(ms.value)
+
     # exponential-midpoint time propagation (td_run with TDPropagator = exp_mid)
     def td_propagate(self, psi, nsteps, dt, order=4, E0=0.0, omega=0.0, T=0.0, pol=(0.0, 0.0, 1.0), t0=0.0,
                      graph=True, nst=None, stream=None):
@@ -306,6 +320,35 @@ class Hamiltonian:
         check(load().hpsi_taylor_step(self.handle, C.byref(b), dt.real, dt.imag, order, None, None, None,
                                       _stream_ptr(stream)))
         return None
+
+
+class Group:
+    """Independent systems advanced together (hpsi_group)."""
+
+    def __init__(self, hams):
+        self.hams = list(hams)
+        arr = (C.c_void_p * len(self.hams))(*[h.handle.value for h in self.hams])
+        h = C.c_void_p()
+        check(load().hpsi_group_create(len(self.hams), arr, C.byref(h)))
+        self.handle = h
+
+    def taylor_steps(self, psis, nsteps, dt, order=4, graph=True, nsts=None, stream=None):
+        bs = (Batch * len(psis))()
+        for i, x in enumerate(psis):
+            bs[i] = as_batch(x, nst=None if nsts is None else nsts[i])
+        check(load().hpsi_group_taylor_steps(self.handle, bs, int(nsteps), float(dt), int(order), 1 if graph else 0,
+                                             _stream_ptr(stream)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().hpsi_group_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def nrm2_noalloc(np_inner: int, vol_pp: float, psi, nst=None, stream=None) -> np.ndarray:
