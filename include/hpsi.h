@@ -224,6 +224,27 @@ hpsi_status hpsi_autotune(hpsi_hamiltonian *ham, int32_t dtype, int64_t ld,
                           int32_t shape_out[4], double *ms_out, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* Exact discrete adjoint of the Taylor propagator for optimal control
+ * (served to opt_control's backward propagation, bwd_step / bwd_step_2,
+ * src/opt_control/propagation.F90:477-783).  Forward: nsteps Taylor steps of
+ * H_n = H + eps[n] pol.r from psi0 (psi0 is not modified); objective
+ * J = sum_i |<phi_i|psi_i(T)>|^2 with phi = targets (target_groundstate,
+ * src/opt_control/target_groundstate_inc.F90:83-152).  Backward with
+ * lambda_n = T_n^dagger lambda_{n+1}; psi_n is recomputed from checkpoints
+ * stored every `ckpt` steps.  Outputs (host, each optional):
+ *   J_out;  grad_eps[nsteps] = dJ/d eps_n, exact for the discrete propagator;
+ *   grad_v[np] = dJ/d v(r), the vector-Jacobian product for the local potential;
+ *   grad_eps_cont[nsteps] = 2 dt Im <lambda_{n+1}|pol.r|psi_n>, the
+ *   continuous-adjoint gradient the reference computes (calculate_g /
+ *   update_field, propagation.F90:932-998, 1016-1103).  complex128 only. */
+hpsi_status hpsi_adjoint_gradient(hpsi_hamiltonian *ham, const hpsi_batch *psi0,
+                                  const hpsi_batch *targets, int32_t nsteps,
+                                  double dt, int32_t order, const double *eps,
+                                  const double pol[3], int32_t ckpt, double *J_out,
+                                  double *grad_eps, double *grad_v,
+                                  double *grad_eps_cont, void *stream);
+
+/* ------------------------------------------------------------------ */
 /* FP64 reductions over the np inner points (dV = vol_pp), results in host
  * arrays:
  *   hpsi_nrm2        out[nst]      X(mesh_batch_nrm2), src/grid/mesh_batch_inc.F90:970-1167

@@ -429,6 +429,7 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   h->obsbuf.release();
   h->ketobs.release();
   h->tdbuf.release();
+  h->adjbuf.release();
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   if (h->capture_event) cudaEventDestroy(h->capture_event);
   h->small.release();

@@ -86,6 +86,6 @@ struct hpsi_hamiltonian {
   cudaStream_t capture_stream = nullptr;  // graph capture / replay stream of TD runs
   cudaEvent_t capture_event = nullptr;
   // workspaces
-  hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small, tdbuf;
+  hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small, tdbuf, adjbuf;
   void proj_free();
 };

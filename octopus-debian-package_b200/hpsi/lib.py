@@ -82,6 +82,10 @@ SIGNATURES = {
                                             C.c_int32, C.c_void_p]),
     "hpsi_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                   C.c_void_p]),
+    "hpsi_adjoint_gradient": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_int32, C.c_double,
+                                          C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32,
+                                          C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_nrm2": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_dotp_matrix": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(C.c_double),
                                      C.c_void_p]),
@@ -272,6 +276,21 @@ class Hamiltonian:
         ms = C.c_double()
         check(load().hpsi_autotune(self.handle, int(dtype), int(ld), shp, C.byref(ms), _stream_ptr(stream)))
         return dict(sc=shp[0], ry=shp[1], zb=shp[2], tile=shp[3]), float(ms.value)
+
+    def adjoint_gradient(self, psi0, targets, eps, dt, order=4, pol=(0.0, 0.0, 1.0), ckpt=25, want_v=True,
+                         stream=None):
+        """(J, dJ/deps, dJ/dv or None, continuous-adjoint dJ/deps) for J = sum |<phi|psi(T)>|^2."""
+        eps = np.ascontiguousarray(np.asarray(eps, dtype=np.float64))
+        n = len(eps)
+        b0, bt = as_batch(psi0), as_batch(targets)
+        p = np.ascontiguousarray(np.asarray(pol, dtype=np.float64))
+        J = C.c_double()
+        ge, gc = np.zeros(n), np.zeros(n)
+        gv = np.zeros(self.dmesh.mesh.np) if want_v else None
+        check(load().hpsi_adjoint_gradient(self.handle, C.byref(b0), C.byref(bt), n, float(dt), int(order), _dp(eps),
+                                           _dp(p), int(ckpt), C.byref(J), _dp(ge), _dp(gv) if want_v else None,
+                                           _dp(gc), _stream_ptr(stream)))
+        return float(J.value), ge, gv, gc
 
     # exponential-midpoint time propagation (td_run with TDPropagator = exp_mid)
     def td_propagate(self, psi, nsteps, dt, order=4, E0=0.0, omega=0.0, T=0.0, pol=(0.0, 0.0, 1.0), t0=0.0,
