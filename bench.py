@@ -286,6 +286,27 @@ def main():
     ms_t32 = timed(lambda: ham.taylor_step(xt32, 0.02), tk, 1)
     del xt, xt32
 
+    # ---- TD steps (exp_mid + laser): FP64 plain launches vs FP32 graph replay --
+    # dt = 0.005: at h = 0.2 the order-4 star Laplacian reaches E_max ~ 244 Ha, and
+    # the 4th-order Taylor series is stable only for dt * E_max <= 2 sqrt(2); dt = 0.02
+    # (dt * E_max = 4.9) diverges within a few steps in any implementation.
+    dt_td = 0.005
+    laser = dict(E0=0.01, omega=0.057, T=2000 * dt_td)
+    td = {}
+    for name, xs, graph in (("td_fp64_plain", x.clone(), False), ("td_fp32_graph", x32.clone(), True)):
+        ham.td_propagate(xs, 1, dt_td, graph=graph, **laser)  # warm-up (workspaces, graph path)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        E, D, N = ham.td_propagate(xs, tk, dt_td, graph=graph, **laser)
+        el = max_over_ranks(time.perf_counter() - t0)
+        td[name] = {"steps_per_s": tk / el, "ms_per_step": el / tk * 1e3, "energy": E, "dipole": D}
+        del xs
+    e64, e32 = td["td_fp64_plain"].pop("energy"), td["td_fp32_graph"].pop("energy")
+    d64, d32 = td["td_fp64_plain"].pop("dipole"), td["td_fp32_graph"].pop("dipole")
+    td["fp32_vs_fp64"] = {"energy_rel_err_max": float(np.max(np.abs(e32 - e64) / np.abs(e64))),
+                          "dipole_abs_err_max": float(np.max(np.abs(d32 - d64))), "steps": tk, "dt": dt_td}
+
     # ---- e2e through the C ABI with pinned host buffers -----------------------
     xh = torch.from_numpy(sysm.psi).pin_memory()
     yh = torch.zeros((m.np, nst), dtype=torch.complex128).pin_memory()
@@ -330,6 +351,7 @@ def main():
                 "fp32_storage_hpsi": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps},
                 "taylor4_fp64": {"steps_per_s": tk / (ms_t64 / 1e3), "ms_per_step": ms_t64 / tk},
                 "taylor4_fp32": {"steps_per_s": tk / (ms_t32 / 1e3), "ms_per_step": ms_t32 / tk},
+                **td,
             },
         }
         if cpu:
