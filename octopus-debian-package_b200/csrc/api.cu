@@ -14,6 +14,7 @@
 #include "projector.cuh"
 #include "reduce.cuh"
 #include "stencil.cuh"
+#include "stencil_blk.cuh"
 
 namespace hpsi {
 
@@ -188,19 +189,44 @@ int pass_sc(int dtype, long long ld) {
   return 1;
 }
 
-PassShape default_shape(int dtype, long long ld) {
+// Shape of the cp.async pass (one complex state per thread, 16 x 16 tiles):
+// a thread keeps RY rows of 9 complex running sums, FP64 2 rows, FP32 4.
+PassShape legacy_shape(int dtype, long long ld) {
   const int sc = pass_sc(dtype, ld);
-  // a thread keeps RY rows of 9 complex running sums: FP64 2 rows, FP32 4
-  PassShape s = dtype == HPSI_C128 ? PassShape{sc, 16, 16, 2} : PassShape{sc, 16, 16, 4};
-  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb"
+  return dtype == HPSI_C128 ? PassShape{sc, 16, 16, 2} : PassShape{sc, 16, 16, 4};
+}
+
+// Shape of the register-blocked pass (one real lane per thread, 16 x 8 tiles).
+PassShape blk_shape(int dtype) {
+  // measured on the R = 12 bohr sphere (128 states): 512-thread blocks of
+  // FP64 2 x 2 and FP32 2 x 4 cells beat the 256-thread 2 x 4 / 4 x 4 ones
+  PassShape s = dtype == HPSI_C128 ? PassShape{blk_chunk_states<double>(), 16, 8, 2}
+                                   : PassShape{blk_chunk_states<float>(), 16, 8, 4};
+  s.blk = 1;
+  s.rx = 2;
+  s.unroll = dtype == HPSI_C128 ? 3 : 1;  // planes per unrolled group of the z march
+  return s;
+}
+
+PassShape default_shape(int dtype, long long ld) {
+  PassShape s = ld % blk_shape(dtype).sc == 0 ? blk_shape(dtype) : legacy_shape(dtype, ld);
+  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx"
   const char *env = std::getenv(dtype == HPSI_C128 ? "HPSI_PASS_SHAPE64" : "HPSI_PASS_SHAPE32");
   if (env) {
-    int a = 0, b = 0, c = 0, u = 0;
-    if (std::sscanf(env, "%d,%d,%d,%d", &a, &b, &c, &u) >= 2 && ld % a == 0) {
-      s.sc = a;
-      s.ry = b;
+    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0;
+    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x) >= 2 && a > 0 && ld % a == 0) {
+      if (t && ld % blk_shape(dtype).sc == 0) {
+        s = blk_shape(dtype);  // fixed chunk: block, z depth and group are taken
+        if (u == 1 || u == 3) s.unroll = u;
+        if (x > 0) s.rx = x;
+        if (b > 0) s.ry = b;
+      } else {
+        s = legacy_shape(dtype, ld);
+        s.sc = a;
+        s.ry = b;
+        s.unroll = u;
+      }
       s.zb = c;
-      s.unroll = u;
     }
   }
   return s;
@@ -342,6 +368,19 @@ hpsi_status hpsi_mesh_create(const hpsi_mesh_desc *d, hpsi_mesh **out) {
   }
   for (auto &t : m->tile_z)
     if (t.y >= 0) m->column_planes += t.y - t.x + 1;
+  m->tiles_y8 = 2 * m->tiles_y;
+  m->tile_z8.assign(size_t(m->tiles_x) * m->tiles_y8, make_int2(1 << 30, -1));
+  std::vector<int2> col_z(size_t(B.NX) * B.NY, make_int2(1 << 30, -(1 << 30)));
+  for (int i = 0; i < np; ++i) {
+    const int c = cell_of_row[i];
+    const int x = c % B.NX, y = (c / B.NX) % B.NY, z = c / (B.NX * B.NY);
+    int2 &t = m->tile_z8[size_t((y - HAL) / 8) * m->tiles_x + (x - HAL) / PASS_TILE];
+    t.x = std::min(t.x, z);
+    t.y = std::max(t.y, z);
+    int2 &cz = col_z[size_t(y) * B.NX + x];
+    cz.x = std::min(cz.x, z);
+    cz.y = std::max(cz.y, z);
+  }
   m->np = np;
   m->np_part = npp;
   m->order = ord;
@@ -365,6 +404,16 @@ hpsi_status hpsi_mesh_create(const hpsi_mesh_desc *d, hpsi_mesh **out) {
   };
   up(&m->d_cell_row, cell_row);
   up(&m->d_src_raw, cell_row);
+  if (s == HPSI_OK) {
+    s = dev_alloc(reinterpret_cast<void **>(&m->d_col_z), col_z.size() * sizeof(int2));
+    if (s == HPSI_OK) {
+      cudaError_t e = cudaMemcpy(m->d_col_z, col_z.data(), col_z.size() * sizeof(int2), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        set_error(cudaGetErrorString(e));
+        s = HPSI_ERR_CUDA;
+      }
+    }
+  }
   up(&m->d_src_zero, src_zero);
   up(&m->d_cell_of_row, cell_of_row);
   if (m->periodic) {
@@ -387,6 +436,7 @@ hpsi_status hpsi_mesh_destroy(hpsi_mesh *m) {
   dev_free(m->d_src_per);
   dev_free(m->d_per_inner);
   dev_free(m->d_cell_of_row);
+  dev_free(m->d_col_z);
   m->scratch.release();
   m->scratch2.release();
   for (auto &kv : m->items) dev_free(kv.second.first);
@@ -672,26 +722,33 @@ namespace hpsi {
 
 // z block depth of a pass: the largest depth that still gives about four
 // waves of CTAs (each block re-reads a 4-plane halo above and below).
-int choose_zb(const hpsi_mesh *m, int chunks) {
+// ty: tile height of the pass (16, or 8 for the blocked pass).
+int choose_zb(const hpsi_mesh *m, int chunks, int ty) {
   const long long want = 4LL * m->num_sms;
   const int cands[] = {1 << 20, 96, 64, 48, 32, 24, 16};
+  const auto &tz = ty == 8 ? m->tile_z8 : m->tile_z;
   for (int zb : cands) {
     long long n = 0;
-    for (auto &t : m->tile_z)
+    for (auto &t : tz)
       if (t.y >= 0) n += (t.y - t.x + zb) / zb;
     if (n * chunks >= want) return zb;
   }
   return 16;
 }
+int choose_zb(const hpsi_mesh *m, int chunks) { return choose_zb(m, chunks, 16); }
 
-// Work list {tile x, tile y, first plane, end plane} for a z block depth.
-hpsi_status mesh_items(hpsi_mesh *m, int zb, const int4 **items, int *nitems) {
-  auto it = m->items.find(zb);
+// Work list {tile x, tile y, first plane, end plane} for a z block depth and
+// tile height (16: 16 x 16 tiles, 8: 16 x 8 tiles, tile y in 8-row units).
+hpsi_status mesh_items(hpsi_mesh *m, int zb, int ty, const int4 **items, int *nitems) {
+  const int key = 2 * zb + (ty == 8 ? 1 : 0);
+  auto it = m->items.find(key);
   if (it == m->items.end()) {
     std::vector<int4> v;
-    for (int by = 0; by < m->tiles_y; ++by)
+    const int tyn = ty == 8 ? m->tiles_y8 : m->tiles_y;
+    const auto &tz = ty == 8 ? m->tile_z8 : m->tile_z;
+    for (int by = 0; by < tyn; ++by)
       for (int bx = 0; bx < m->tiles_x; ++bx) {
-        const int2 t = m->tile_z[size_t(by) * m->tiles_x + bx];
+        const int2 t = tz[size_t(by) * m->tiles_x + bx];
         if (t.y < 0) continue;
         for (int z = t.x; z <= t.y; z += zb) v.push_back(make_int4(bx, by, z, std::min(z + zb, t.y + 1)));
       }
@@ -699,11 +756,14 @@ hpsi_status mesh_items(hpsi_mesh *m, int zb, const int4 **items, int *nitems) {
     hpsi_status s = dev_alloc(reinterpret_cast<void **>(&d), std::max<size_t>(1, v.size()) * sizeof(int4));
     if (s) return s;
     if (!v.empty()) HPSI_TRY_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    it = m->items.emplace(zb, std::make_pair(d, int(v.size()))).first;
+    it = m->items.emplace(key, std::make_pair(d, int(v.size()))).first;
   }
   *items = it->second.first;
   *nitems = it->second.second;
   return HPSI_OK;
+}
+hpsi_status mesh_items(hpsi_mesh *m, int zb, const int4 **items, int *nitems) {
+  return mesh_items(m, zb, 16, items, nitems);
 }
 
 // Build the pass arguments shared by apply and Taylor passes.
@@ -714,6 +774,7 @@ void base_pass_args(const hpsi_hamiltonian *h, int terms, const int *src_map, Pa
   a.cell_src = src_map;
   a.cell_row = m->d_cell_row;
   a.per_inner = m->d_per_inner;
+  a.col_z = m->d_col_z;
   a.np = m->np;
   if ((terms & HPSI_TERM_KINETIC) && h->have_kinetic) {
     std::memcpy(a.wx, h->wx, sizeof(a.wx));
@@ -747,6 +808,8 @@ hpsi_status run_bra(hpsi_hamiltonian *h, const T *psi, long long ld, T *proj, cu
   p.map = h->d_map;
   p.pt = sizeof(T) == 8 ? static_cast<const void *>(h->d_pt) : static_cast<const void *>(h->d_pt_f);
   p.scal = sizeof(T) == 8 ? static_cast<const void *>(h->d_scal) : static_cast<const void *>(h->d_scal_f);
+  p.pt64 = h->d_pt;
+  p.scal64 = h->d_scal;
   p.psi = psi;
   p.psi_ld = ld;
   p.proj = proj;
@@ -754,9 +817,9 @@ hpsi_status run_bra(hpsi_hamiltonian *h, const T *psi, long long ld, T *proj, cu
   p.nprojections = h->nprojections;
   p.min_npoints = h->min_npoints;
   const int ksplit = bra_ksplit(p, h->mesh->num_sms);
-  hpsi_status s = h->bra_partial.ensure(size_t(ksplit) * h->nprojections * ld * 2 * sizeof(T));
+  hpsi_status s = h->bra_partial.ensure(size_t(ksplit) * h->nprojections * ld * 2 * sizeof(double));
   if (s) return s;
-  p.partial = h->bra_partial.ptr;
+  p.partial = static_cast<double *>(h->bra_partial.ptr);
   ProfScope prof(sizeof(T) == 8 ? "bra_fp64" : "bra_fp32", st);
   return launch_bra<T>(p, h->use_tensor_bra, ksplit, st);
 }
@@ -812,9 +875,26 @@ hpsi_status build_pass_args(hpsi_hamiltonian *h, int terms, const int *src_map, 
   a.a_re = a_re;
   a.a_im = a_im;
   a.chunks = int(ld / shape.sc);
-  a.zb = shape.zb > 0 ? shape.zb : choose_zb(h->mesh, a.chunks);
-  return mesh_items(h->mesh, a.zb, &a.items, &a.nitems);
+  const int ty = shape.blk ? 8 : 16;
+  a.zb = shape.zb > 0 ? shape.zb : choose_zb(h->mesh, a.chunks, ty);
+  return mesh_items(h->mesh, a.zb, ty, &a.items, &a.nitems);
 }
+
+// Rows of the tensor the input of a pass holds: the caller's boundary rows
+// are read only through the raw map; Taylor workspaces hold np rows.
+long long pass_in_rows(const hpsi_hamiltonian *h, const int *src_map) {
+  return src_map == h->mesh->d_src_raw ? h->mesh->np_part : h->mesh->np;
+}
+
+// Launch a pass with the kernel its shape names.
+template <typename T>
+hpsi_status launch_pass_any(const PassArgs &a, const PassShape &shape, long long in_rows, cudaStream_t st) {
+  (void)in_rows;
+  if (shape.blk) return launch_pass_blk<T>(a, shape.rx, shape.ry, shape.unroll, st);
+  return launch_pass<T>(a, shape, st);
+}
+template hpsi_status launch_pass_any<double>(const PassArgs &, const PassShape &, long long, cudaStream_t);
+template hpsi_status launch_pass_any<float>(const PassArgs &, const PassShape &, long long, cudaStream_t);
 
 // One fused pass with its KB bra before and ket after.
 template <typename T>
@@ -822,10 +902,22 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
                      long long out_ld, long long ld, int mode, const T *psi0, long long psi0_ld, double a_re,
                      double a_im, double *obs_partial, int *ncta_out, cudaStream_t st) {
   PassArgs a;
-  const PassShape shape = pass_shape(h, sizeof(T) == 8 ? HPSI_C128 : HPSI_C64, ld);
+  const int dtype = sizeof(T) == 8 ? HPSI_C128 : HPSI_C64;
+  PassShape shape = pass_shape(h, dtype, ld);
   hpsi_status si = build_pass_args<T>(h, terms, src_map, in, in_ld, out, out_ld, ld, mode, psi0, psi0_ld, a_re,
                                       a_im, shape, a);
   if (si) return si;
+  if (shape.blk) {
+    PassArgs chk = a;
+    if (obs_partial) chk.obs = obs_partial;
+    if (obs_partial && !psi0) chk.psi0 = in, chk.psi0_ld = in_ld;
+    if (!blk_pass_eligible<T>(chk, ld)) {
+      shape = legacy_shape(dtype, ld);
+      si = build_pass_args<T>(h, terms, src_map, in, in_ld, out, out_ld, ld, mode, psi0, psi0_ld, a_re, a_im, shape,
+                              a);
+      if (si) return si;
+    }
+  }
   const bool nl = (terms & HPSI_TERM_NON_LOCAL_POTENTIAL) && h->nmat > 0;
   if (nl) {
     const size_t pbytes = size_t(h->nprojections) * ld * 2 * sizeof(T);
@@ -842,7 +934,7 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
   if (obs_partial && !psi0) a.psi0 = in, a.psi0_ld = in_ld;
   {
     ProfScope prof(sizeof(T) == 8 ? "pass_fp64" : "pass_fp32", st);
-    hpsi_status s = launch_pass<T>(a, shape, st);
+    hpsi_status s = launch_pass_any<T>(a, shape, pass_in_rows(h, src_map), st);
     if (s) return s;
   }
   if (nl) {
@@ -886,8 +978,12 @@ size_t obs_partial_bytes(hpsi_hamiltonian *h, long long ld) {
     const PassShape sh = pass_shape(h, dt, ld);
     const int4 *items;
     int nitems = 0;
-    const int zb = sh.zb > 0 ? sh.zb : choose_zb(h->mesh, int(ld / sh.sc));
-    if (mesh_items(h->mesh, zb, &items, &nitems) == HPSI_OK)
+    const int ty = sh.blk ? 8 : 16;
+    const int zb = sh.zb > 0 ? sh.zb : choose_zb(h->mesh, int(ld / sh.sc), ty);
+    if (mesh_items(h->mesh, zb, ty, &items, &nitems) == HPSI_OK)
+      n = std::max(n, size_t(nitems));
+    const PassShape lg = legacy_shape(dt, ld);
+    if (mesh_items(h->mesh, choose_zb(h->mesh, int(ld / lg.sc)), &items, &nitems) == HPSI_OK)
       n = std::max(n, size_t(nitems));
   }
   return std::max<size_t>(n, 1) * ld * 6 * sizeof(double);

@@ -47,11 +47,14 @@ struct hpsi_mesh {
   int *d_cell_of_row = nullptr;
   int device = 0, num_sms = 148;
   hpsi::Workspace scratch, scratch2, stage_in, stage_out;
-  // z range {first, last} (cells) of the inner points of each 16x16 tile column
-  int tiles_x = 0, tiles_y = 0;
-  std::vector<int2> tile_z;
+  // z range {first, last} (cells) of the inner points of each 16x16 tile
+  // column, and of each 16x8 tile column (the blocked pass)
+  int tiles_x = 0, tiles_y = 0, tiles_y8 = 0;
+  std::vector<int2> tile_z, tile_z8;
   long long column_planes = 0;          // sum of the tile z extents
-  std::map<int, std::pair<int4 *, int>> items;  // work list per z block depth
+  // work list per (z block depth, tile height): key 2 * zb + (height == 8)
+  std::map<int, std::pair<int4 *, int>> items;
+  int2 *d_col_z = nullptr;  // per (y, x) cell column: z range of its inner points
 };
 
 struct hpsi_hamiltonian {

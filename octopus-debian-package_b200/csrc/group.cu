@@ -98,6 +98,8 @@ static hpsi_status group_build(hpsi_group *g, int dtype, const std::vector<long 
     }
     g->shapes[s].sc = sc;
     g->shapes[s].ry = dtype == HPSI_C128 ? 2 : 4;
+    g->shapes[s].tx = g->shapes[s].ty = 16;
+    g->shapes[s].blk = 0;  // the persistent group kernel is the one-complex-per-thread pass
   }
   g->sc = sc;
   for (int first = 0; first < n; first += GROUP_MAX) {

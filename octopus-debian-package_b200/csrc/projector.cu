@@ -7,11 +7,12 @@
 // covered row after the stencil pass: one thread per output element, so no
 // write races and no colouring are needed.
 //
-// FP64: the contraction runs on the FP64 tensor cores (DMMA,
-// mma.sync.m8n8k4.f64): M = 8 real lanes per warp, N = 8 projectors per
-// tile, K = 4 sphere points per step, with the gathered rows and the
-// projector block staged in shared memory by cp.async.  FP32 uses the SIMT
-// kernel below (also used as the FP64 cross-check).
+// The contraction runs on the FP64 tensor cores (DMMA,
+// mma.sync.m8n8k4.f64) for both storage types: M = 8 real lanes per warp,
+// N = 8 projectors per tile, K = 4 sphere points per step, with the gathered
+// rows and the projector block staged in shared memory by cp.async.  The SIMT
+// kernel below serves matrices with more than 16 projectors and is the
+// cross-check of the tensor path.
 #include <algorithm>
 #include <type_traits>
 
@@ -34,9 +35,15 @@ __device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, do
 
 // grid: (nmat, ld2 / LANES, ksplit); block: 128 threads (4 warps x 8 lanes
 // each).  Split z sums sphere points [z*npts/ksplit, (z+1)*npts/ksplit) into
-// partial[z] (unscaled); bra_reduce_kernel adds the splits and applies scal.
+// partial[z] (unscaled, FP64); bra_reduce_kernel adds the splits and applies
+// scal.  T is the storage type of psi: FP32 rows are staged as stored and
+// widened to FP64 when the A fragment is read, so both precisions contract
+// in FP64 against the FP64 projector values.
+template <typename T>
 __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
-  __shared__ __align__(16) double sA[2][KB][APAD];
+  constexpr int AP = sizeof(T) == 8 ? APAD : 40;  // 40 floats: conflict-free fragment reads
+  constexpr int CPR = LANES * int(sizeof(T)) / 16;  // 16-byte copies per staged row
+  __shared__ __align__(16) T sA[2][KB][AP];
   __shared__ __align__(16) double sB[2][KB][NMAX];
   const int m = blockIdx.x;
   const int l0 = blockIdx.y * LANES;
@@ -45,23 +52,21 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
   const int kend = int((long long)md.x * (blockIdx.z + 1) / gridDim.z);
   const int npts = kend - kbeg, npr = md.y;
   const int *map = p.map + md.z + kbeg;
-  const double *pt = static_cast<const double *>(p.pt) + md.w + (long long)kbeg * npr;
-  const double *psi = static_cast<const double *>(p.psi);
+  const double *pt = p.pt64 + md.w + (long long)kbeg * npr;
+  const T *psi = static_cast<const T *>(p.psi);
   const long long ld2 = 2 * p.psi_ld;
   const int tid = threadIdx.x, warp = tid >> 5, ln = tid & 31;
+  constexpr int EPC = 16 / int(sizeof(T));  // elements per 16-byte copy
 
   auto stage = [&](int k0, int b) {
-    // psi rows: KB points x 32 lanes = KB*8 copies of 16 bytes
-    for (int i = tid; i < KB * 8; i += 128) {
-      const int k = i >> 3, part = i & 7;
-      double *d = &sA[b][k][part * 4];
+    for (int i = tid; i < KB * CPR; i += 128) {
+      const int k = i / CPR, part = i % CPR;
+      T *d = &sA[b][k][part * EPC];
       if (k0 + k < npts) {
         const int row = __ldg(map + k0 + k);
-        const double *g = psi + row * ld2 + l0 + part * 4;
-        cp_async16(d, g);
-        cp_async16(d + 2, g + 2);
+        cp_async16(d, psi + row * ld2 + l0 + part * EPC);
       } else {
-        d[0] = d[1] = d[2] = d[3] = 0.0;
+        *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
       }
     }
     for (int i = tid; i < KB * NMAX; i += 128) {
@@ -82,7 +87,7 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < KB; kk += 4) {
-      const double a = sA[b][kk + (ln & 3)][warp * 8 + (ln >> 2)];
+      const double a = double(sA[b][kk + (ln & 3)][warp * 8 + (ln >> 2)]);
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt) {
         const double bb = sB[b][kk + (ln & 3)][nt * 8 + (ln >> 2)];
@@ -93,8 +98,7 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
   }
   // C fragment: row (lane) = ln >> 2, cols (projectors) = (ln & 3) * 2 + {0,1}
   const int lane = l0 + warp * 8 + (ln >> 2);
-  double *out = static_cast<double *>(p.partial) +
-                ((long long)blockIdx.z * p.nprojections + p.proj_row[m]) * 2 * p.proj_ld;
+  double *out = p.partial + ((long long)blockIdx.z * p.nprojections + p.proj_row[m]) * 2 * p.proj_ld;
 #pragma unroll
   for (int nt = 0; nt < 2; ++nt) {
     const int j0 = nt * 8 + (ln & 3) * 2;
@@ -103,17 +107,17 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
   }
 }
 
-// proj[j][l] = scal[j] * sum_z partial[z][j][l]  (one thread per real lane)
+// proj[j][l] = scal[j] * sum_z partial[z][j][l]  (one thread per real lane;
+// FP64 sums, rounded once to the storage type)
 template <typename T>
 __global__ void bra_reduce_kernel(const ProjArgs p, int ksplit) {
   const long long n = (long long)p.nprojections * 2 * p.proj_ld;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int j = int(i / (2 * p.proj_ld));
-  const T *part = static_cast<const T *>(p.partial);
-  T acc = T(0);
-  for (int z = 0; z < ksplit; ++z) acc += part[(long long)z * n + i];
-  static_cast<T *>(p.proj)[i] = acc * static_cast<const T *>(p.scal)[j];
+  double acc = 0.0;
+  for (int z = 0; z < ksplit; ++z) acc += p.partial[(long long)z * n + i];
+  static_cast<T *>(p.proj)[i] = T(acc * p.scal64[j]);
 }
 
 // SIMT bra: grid (nmat, ceil(ld2/32)); block 128 = 32 lanes x 4 point groups
@@ -169,16 +173,14 @@ template <typename T>
 hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStream_t st) {
   if (p.nmat == 0) return HPSI_OK;
   const long long ld2 = 2 * p.psi_ld;
-  if constexpr (sizeof(T) == 8) {
-    if (use_tensor && p.max_nproj <= NMAX && ld2 % LANES == 0) {
-      dim3 grid(p.nmat, unsigned(ld2 / LANES), ksplit);
-      bra_dmma_kernel<<<grid, 128, 0, st>>>(p);
-      HPSI_CHECK_LAUNCH();
-      const long long n = (long long)p.nprojections * ld2;
-      bra_reduce_kernel<T><<<unsigned((n + 255) / 256), 256, 0, st>>>(p, ksplit);
-      HPSI_CHECK_LAUNCH();
-      return HPSI_OK;
-    }
+  if (use_tensor && p.max_nproj <= NMAX && ld2 % LANES == 0) {
+    dim3 grid(p.nmat, unsigned(ld2 / LANES), ksplit);
+    bra_dmma_kernel<T><<<grid, 128, 0, st>>>(p);
+    HPSI_CHECK_LAUNCH();
+    const long long n = (long long)p.nprojections * ld2;
+    bra_reduce_kernel<T><<<unsigned((n + 255) / 256), 256, 0, st>>>(p, ksplit);
+    HPSI_CHECK_LAUNCH();
+    return HPSI_OK;
   }
   if (p.max_nproj > 32) {
     set_error("projector matrices with more than 32 projectors are not supported");

@@ -13,13 +13,15 @@ struct ProjArgs {
   const int *map;        // sphere point -> mesh row
   const void *pt;        // projector values, projector index fastest per point
   const void *scal;      // per projector scale (storage type)
+  const double *pt64;    // the projector values in FP64 (tensor-core path)
+  const double *scal64;  // the scales in FP64
   const void *psi;       // batch
   long long psi_ld;
   void *proj;            // projections [nprojections][proj_ld] complex
   long long proj_ld;
   int nprojections;
   int min_npoints;       // smallest sphere (bounds the K split)
-  void *partial;         // split-K partials [ksplit][nprojections][proj_ld] complex
+  double *partial;       // split-K partials [ksplit][nprojections][proj_ld] complex, FP64
 };
 
 struct KetArgs {

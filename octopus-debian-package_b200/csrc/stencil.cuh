@@ -42,6 +42,7 @@ struct PassArgs {
   int obs_ld;
   double obs_pol[3];      // dipole direction
 
+  const int2 *col_z;      // per (y, x) cell column: {first, last} z of its inner points
   const int4 *items;      // work items {tile x, tile y, first plane, end plane}
   int nitems;
   int chunks;             // state chunks per item (ld / SC)
@@ -54,6 +55,8 @@ struct PassShape {
   int tx, ty, ry;
   int zb = 0;  // output planes per work item (0: chosen from the wave count)
   int unroll = 0;  // 1: nine-plane unrolled ring, 0: switch-selected ring
+  int blk = 0;     // 1: register-blocked real-lane pass (sc = its chunk, tiles 16 x 8)
+  int rx = 0;      // blocked pass: cells per thread along x (ry along y)
 };
 
 // Launch the fused pass for a storage type (double -> FP64, float -> FP32).

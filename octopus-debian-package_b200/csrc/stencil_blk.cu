@@ -1,0 +1,501 @@
+// Fused H.psi stencil pass with register-blocked real lanes (sm_100a).
+//
+// Same arithmetic and pass modes as the one-complex-per-thread pass in
+// stencil.cu, with a division of work that cuts shared-memory reads per
+// output: a CTA of 256 threads owns a 16 x 8 cell tile and one chunk of
+// 128 bytes of every cell row (FP64 8 complex states, FP32 16); each thread
+// owns one real lane (the re or im part of one state) of an RX x RY block of
+// cells (FP64 2 x 4, FP32 4 x 4) and keeps nine running z sums per cell in
+// registers.  Per output it reads 1 + 8/RX + 8/RY values from shared memory
+// (7 FP64, 5 FP32) instead of 13 double2.  The Horner update takes the other
+// part of h = (H u)(r) from the neighbouring lane by one shuffle.
+//
+// Halo planes (24 x 16 cells) are gathered through the load map into an
+// NBUF-deep ring with 16-byte cp.async copies (eight threads per 128-byte cell
+// chunk, so every warp copies four whole chunks); zero-boundary cells are
+// stored as zeros and Bloch-phase images are multiplied on load.  The load
+// map of each plane and the output rows four planes below travel in a side
+// ring two stage rounds ahead of the data, so every gather knows its rows
+// when it is issued.  One __syncthreads per plane.
+//
+// A TMA tile::gather4 fill of the same 128-byte chunks (one producer warp,
+// mbarrier hand-over) was measured 3x slower than this form on the same
+// tiles: the bulk-copy engine does not keep enough 128-byte requests in
+// flight per SM, while 256 threads issuing cp.async do.
+//
+// Reference semantics as in stencil.cu: X(nl_operator_operate_batch)
+// (src/grid/nl_operator_inc.F90:21-130), the local potential
+// (src/hamiltonian/hamiltonian_elec_base_inc.F90:233-242) and the Taylor
+// axpys (src/electrons/exponential.F90:738-746).
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+
+#include "stencil.cuh"
+#include "stencil_blk.cuh"
+
+namespace hpsi {
+
+namespace {
+
+// Lanes of one cell chunk: 128 bytes (FP64 16 = 8 complex states, FP32 32).
+template <typename T>
+constexpr int blk_lanes() {
+  return 128 / int(sizeof(T));
+}
+
+template <typename T, bool X0, int RX_, int RY_>
+struct BlkLayout {
+  static constexpr int SL = blk_lanes<T>(), RX = RX_, RY = RY_;
+  static constexpr int TX = BLK_TILE_X, TY = BLK_TILE_Y, HAL = 4;
+  static constexpr int HX = TX + 2 * HAL, HY = TY + 2 * HAL;
+  static constexpr int HC = HX * HY, IC = TX * TY;
+  static constexpr int CELLB = SL * int(sizeof(T));  // bytes of one cell chunk
+  static constexpr int PCS = CELLB / 16;             // 16-byte pieces per cell chunk
+  static constexpr int EPP = 16 / int(sizeof(T));    // elements per piece
+  static_assert(CELLB == 128, "one cell chunk is 128 bytes");
+  static constexpr int NT = SL * (TX / RX) * (TY / RY);
+  static_assert(NT == 256 || NT == 512, "256 or 512 threads");
+  static_assert((HC * PCS) % NT == 0 && (IC * PCS) % NT == 0, "copy rounds tile the threads");
+  static constexpr int HROUNDS = HC * PCS / NT, IROUNDS = IC * PCS / NT;
+  static constexpr int NBUF = X0 ? 3 : 4;   // data stages
+  static constexpr int NSIDE = 2 * NBUF - 1;  // side slots (issued 2 NBUF - 2 planes ahead)
+  static constexpr int SIDE_AHEAD = 2 * NBUF - 2;
+  // data stage: halo plane, psi0 rows of the output plane, potential
+  static constexpr size_t o_psi0 = size_t(HC) * CELLB;
+  static constexpr size_t o_v = o_psi0 + (X0 ? size_t(IC) * CELLB : 0);
+  static constexpr size_t STAGE = o_v + size_t(IC) * sizeof(double);
+  // side slot: load map of the halo plane, rows of the output plane 4 below
+  static constexpr size_t s_rows = size_t(HC) * sizeof(int);
+  static constexpr size_t SIDEB = s_rows + size_t(IC) * sizeof(int);
+  static constexpr size_t o_side = NBUF * STAGE;
+  static constexpr size_t bytes = o_side + NSIDE * SIDEB;
+  static_assert(bytes <= 232448, "shared memory per CTA");
+  static_assert(STAGE % 16 == 0 && SIDEB % 16 == 0, "16-byte copies");
+  static constexpr int NMAPP = HC / 4, NROWP = IC / 4, NVP = IC / 2;  // 16-byte side/v pieces
+  static_assert(NMAPP + NROWP <= NT && NVP <= NT, "one side piece per thread");
+};
+
+template <typename T>
+__device__ __forceinline__ T wsel_t(const double *d, const float *f, int k);
+template <>
+__device__ __forceinline__ double wsel_t<double>(const double *d, const float *, int k) {
+  return d[k];
+}
+template <>
+__device__ __forceinline__ float wsel_t<float>(const double *, const float *f, int k) {
+  return f[k];
+}
+
+__device__ __forceinline__ void zero16(void *d) {
+  *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// grid: nitems (16 x 8 tiles x z blocks) * chunks.
+// Plane k of a CTA is halo plane zbeg + k: data stage k % NBUF, side slot
+// k % NSIDE.  Iteration k computes plane k and issues the data of plane
+// k + NBUF - 1 and the side data of plane k + 2 NBUF - 2 (one commit group).
+template <typename T, bool HORNER, bool OBS, int U, int RX_, int RY_>
+__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
+    pass_blk_kernel(const __grid_constant__ PassArgs p) {
+  constexpr bool X0 = HORNER || OBS;
+  using LY = BlkLayout<T, X0, RX_, RY_>;
+  constexpr int SL = LY::SL, RX = LY::RX, RY = LY::RY, TX = LY::TX, TY = LY::TY, HAL = LY::HAL;
+  constexpr int HX = LY::HX, NBUF = LY::NBUF, NSIDE = LY::NSIDE, PCS = LY::PCS, EPP = LY::EPP;
+  extern __shared__ __align__(16) unsigned char smem[];
+
+  const CellBox &B = p.box;
+  const int chunk = blockIdx.x % p.chunks;
+  const int ih = blockIdx.x / p.chunks;  // work item (16 x 8 tile, z block)
+  const int4 it = p.items[ih];
+  const int cx0 = HAL + it.x * TX, cy0 = HAL + it.y * TY;
+  const int zs = it.z, ze = it.w;
+  const int zbeg = zs - HAL, nplanes = ze - zs + 2 * HAL;
+  const long long planeN = (long long)B.NX * B.NY;
+  const int tid = threadIdx.x;
+  const int col = chunk * SL;
+
+  auto stage = [&](int k) { return smem + size_t(k % NBUF) * LY::STAGE; };
+  auto side = [&](int k) { return smem + LY::o_side + size_t(k % NSIDE) * LY::SIDEB; };
+
+  // ---- copy roles ---------------------------------------------------------------
+  const int cpc = tid / PCS, piece = tid % PCS;  // cell (+ 32 per round) and 16-byte piece
+  const T *in_base = static_cast<const T *>(p.in) + col + piece * EPP;
+  const long long in_ld2 = 2 * p.in_ld;
+  const T *x0_base = static_cast<const T *>(p.psi0) + col + piece * EPP;
+  const long long x0_ld2 = 2 * p.psi0_ld;
+  // side piece of this thread: map cells 4t..4t+3 (t < NMAPP), or rows cells
+  long long side_src = 0;
+  int side_dst = -1, side_kind = 0;  // 1 map, 2 rows
+  if (tid < LY::NMAPP) {
+    const int c = 4 * tid, hy = c / HX, hx = c % HX;
+    side_kind = 1;
+    side_dst = c;
+    side_src = (long long)(cy0 - HAL + hy) * B.NX + cx0 - HAL + hx;
+  } else if (tid < LY::NMAPP + LY::NROWP) {
+    const int c = 4 * (tid - LY::NMAPP);
+    side_kind = 2;
+    side_dst = c;
+    side_src = (long long)(cy0 + c / TX) * B.NX + cx0 + c % TX;
+  }
+  const int vc = 2 * tid;  // potential cells of this thread (tid < NVP)
+  const long long v_src = (long long)(cy0 + vc / TX) * B.NX + cx0 + vc % TX;
+
+  // side data of plane k (map of plane zbeg+k, rows of plane zbeg+k-4)
+  auto issue_side = [&](int k) {
+    if (k >= nplanes || side_kind == 0) return;
+    unsigned char *sd = side(k);
+    const int q = zbeg + k;
+    if (side_kind == 1) {
+      cp_async16(reinterpret_cast<int *>(sd) + side_dst, p.cell_src + q * planeN + side_src);
+    } else {
+      int *d = reinterpret_cast<int *>(sd + LY::s_rows) + side_dst;
+      if (q - HAL >= zs)
+        cp_async16(d, p.cell_row + (q - HAL) * planeN + side_src);
+      else
+        *reinterpret_cast<int4 *>(d) = make_int4(-1, -1, -1, -1);
+    }
+  };
+  // data of plane k: halo through the map, psi0 of the output plane, potential
+  auto issue_data = [&](int k) {
+    if (k >= nplanes) return;
+    unsigned char *st = stage(k);
+    const unsigned char *sd = side(k);
+    const int *map = reinterpret_cast<const int *>(sd);
+    T *halo = reinterpret_cast<T *>(st) + piece * EPP;
+#pragma unroll 1
+    for (int j = 0; j < LY::HROUNDS; ++j) {
+      const int cell = cpc + j * (LY::NT / PCS);
+      const int src = map[cell];
+      T *d = halo + cell * SL;
+      if (src >= 0) {
+        cp_async16(d, in_base + src * in_ld2);
+      } else if (src == -1) {
+        zero16(d);
+      } else {
+        // periodic image times the Bloch phase correction
+        const int b = -(src + 2);
+        const T *g = in_base + __ldg(p.per_inner + b) * in_ld2;
+        const T pr = static_cast<const T *>(p.phase_corr)[2 * b];
+        const T pi = static_cast<const T *>(p.phase_corr)[2 * b + 1];
+#pragma unroll
+        for (int e = 0; e < EPP; e += 2) {
+          const T xr = g[e], xi = g[e + 1];
+          d[e] = xr * pr - xi * pi;
+          d[e + 1] = xr * pi + xi * pr;
+        }
+      }
+    }
+    const int q = zbeg + k;
+    if (X0 && q - HAL >= zs) {
+      const int *rows = reinterpret_cast<const int *>(sd + LY::s_rows);
+      T *x0 = reinterpret_cast<T *>(st + LY::o_psi0) + piece * EPP;
+#pragma unroll
+      for (int j = 0; j < LY::IROUNDS; ++j) {
+        const int cell = cpc + j * (LY::NT / PCS);
+        const int row = rows[cell];
+        if (row >= 0 && row < p.np) cp_async16(x0 + cell * SL, x0_base + row * x0_ld2);
+      }
+    }
+    if (tid < LY::NVP) {
+      double *vd = reinterpret_cast<double *>(st + LY::o_v) + vc;
+      if (p.v_cell)
+        cp_async16(vd, p.v_cell + q * planeN + v_src);
+      else
+        zero16(vd);
+    }
+  };
+
+  // ---- prologue: side data of planes 0..NBUF-2 synchronously, then the first
+  // NBUF-1 groups (data of planes 0..NBUF-2, side of planes NBUF-1..2NBUF-3)
+  for (int k = 0; k < NBUF - 1 && k < nplanes; ++k) {
+    unsigned char *sd = side(k);
+    const int q = zbeg + k;
+    for (int i = tid; i < LY::HC; i += LY::NT) {
+      const int hy = i / HX, hx = i % HX;
+      reinterpret_cast<int *>(sd)[i] = __ldg(p.cell_src + q * planeN + (long long)(cy0 - HAL + hy) * B.NX + cx0 - HAL + hx);
+    }
+    for (int i = tid; i < LY::IC; i += LY::NT)
+      reinterpret_cast<int *>(sd + LY::s_rows)[i] =
+          q - HAL >= zs ? __ldg(p.cell_row + (q - HAL) * planeN + (long long)(cy0 + i / TX) * B.NX + cx0 + i % TX)
+                        : -1;
+  }
+  __syncthreads();
+  for (int k = 0; k < NBUF - 1; ++k) {
+    issue_data(k);
+    issue_side(k + NBUF - 1);
+    cp_async_commit();
+  }
+
+  // ---- compute roles --------------------------------------------------------------
+  const int lane = tid & 31;
+  const int l = tid % SL;
+  const int g = tid / SL;
+  const int bx = (g % (TX / RX)) * RX, by = (g / (TX / RX)) * RY;
+  const double fscale = p.fld_scale_dev ? *p.fld_scale_dev : 1.0;
+  const double fz = p.fld[2] * fscale * B.h[2];
+  const double fx0 = fscale * p.fld[0] * B.h[0], fy0 = fscale * p.fld[1] * B.h[1];
+  const double fxy0 = fx0 * double(cx0 + bx + B.lo[0]) + fy0 * double(cy0 + by + B.lo[1]);
+  const T are = static_cast<T>(p.a_re), aim = static_cast<T>(p.a_im);
+  const bool odd = (l & 1) != 0;
+  T *out = static_cast<T *>(p.out);
+  const long long out_ld2 = 2 * p.out_ld;
+  const int ocol = col + l;
+  Kahan ke = {0, 0}, kn = {0, 0}, kd = {0, 0};
+  (void)lane;
+
+  // z range of the inner points under this thread's cells: planes more than
+  // 4 away from it feed no output of the block and are skipped
+  int gz0 = 1 << 30, gz1 = -(1 << 30);
+#pragma unroll
+  for (int r = 0; r < RY; ++r)
+#pragma unroll
+    for (int cx = 0; cx < RX; ++cx) {
+      const int2 cz = __ldg(p.col_z + (long long)(cy0 + by + r) * B.NX + cx0 + bx + cx);
+      gz0 = min(gz0, cz.x);
+      gz1 = max(gz1, cz.y);
+    }
+
+  T acc[RX][RY][9];
+#pragma unroll
+  for (int cx = 0; cx < RX; ++cx)
+#pragma unroll
+    for (int r = 0; r < RY; ++r)
+#pragma unroll
+      for (int j = 0; j < 9; ++j) acc[cx][r][j] = T(0);
+
+  // one plane.  The running sums of a group of U planes sit in static slots:
+  // plane K of the group adds its centre to slot (4 + K) % 9 and emits slot K;
+  // after the group the nine slots rotate by U (U = 9 would need no rotation
+  // but unrolls nine planes of code, more than the instruction cache holds).
+  auto plane = [&](auto Kc, int k) {
+    constexpr int K = decltype(Kc)::value;
+    constexpr int S4 = (4 + K) % 9;  // running sum of output plane zbeg + k
+    cp_async_wait<NBUF - 2>();
+    __syncthreads();
+    issue_data(k + NBUF - 1);
+    issue_side(k + LY::SIDE_AHEAD);
+    cp_async_commit();
+
+    const unsigned char *st = stage(k);
+    const T *P = reinterpret_cast<const T *>(st) + l;
+    const double *vs = reinterpret_cast<const double *>(st + LY::o_v);
+    const int pz = zbeg + k;
+    const double vz = fz * double(pz + B.lo[2]);
+
+    if (pz >= gz0 - HAL && pz <= gz1 + HAL) {
+      // rows of the owned columns: y arms of every owned cell; the owned
+      // cells themselves carry the centre (+ potential), the z arms and the x
+      // arms of their siblings.  Columns innermost: consecutive multiply-adds
+      // go to different running sums.
+#pragma unroll
+      for (int i = 0; i < RY + 8; ++i) {
+#pragma unroll
+        for (int cx = 0; cx < RX; ++cx) {
+          const T val = P[((by + i) * HX + bx + cx + HAL) * SL];
+#pragma unroll
+          for (int r = 0; r < RY; ++r) {
+            const int d = i - r;
+            if (d < 0 || d > 8) continue;
+            if (d != 4) {
+              acc[cx][r][S4] = fma(wsel_t<T>(p.wy, p.wyf, d), val, acc[cx][r][S4]);
+              continue;
+            }
+            const double vv = vs[(by + r) * TX + bx + cx] + fxy0 + fx0 * double(cx) + fy0 * double(r) + vz;
+            acc[cx][r][S4] = fma(wsel_t<T>(p.wx, p.wxf, 4) + static_cast<T>(vv), val, acc[cx][r][S4]);
+#pragma unroll
+            for (int c2 = 0; c2 < RX; ++c2)
+              if (c2 != cx) acc[c2][r][S4] = fma(wsel_t<T>(p.wx, p.wxf, cx - c2 + 4), val, acc[c2][r][S4]);
+#pragma unroll
+            for (int j = 0; j < 9; ++j)
+              if (j != 4)
+                acc[cx][r][(j + K) % 9] = fma(wsel_t<T>(p.wz, p.wzf, 8 - j), val, acc[cx][r][(j + K) % 9]);
+          }
+        }
+      }
+      // x arms from outside the owned block (rows innermost)
+#pragma unroll
+      for (int dx = -4; dx < RX + 4; ++dx) {
+        if (dx >= 0 && dx < RX) continue;
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+          const T val = P[((by + r + HAL) * HX + bx + dx + HAL) * SL];
+#pragma unroll
+          for (int cx = 0; cx < RX; ++cx) {
+            const int dd = dx - cx;
+            if (dd < -4 || dd > 4) continue;
+            acc[cx][r][S4] = fma(wsel_t<T>(p.wx, p.wxf, dd + 4), val, acc[cx][r][S4]);
+          }
+        }
+      }
+    }
+
+    // outputs of plane zo = pz - 4 are complete (slot K)
+    const int zo = pz - HAL;
+    if (zo >= zs) {
+      const int *rows = reinterpret_cast<const int *>(side(k) + LY::s_rows);
+      const T *x0s = reinterpret_cast<const T *>(st + LY::o_psi0) + l;
+#pragma unroll
+      for (int cx = 0; cx < RX; ++cx)
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+          const int cell = (by + r) * TX + bx + cx;
+          const T h = acc[cx][r][K];
+          acc[cx][r][K] = T(0);
+          T val = h;
+          if constexpr (HORNER) {
+            const T hp = __shfl_xor_sync(0xffffffffu, h, 1);  // the other part of this state
+            const T x0 = x0s[cell * SL];
+            val = odd ? x0 + are * h + aim * hp : x0 + are * h - aim * hp;
+          }
+          const int row = rows[cell];
+          if (row < 0 || row >= p.np) continue;
+          if constexpr (OBS) {
+            const double x0 = double(x0s[cell * SL]);
+            const double rr = p.obs_pol[0] * B.h[0] * double(cx0 + bx + cx + B.lo[0]) +
+                              p.obs_pol[1] * B.h[1] * double(cy0 + by + r + B.lo[1]) +
+                              p.obs_pol[2] * B.h[2] * double(zo + B.lo[2]);
+            kadd(ke, x0 * double(h));
+            kadd(kn, x0 * x0);
+            kadd(kd, x0 * x0 * rr);
+          }
+          out[row * out_ld2 + ocol] = val;
+        }
+    } else {
+#pragma unroll
+      for (int cx = 0; cx < RX; ++cx)
+#pragma unroll
+        for (int r = 0; r < RY; ++r) acc[cx][r][K] = T(0);
+    }
+  };
+
+  auto rotate = [&]() {
+#pragma unroll
+    for (int cx = 0; cx < RX; ++cx)
+#pragma unroll
+      for (int r = 0; r < RY; ++r) {
+        T t[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) t[j] = acc[cx][r][(j + U) % 9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) acc[cx][r][j] = t[j];
+      }
+  };
+
+#pragma unroll 1
+  for (int k = 0; k < nplanes; k += U) {
+    plane(std::integral_constant<int, 0>{}, k);
+    if constexpr (U > 1)
+      if (k + 1 < nplanes) plane(std::integral_constant<int, (U > 1 ? 1 : 0)>{}, k + 1);
+    if constexpr (U > 2)
+      if (k + 2 < nplanes) plane(std::integral_constant<int, (U > 2 ? 2 : 0)>{}, k + 2);
+    if constexpr (U % 9 != 0) rotate();
+  }
+  static_assert(U >= 1 && U <= 3, "group of 1..3 planes");
+  cp_async_wait<0>();
+
+  if constexpr (OBS) {
+    // per-state sums over the threads of this chunk; the two lanes of a state
+    // fold into one entry
+    __syncthreads();
+    double *red = reinterpret_cast<double *>(smem);  // threads x 6
+    {
+      double *o = red + tid * 6;
+      o[0] = ke.s;
+      o[1] = ke.c;
+      o[2] = kn.s;
+      o[3] = kn.c;
+      o[4] = kd.s;
+      o[5] = kd.c;
+    }
+    __syncthreads();
+    if (tid < SL / 2) {
+      Kahan a[3] = {{0, 0}, {0, 0}, {0, 0}};
+      for (int t = 2 * tid; t < LY::NT; t += SL)
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            kadd(a[c], red[(t + q) * 6 + 2 * c]);
+            a[c].c += red[(t + q) * 6 + 2 * c + 1];
+          }
+      double *o = p.obs + ((long long)ih * p.obs_ld + chunk * (SL / 2) + tid) * 6;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        o[2 * c] = a[c].s;
+        o[2 * c + 1] = a[c].c;
+      }
+    }
+  }
+}
+
+template <typename T, bool HORNER, bool OBS, int U, int RX, int RY>
+hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
+  using LY = BlkLayout<T, HORNER || OBS, RX, RY>;
+  auto kern = pass_blk_kernel<T, HORNER, OBS, U, RX, RY>;
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [&] {
+    attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LY::bytes));
+  });
+  HPSI_TRY_CUDA(attr);
+  const unsigned nblocks = unsigned(a.nitems) * unsigned(a.chunks);
+  kern<<<nblocks, LY::NT, LY::bytes, st>>>(a);
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+
+template <typename T, int U, int RX, int RY>
+hpsi_status launch_blk_u(const PassArgs &a, cudaStream_t st) {
+  const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr;
+  if (horner && obs) return launch_blk_mode<T, true, true, U, RX, RY>(a, st);
+  if (horner) return launch_blk_mode<T, true, false, U, RX, RY>(a, st);
+  if (obs) return launch_blk_mode<T, false, true, U, RX, RY>(a, st);
+  return launch_blk_mode<T, false, false, U, RX, RY>(a, st);
+}
+
+template <typename T, int RX, int RY>
+hpsi_status launch_blk_b(const PassArgs &a, int group, cudaStream_t st) {
+  if (group == 1) return launch_blk_u<T, 1, RX, RY>(a, st);
+  return launch_blk_u<T, 3, RX, RY>(a, st);
+}
+
+}  // namespace
+
+template <typename T>
+int blk_chunk_states() {
+  return blk_lanes<T>() / 2;
+}
+
+template <typename T>
+bool blk_pass_eligible(const PassArgs &a, long long ld) {
+  if (ld % blk_chunk_states<T>() != 0) return false;
+  if (reinterpret_cast<uintptr_t>(a.in) % 16 != 0 || reinterpret_cast<uintptr_t>(a.out) % 16 != 0) return false;
+  if ((a.mode == PASS_HORNER || a.obs) && reinterpret_cast<uintptr_t>(a.psi0) % 16 != 0) return false;
+  if ((2 * a.in_ld * sizeof(T)) % 16 != 0 || (2 * a.psi0_ld * sizeof(T)) % 16 != 0) return false;
+  return true;
+}
+
+// Thread blocks: FP64 2 x 4 cells (256 threads) or 2 x 2 (512); FP32 4 x 4
+// (256) or 2 x 4 (512).
+template <typename T>
+hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int group, cudaStream_t st) {
+  if (a.nitems == 0) return HPSI_OK;
+  if constexpr (sizeof(T) == 8) {
+    if (rx == 2 && ry == 4) return launch_blk_b<T, 2, 4>(a, group, st);
+    if (rx == 2 && ry == 2) return launch_blk_b<T, 2, 2>(a, group, st);
+  } else {
+    if (rx == 4 && ry == 4) return launch_blk_b<T, 4, 4>(a, group, st);
+    if (rx == 2 && ry == 4) return launch_blk_b<T, 2, 4>(a, group, st);
+  }
+  set_error("launch_pass_blk: no kernel for this cell block");
+  return HPSI_ERR_UNSUPPORTED;
+}
+
+template int blk_chunk_states<double>();
+template int blk_chunk_states<float>();
+template bool blk_pass_eligible<double>(const PassArgs &, long long);
+template bool blk_pass_eligible<float>(const PassArgs &, long long);
+template hpsi_status launch_pass_blk<double>(const PassArgs &, int, int, int, cudaStream_t);
+template hpsi_status launch_pass_blk<float>(const PassArgs &, int, int, int, cudaStream_t);
+
+}  // namespace hpsi

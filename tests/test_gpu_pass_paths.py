@@ -1,0 +1,146 @@
+"""GPU parity of both stencil-pass kernels against the FP64 CPU oracle.
+
+The register-blocked pass (one real lane per thread, 16 x 8 tiles) serves
+batches whose width is a multiple of its state chunk (8 complex states FP64,
+16 FP32); the one-complex-per-thread pass serves the rest.  Both
+are forced here through the shape override and compared with the oracle and
+with each other: FP64 to 1e-12 relative max-norm per state, FP32 storage to
+2e-5.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_maxnorm_per_state, small_sphere_system
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 2e-5
+
+LEGACY = {"HPSI_PASS_SHAPE64": "4,2,0,0,0", "HPSI_PASS_SHAPE32": "8,4,0,0,0"}
+
+
+def _setup(mesh, v=None, proj=None):
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    w = laplacian_weights(mesh.spacing)
+    pts = star_points()
+    dm = lib.DeviceMesh(mesh)
+    ham = lib.Hamiltonian(dm, w, pts, v=v, projectors=proj)
+    return dm, ham, w, pts
+
+
+def _oracle(mesh, w, pts, v=None, proj=None, bc="zero"):
+    from oracle import oracle as O
+    P = O.Projectors(proj.maps, proj.mats, proj.scals) if proj is not None else None
+    return O.Hamiltonian(mesh, w, pts, v=v, projectors=P, bc=bc)
+
+
+def _dev(x, cuda, ld, dtype):
+    import torch
+    out = np.zeros((x.shape[0], ld), dtype=dtype)
+    out[:, : x.shape[1]] = x
+    return torch.from_numpy(out).to(cuda)
+
+
+def _set_path(monkeypatch, path, zb=0):
+    for k in LEGACY:
+        monkeypatch.delenv(k, raising=False)
+    if path == "legacy":
+        for k, v in LEGACY.items():
+            monkeypatch.setenv(k, v)
+    elif zb:
+        monkeypatch.setenv("HPSI_PASS_SHAPE64", f"8,4,{zb},0,1")
+        monkeypatch.setenv("HPSI_PASS_SHAPE32", f"16,4,{zb},0,1")
+
+
+@pytest.mark.parametrize("path", ["blk", "legacy"])
+@pytest.mark.parametrize("dtype,ld,nst", [(np.complex128, 16, 13), (np.complex128, 8, 8),
+                                          (np.complex64, 16, 11), (np.complex64, 32, 20)])
+def test_apply_and_taylor(cuda, monkeypatch, path, dtype, ld, nst):
+    import torch
+    from hpsi import lib
+    _set_path(monkeypatch, path)
+    m, v, proj, psi = small_sphere_system(seed=41, nst=nst, radius=4.2, natoms=4)
+    dm, ham, w, pts = _setup(m, v=v, proj=proj)
+    o = _oracle(m, w, pts, v=v, proj=proj)
+    tol = TOL64 if dtype == np.complex128 else TOL32
+    x = _dev(psi, cuda, ld, dtype)
+    y = torch.zeros((m.np, ld), dtype=x.dtype, device=cuda)
+    ham.apply(x, y, nst=nst)
+    got = y.cpu().numpy()[:, :nst].astype(np.complex128)
+    assert rel_maxnorm_per_state(got, o.apply(psi)) <= tol
+    e, d, n = ham.taylor_step(x, 0.02, order=4, nst=nst, observables=True)
+    got = x.cpu().numpy()[: m.np, :nst].astype(np.complex128)
+    assert rel_maxnorm_per_state(got, o.taylor(psi, 0.02, order=4)) <= tol
+    h = o.apply(psi)
+    dv = m.vol_pp
+    e_ref = dv * np.real(np.sum(psi[: m.np].conj() * h, axis=0))
+    n_ref = dv * np.sum(np.abs(psi[: m.np]) ** 2, axis=0)
+    assert np.max(np.abs(e - e_ref) / np.abs(e_ref)) <= (1e-12 if dtype == np.complex128 else 1e-5)
+    assert np.max(np.abs(n - n_ref) / n_ref) <= (1e-12 if dtype == np.complex128 else 1e-6)
+
+
+@pytest.mark.parametrize("zb", [0, 5, 9])
+def test_blk_zblocks_and_tiles(cuda, monkeypatch, zb):
+    """A box several tiles wide in x and y, cut into z blocks of several depths
+    (the block edges re-read a 4-plane halo)."""
+    import torch
+    from hpsi import fixtures, lib
+    from hpsi.mesh import index_box_mesh
+    _set_path(monkeypatch, "blk", zb=zb)
+    rng = np.random.default_rng(43)
+    m = index_box_mesh((37, 21, 19), 0.3)
+    v = fixtures.soft_coulomb(m, rng)
+    psi = fixtures.random_states(m, 16, rng, orthonormal=False)
+    dm, ham, w, pts = _setup(m, v=v)
+    ref = _oracle(m, w, pts, v=v).apply(psi)
+    x = _dev(psi, cuda, 16, np.complex128)
+    y = torch.zeros((m.np, 16), dtype=x.dtype, device=cuda)
+    ham.apply(x, y)
+    assert rel_maxnorm_per_state(y.cpu().numpy(), ref) <= TOL64
+
+
+def test_blk_periodic_and_raw_boundary(cuda, monkeypatch):
+    """Periodic images without Bloch phase (map to inner rows) and set_bc=False
+    (boundary rows read as stored: the input tensor spans np_part rows)."""
+    import torch
+    from hpsi import fixtures, lib
+    from hpsi.mesh import index_box_mesh, sphere_mesh
+    _set_path(monkeypatch, "blk")
+    rng = np.random.default_rng(47)
+    m = index_box_mesh((12, 10, 8), 0.3, periodic=True)
+    v = fixtures.soft_coulomb(m, rng)
+    psi = fixtures.random_states(m, 8, rng, orthonormal=False)
+    dm, ham, w, pts = _setup(m, v=v)
+    ref = _oracle(m, w, pts, v=v, bc="periodic").apply(psi)
+    x = _dev(psi, cuda, 8, np.complex128)
+    y = torch.zeros((m.np, 8), dtype=x.dtype, device=cuda)
+    ham.apply(x, y)
+    assert rel_maxnorm_per_state(y.cpu().numpy(), ref) <= TOL64
+
+    m = sphere_mesh(3.0, 0.4)
+    r2 = np.sum(m.x * m.x, axis=1)
+    f = (10 * np.exp(0.345j) * np.exp(-(1 / 3.0 + 0.01j) * r2) + (100 - 50j))[:, None] * \
+        np.exp(0.1j * np.arange(8))[None, :]
+    dm, ham, w, pts = _setup(m)
+    ref = _oracle(m, w, pts, bc="none").apply(f)
+    xd = _dev(f, cuda, 8, np.complex128)
+    y = torch.zeros((m.np, 8), dtype=torch.complex128, device=cuda)
+    ham.apply(xd, y, terms=1, set_bc=False)
+    assert rel_maxnorm_per_state(y.cpu().numpy(), ref) <= TOL64
+
+
+def test_paths_agree_fp32(cuda, monkeypatch):
+    """The two FP32 kernels sum in different orders; they agree to FP32 rounding."""
+    import torch
+    m, v, proj, psi = small_sphere_system(seed=53, nst=16, radius=4.2, natoms=4)
+    outs = []
+    for path in ("blk", "legacy"):
+        _set_path(monkeypatch, path)
+        dm, ham, w, pts = _setup(m, v=v, proj=proj)
+        x = _dev(psi, cuda, 16, np.complex64)
+        y = torch.zeros((m.np, 16), dtype=x.dtype, device=cuda)
+        ham.apply(x, y)
+        outs.append(y.cpu().numpy().astype(np.complex128))
+    assert rel_maxnorm_per_state(outs[0], outs[1]) <= 2e-6
