@@ -12,8 +12,9 @@ Inputs are seeded synthetic data (no data set exists for this path).
 value  = point-states per second of H.psi with psi resident in HBM (the batch,
          2.2 GB, is far larger than the 126 MB L2, so no flush is needed);
 e2e    = the same metric through the C ABI with pinned host buffers (the
-         host->device copy of psi and the device->host copy of H psi inside
-         the timed region of every step);
+         host->device copy of psi's np inner rows and the device->host copy of
+         H psi inside the timed region of every step, pipelined over state
+         slabs by the library);
 extra  = FP32-storage H.psi, the fused Taylor step (FP64 and FP32).
 Multi-GPU: independent replicas (the path has no exchange step), weak scaling.
 --impl reference times the reference CPU path (the reference's own compiled
@@ -336,7 +337,7 @@ def main():
                        "step": "one H.psi (kinetic + local + KB) over the whole batch",
                        "l2": "inputs (2.2 GB) larger than L2; no flush",
                        "parallelism": f"replicas x{world}"},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(m.np_part * nst * S),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(m.np * nst * S),
                     "d2h_bytes_per_step": int(m.np * nst * S)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,

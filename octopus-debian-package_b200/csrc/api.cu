@@ -198,28 +198,31 @@ PassShape legacy_shape(int dtype, long long ld) {
 
 // Shape of the register-blocked pass (one real lane per thread, 16 x 8 tiles).
 PassShape blk_shape(int dtype) {
-  // measured on the R = 12 bohr sphere (128 states): 512-thread blocks of
-  // FP64 2 x 2 and FP32 2 x 4 cells beat the 256-thread 2 x 4 / 4 x 4 ones
+  // measured on the R = 12 bohr sphere (128 states): FP64 2 x 2 cells of one
+  // real lane (512 threads); FP32 2 x 2 cells of one complex state with
+  // packed multiply-adds (512 threads)
   PassShape s = dtype == HPSI_C128 ? PassShape{blk_chunk_states<double>(), 16, 8, 2}
-                                   : PassShape{blk_chunk_states<float>(), 16, 8, 4};
+                                   : PassShape{blk_chunk_states<float>(), 16, 8, 2};
   s.blk = 1;
   s.rx = 2;
-  s.unroll = dtype == HPSI_C128 ? 3 : 1;  // planes per unrolled group of the z march
+  s.cplx = dtype == HPSI_C128 ? 0 : 1;
+  s.unroll = 3;  // planes per unrolled group of the z march
   return s;
 }
 
 PassShape default_shape(int dtype, long long ld) {
   PassShape s = ld % blk_shape(dtype).sc == 0 ? blk_shape(dtype) : legacy_shape(dtype, ld);
-  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx"
+  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx,cplx"
   const char *env = std::getenv(dtype == HPSI_C128 ? "HPSI_PASS_SHAPE64" : "HPSI_PASS_SHAPE32");
   if (env) {
-    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0;
-    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x) >= 2 && a > 0 && ld % a == 0) {
+    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0, cx = -1;
+    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx) >= 2 && a > 0 && ld % a == 0) {
       if (t && ld % blk_shape(dtype).sc == 0) {
-        s = blk_shape(dtype);  // fixed chunk: block, z depth and group are taken
+        s = blk_shape(dtype);  // fixed chunk: block, element, z depth and group are taken
         if (u == 1 || u == 3) s.unroll = u;
         if (x > 0) s.rx = x;
         if (b > 0) s.ry = b;
+        if (cx >= 0) s.cplx = cx;
       } else {
         s = legacy_shape(dtype, ld);
         s.sc = a;
@@ -482,6 +485,12 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   h->adjbuf.release();
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   if (h->capture_event) cudaEventDestroy(h->capture_event);
+  if (h->xfer_in) cudaStreamDestroy(h->xfer_in);
+  if (h->xfer_out) cudaStreamDestroy(h->xfer_out);
+  for (auto &e : h->xev)
+    if (e) cudaEventDestroy(e);
+  h->slab_in.release();
+  h->slab_out.release();
   h->small.release();
   delete h;
   return HPSI_OK;
@@ -890,7 +899,7 @@ long long pass_in_rows(const hpsi_hamiltonian *h, const int *src_map) {
 template <typename T>
 hpsi_status launch_pass_any(const PassArgs &a, const PassShape &shape, long long in_rows, cudaStream_t st) {
   (void)in_rows;
-  if (shape.blk) return launch_pass_blk<T>(a, shape.rx, shape.ry, shape.unroll, st);
+  if (shape.blk) return launch_pass_blk<T>(a, shape.rx, shape.ry, shape.cplx, shape.unroll, st);
   return launch_pass<T>(a, shape, st);
 }
 template hpsi_status launch_pass_any<double>(const PassArgs &, const PassShape &, long long, cudaStream_t);
@@ -1096,6 +1105,67 @@ hpsi_status stage_batch(Workspace &ws, const hpsi_batch *b, int rows, bool copy_
   return HPSI_OK;
 }
 
+// H psi for host batches, pipelined over state slabs: the copy-in of slab
+// i + 1, the passes of slab i and the copy-out of slab i - 1 run at once on
+// three streams (two copy engines and the SMs), double-buffered on the
+// device.  Rows copied in: np when the boundary condition is applied (the
+// boundary rows are then never read), np_part otherwise.
+template <typename T>
+hpsi_status apply_h_host_pipelined(hpsi_hamiltonian *h, const hpsi_batch *psi, hpsi_batch *hpsi, int terms,
+                                   int set_bc, long long w, cudaStream_t st) {
+  hpsi_mesh *m = h->mesh;
+  const size_t esz = 2 * sizeof(T);
+  const long long ld = psi->ld, ldo = hpsi->ld;
+  const int nslab = int(ld / w);
+  const int rows_in = set_bc ? m->np : m->np_part;
+  const size_t in_bytes = size_t(m->np_part) * w * esz, out_bytes = size_t(m->np) * w * esz;
+  hpsi_status s = h->slab_in.ensure(2 * in_bytes);
+  if (!s) s = h->slab_out.ensure(2 * out_bytes);
+  if (s) return s;
+  if (!h->xfer_in) {
+    HPSI_TRY_CUDA(cudaStreamCreateWithFlags(&h->xfer_in, cudaStreamNonBlocking));
+    HPSI_TRY_CUDA(cudaStreamCreateWithFlags(&h->xfer_out, cudaStreamNonBlocking));
+    for (auto &e : h->xev) HPSI_TRY_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  cudaEvent_t *in_done = h->xev, *comp_done = h->xev + 2, *out_done = h->xev + 4;
+  // the copy streams start after the work already queued on st
+  HPSI_TRY_CUDA(cudaEventRecord(comp_done[0], st));
+  HPSI_TRY_CUDA(cudaStreamWaitEvent(h->xfer_in, comp_done[0], 0));
+  HPSI_TRY_CUDA(cudaStreamWaitEvent(h->xfer_out, comp_done[0], 0));
+  for (int i = 0; i < nslab; ++i) {
+    const int b = i & 1;
+    T *din = reinterpret_cast<T *>(static_cast<char *>(h->slab_in.ptr) + b * in_bytes);
+    T *dout = reinterpret_cast<T *>(static_cast<char *>(h->slab_out.ptr) + b * out_bytes);
+    const size_t col = size_t(i) * w * esz;
+    if (i >= 2) HPSI_TRY_CUDA(cudaStreamWaitEvent(h->xfer_in, comp_done[b], 0));
+    HPSI_TRY_CUDA(cudaMemcpy2DAsync(din, w * esz, static_cast<const char *>(psi->ptr) + col, ld * esz, w * esz,
+                                    rows_in, cudaMemcpyHostToDevice, h->xfer_in));
+    HPSI_TRY_CUDA(cudaEventRecord(in_done[b], h->xfer_in));
+    HPSI_TRY_CUDA(cudaStreamWaitEvent(st, in_done[b], 0));
+    if (i >= 2) HPSI_TRY_CUDA(cudaStreamWaitEvent(st, out_done[b], 0));
+    s = apply_h_dev<T>(h, din, w, dout, w, terms, set_bc, st);
+    if (s) return s;
+    HPSI_TRY_CUDA(cudaEventRecord(comp_done[b], st));
+    HPSI_TRY_CUDA(cudaStreamWaitEvent(h->xfer_out, comp_done[b], 0));
+    HPSI_TRY_CUDA(cudaMemcpy2DAsync(static_cast<char *>(hpsi->ptr) + size_t(i) * w * esz, ldo * esz, dout, w * esz,
+                                    w * esz, m->np, cudaMemcpyDeviceToHost, h->xfer_out));
+    HPSI_TRY_CUDA(cudaEventRecord(out_done[b], h->xfer_out));
+  }
+  HPSI_TRY_CUDA(cudaStreamSynchronize(h->xfer_out));
+  HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  return HPSI_OK;
+}
+
+// State slab width of the host pipeline: about four slabs, each a multiple
+// of the blocked pass's chunk; 0 when the batch does not split.
+long long pipeline_slab(const hpsi_batch *psi, const hpsi_batch *hpsi) {
+  const long long chunk = psi->dtype == HPSI_C128 ? blk_chunk_states<double>() : blk_chunk_states<float>();
+  if (psi->ld != hpsi->ld || psi->nst != psi->ld) return 0;
+  for (int nslab : {4, 8, 2})
+    if (psi->ld % (nslab * chunk) == 0) return psi->ld / nslab;
+  return 0;
+}
+
 }  // namespace hpsi
 
 extern "C" {
@@ -1117,6 +1187,12 @@ hpsi_status hpsi_apply_h(hpsi_hamiltonian *h, const hpsi_batch *psi, hpsi_batch 
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const bool din = is_device_ptr(psi->ptr), dout = is_device_ptr(hpsi->ptr);
+  if (!din && !dout) {
+    const long long w = pipeline_slab(psi, hpsi);
+    if (w > 0)
+      return psi->dtype == HPSI_C128 ? apply_h_host_pipelined<double>(h, psi, hpsi, terms, set_bc, w, st)
+                                     : apply_h_host_pipelined<float>(h, psi, hpsi, terms, set_bc, w, st);
+  }
   const void *pin = psi->ptr;
   void *pout = hpsi->ptr;
   long long ldi = psi->ld, ldo = hpsi->ld;

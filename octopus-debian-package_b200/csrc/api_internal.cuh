@@ -88,6 +88,11 @@ struct hpsi_hamiltonian {
   const double *fld_scale_dev = nullptr;  // set while a TD run replays steps
   cudaStream_t capture_stream = nullptr;  // graph capture / replay stream of TD runs
   cudaEvent_t capture_event = nullptr;
+  // host-batch pipeline: copy-in and copy-out streams, per-buffer events
+  // {copied in, computed, copied out} x 2 buffers, and the slab buffers
+  cudaStream_t xfer_in = nullptr, xfer_out = nullptr;
+  cudaEvent_t xev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  hpsi::Workspace slab_in, slab_out;
   // workspaces
   hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small, tdbuf, adjbuf;
   void proj_free();

@@ -57,6 +57,7 @@ struct PassShape {
   int unroll = 0;  // 1: nine-plane unrolled ring, 0: switch-selected ring
   int blk = 0;     // 1: register-blocked real-lane pass (sc = its chunk, tiles 16 x 8)
   int rx = 0;      // blocked pass: cells per thread along x (ry along y)
+  int cplx = 0;    // blocked pass: 1 = a thread owns a complex state, 0 = one real lane
 };
 
 // Launch the fused pass for a storage type (double -> FP64, float -> FP32).

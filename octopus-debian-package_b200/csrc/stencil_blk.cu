@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
 
 #include "stencil.cuh"
 #include "stencil_blk.cuh"
@@ -44,9 +45,49 @@ constexpr int blk_lanes() {
   return 128 / int(sizeof(T));
 }
 
-template <typename T, bool X0, int RX_, int RY_>
+// Element a thread owns per cell: one real lane, or one complex state.
+template <typename T, bool CPLX>
+struct BlkElem;
+template <>
+struct BlkElem<double, false> {
+  using E = double;
+};
+template <>
+struct BlkElem<float, false> {
+  using E = float;
+};
+template <>
+struct BlkElem<double, true> {
+  using E = double2;
+};
+template <>
+struct BlkElem<float, true> {
+  using E = float2;
+};
+template <typename E>
+__device__ __forceinline__ E ezero() {
+  if constexpr (sizeof(E) == 16)
+    return make_double2(0.0, 0.0);
+  else if constexpr (sizeof(E) == 8 && !std::is_same<E, double>::value)
+    return make_float2(0.f, 0.f);
+  else
+    return E(0);
+}
+__device__ __forceinline__ double fmae(double w, double v, double a) { return fma(w, v, a); }
+__device__ __forceinline__ float fmae(float w, float v, float a) { return fmaf(w, v, a); }
+__device__ __forceinline__ double2 fmae(double w, double2 v, double2 a) {
+  return make_double2(fma(w, v.x, a.x), fma(w, v.y, a.y));
+}
+__device__ __forceinline__ float2 fmae(float w, float2 v, float2 a) {
+  return __ffma2_rn(make_float2(w, w), v, a);  // packed FP32 multiply-add (sm_100)
+}
+
+template <typename T, bool X0, int RX_, int RY_, bool CPLX_>
 struct BlkLayout {
+  static constexpr bool CPLX = CPLX_;
   static constexpr int SL = blk_lanes<T>(), RX = RX_, RY = RY_;
+  static constexpr int LW = CPLX ? 2 : 1;  // reals per thread element
+  static constexpr int SLE = SL / LW;      // thread elements per cell chunk
   static constexpr int TX = BLK_TILE_X, TY = BLK_TILE_Y, HAL = 4;
   static constexpr int HX = TX + 2 * HAL, HY = TY + 2 * HAL;
   static constexpr int HC = HX * HY, IC = TX * TY;
@@ -54,7 +95,7 @@ struct BlkLayout {
   static constexpr int PCS = CELLB / 16;             // 16-byte pieces per cell chunk
   static constexpr int EPP = 16 / int(sizeof(T));    // elements per piece
   static_assert(CELLB == 128, "one cell chunk is 128 bytes");
-  static constexpr int NT = SL * (TX / RX) * (TY / RY);
+  static constexpr int NT = SLE * (TX / RX) * (TY / RY);
   static_assert(NT == 256 || NT == 512, "256 or 512 threads");
   static_assert((HC * PCS) % NT == 0 && (IC * PCS) % NT == 0, "copy rounds tile the threads");
   static constexpr int HROUNDS = HC * PCS / NT, IROUNDS = IC * PCS / NT;
@@ -95,11 +136,13 @@ __device__ __forceinline__ void zero16(void *d) {
 // Plane k of a CTA is halo plane zbeg + k: data stage k % NBUF, side slot
 // k % NSIDE.  Iteration k computes plane k and issues the data of plane
 // k + NBUF - 1 and the side data of plane k + 2 NBUF - 2 (one commit group).
-template <typename T, bool HORNER, bool OBS, int U, int RX_, int RY_>
-__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
+template <typename T, bool HORNER, bool OBS, int U, int RX_, int RY_, bool CPLX>
+__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_, CPLX>::NT, 1)
     pass_blk_kernel(const __grid_constant__ PassArgs p) {
   constexpr bool X0 = HORNER || OBS;
-  using LY = BlkLayout<T, X0, RX_, RY_>;
+  using LY = BlkLayout<T, X0, RX_, RY_, CPLX>;
+  using E = typename BlkElem<T, CPLX>::E;
+  constexpr int SLE = LY::SLE;
   constexpr int SL = LY::SL, RX = LY::RX, RY = LY::RY, TX = LY::TX, TY = LY::TY, HAL = LY::HAL;
   constexpr int HX = LY::HX, NBUF = LY::NBUF, NSIDE = LY::NSIDE, PCS = LY::PCS, EPP = LY::EPP;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -229,18 +272,18 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
 
   // ---- compute roles --------------------------------------------------------------
   const int lane = tid & 31;
-  const int l = tid % SL;
-  const int g = tid / SL;
+  const int l = tid % SLE;
+  const int g = tid / SLE;
   const int bx = (g % (TX / RX)) * RX, by = (g / (TX / RX)) * RY;
   const double fscale = p.fld_scale_dev ? *p.fld_scale_dev : 1.0;
   const double fz = p.fld[2] * fscale * B.h[2];
   const double fx0 = fscale * p.fld[0] * B.h[0], fy0 = fscale * p.fld[1] * B.h[1];
   const double fxy0 = fx0 * double(cx0 + bx + B.lo[0]) + fy0 * double(cy0 + by + B.lo[1]);
   const T are = static_cast<T>(p.a_re), aim = static_cast<T>(p.a_im);
-  const bool odd = (l & 1) != 0;
-  T *out = static_cast<T *>(p.out);
-  const long long out_ld2 = 2 * p.out_ld;
-  const int ocol = col + l;
+  const bool odd = !CPLX && (l & 1) != 0;
+  E *out = static_cast<E *>(p.out);
+  const long long out_lde = 2 * p.out_ld / LY::LW;  // elements per output row
+  const int ocol = col / LY::LW + l;
   Kahan ke = {0, 0}, kn = {0, 0}, kd = {0, 0};
   (void)lane;
 
@@ -256,13 +299,13 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
       gz1 = max(gz1, cz.y);
     }
 
-  T acc[RX][RY][9];
+  E acc[RX][RY][9];
 #pragma unroll
   for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
     for (int r = 0; r < RY; ++r)
 #pragma unroll
-      for (int j = 0; j < 9; ++j) acc[cx][r][j] = T(0);
+      for (int j = 0; j < 9; ++j) acc[cx][r][j] = ezero<E>();
 
   // one plane.  The running sums of a group of U planes sit in static slots:
   // plane K of the group adds its centre to slot (4 + K) % 9 and emits slot K;
@@ -278,7 +321,7 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
     cp_async_commit();
 
     const unsigned char *st = stage(k);
-    const T *P = reinterpret_cast<const T *>(st) + l;
+    const E *P = reinterpret_cast<const E *>(st) + l;
     const double *vs = reinterpret_cast<const double *>(st + LY::o_v);
     const int pz = zbeg + k;
     const double vz = fz * double(pz + B.lo[2]);
@@ -292,24 +335,24 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
       for (int i = 0; i < RY + 8; ++i) {
 #pragma unroll
         for (int cx = 0; cx < RX; ++cx) {
-          const T val = P[((by + i) * HX + bx + cx + HAL) * SL];
+          const E val = P[((by + i) * HX + bx + cx + HAL) * SLE];
 #pragma unroll
           for (int r = 0; r < RY; ++r) {
             const int d = i - r;
             if (d < 0 || d > 8) continue;
             if (d != 4) {
-              acc[cx][r][S4] = fma(wsel_t<T>(p.wy, p.wyf, d), val, acc[cx][r][S4]);
+              acc[cx][r][S4] = fmae(wsel_t<T>(p.wy, p.wyf, d), val, acc[cx][r][S4]);
               continue;
             }
             const double vv = vs[(by + r) * TX + bx + cx] + fxy0 + fx0 * double(cx) + fy0 * double(r) + vz;
-            acc[cx][r][S4] = fma(wsel_t<T>(p.wx, p.wxf, 4) + static_cast<T>(vv), val, acc[cx][r][S4]);
+            acc[cx][r][S4] = fmae(wsel_t<T>(p.wx, p.wxf, 4) + static_cast<T>(vv), val, acc[cx][r][S4]);
 #pragma unroll
             for (int c2 = 0; c2 < RX; ++c2)
-              if (c2 != cx) acc[c2][r][S4] = fma(wsel_t<T>(p.wx, p.wxf, cx - c2 + 4), val, acc[c2][r][S4]);
+              if (c2 != cx) acc[c2][r][S4] = fmae(wsel_t<T>(p.wx, p.wxf, cx - c2 + 4), val, acc[c2][r][S4]);
 #pragma unroll
             for (int j = 0; j < 9; ++j)
               if (j != 4)
-                acc[cx][r][(j + K) % 9] = fma(wsel_t<T>(p.wz, p.wzf, 8 - j), val, acc[cx][r][(j + K) % 9]);
+                acc[cx][r][(j + K) % 9] = fmae(wsel_t<T>(p.wz, p.wzf, 8 - j), val, acc[cx][r][(j + K) % 9]);
           }
         }
       }
@@ -319,12 +362,12 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
         if (dx >= 0 && dx < RX) continue;
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
-          const T val = P[((by + r + HAL) * HX + bx + dx + HAL) * SL];
+          const E val = P[((by + r + HAL) * HX + bx + dx + HAL) * SLE];
 #pragma unroll
           for (int cx = 0; cx < RX; ++cx) {
             const int dd = dx - cx;
             if (dd < -4 || dd > 4) continue;
-            acc[cx][r][S4] = fma(wsel_t<T>(p.wx, p.wxf, dd + 4), val, acc[cx][r][S4]);
+            acc[cx][r][S4] = fmae(wsel_t<T>(p.wx, p.wxf, dd + 4), val, acc[cx][r][S4]);
           }
         }
       }
@@ -334,38 +377,51 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
     const int zo = pz - HAL;
     if (zo >= zs) {
       const int *rows = reinterpret_cast<const int *>(side(k) + LY::s_rows);
-      const T *x0s = reinterpret_cast<const T *>(st + LY::o_psi0) + l;
+      const E *x0s = reinterpret_cast<const E *>(st + LY::o_psi0) + l;
 #pragma unroll
       for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
           const int cell = (by + r) * TX + bx + cx;
-          const T h = acc[cx][r][K];
-          acc[cx][r][K] = T(0);
-          T val = h;
+          const E h = acc[cx][r][K];
+          acc[cx][r][K] = ezero<E>();
+          E val = h;
           if constexpr (HORNER) {
-            const T hp = __shfl_xor_sync(0xffffffffu, h, 1);  // the other part of this state
-            const T x0 = x0s[cell * SL];
-            val = odd ? x0 + are * h + aim * hp : x0 + are * h - aim * hp;
+            const E x0 = x0s[cell * SLE];
+            if constexpr (CPLX) {
+              val.x = x0.x + are * h.x - aim * h.y;
+              val.y = x0.y + are * h.y + aim * h.x;
+            } else {
+              const T hp = __shfl_xor_sync(0xffffffffu, h, 1);  // the other part of this state
+              val = odd ? x0 + are * h + aim * hp : x0 + are * h - aim * hp;
+            }
           }
           const int row = rows[cell];
           if (row < 0 || row >= p.np) continue;
           if constexpr (OBS) {
-            const double x0 = double(x0s[cell * SL]);
+            const E x0 = x0s[cell * SLE];
             const double rr = p.obs_pol[0] * B.h[0] * double(cx0 + bx + cx + B.lo[0]) +
                               p.obs_pol[1] * B.h[1] * double(cy0 + by + r + B.lo[1]) +
                               p.obs_pol[2] * B.h[2] * double(zo + B.lo[2]);
-            kadd(ke, x0 * double(h));
-            kadd(kn, x0 * x0);
-            kadd(kd, x0 * x0 * rr);
+            double eh, n2;
+            if constexpr (CPLX) {
+              eh = double(x0.x) * double(h.x) + double(x0.y) * double(h.y);
+              n2 = double(x0.x) * double(x0.x) + double(x0.y) * double(x0.y);
+            } else {
+              eh = double(x0) * double(h);
+              n2 = double(x0) * double(x0);
+            }
+            kadd(ke, eh);
+            kadd(kn, n2);
+            kadd(kd, n2 * rr);
           }
-          out[row * out_ld2 + ocol] = val;
+          out[row * out_lde + ocol] = val;
         }
     } else {
 #pragma unroll
       for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
-        for (int r = 0; r < RY; ++r) acc[cx][r][K] = T(0);
+        for (int r = 0; r < RY; ++r) acc[cx][r][K] = ezero<E>();
     }
   };
 
@@ -374,7 +430,7 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
     for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
-        T t[9];
+        E t[9];
 #pragma unroll
         for (int j = 0; j < 9; ++j) t[j] = acc[cx][r][(j + U) % 9];
 #pragma unroll
@@ -410,9 +466,10 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
     }
     __syncthreads();
     if (tid < SL / 2) {
+      // threads of state tid: lanes 2 tid, 2 tid + 1 (real lanes) or lane tid
       Kahan a[3] = {{0, 0}, {0, 0}, {0, 0}};
-      for (int t = 2 * tid; t < LY::NT; t += SL)
-        for (int q = 0; q < 2; ++q)
+      for (int t = LY::LW == 1 ? 2 * tid : tid; t < LY::NT; t += SLE)
+        for (int q = 0; q < 3 - LY::LW; ++q)
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             kadd(a[c], red[(t + q) * 6 + 2 * c]);
@@ -428,10 +485,10 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_>::NT, 1)
   }
 }
 
-template <typename T, bool HORNER, bool OBS, int U, int RX, int RY>
+template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX>
 hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
-  using LY = BlkLayout<T, HORNER || OBS, RX, RY>;
-  auto kern = pass_blk_kernel<T, HORNER, OBS, U, RX, RY>;
+  using LY = BlkLayout<T, HORNER || OBS, RX, RY, CPLX>;
+  auto kern = pass_blk_kernel<T, HORNER, OBS, U, RX, RY, CPLX>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
@@ -444,19 +501,19 @@ hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
   return HPSI_OK;
 }
 
-template <typename T, int U, int RX, int RY>
+template <typename T, int U, int RX, int RY, bool CPLX>
 hpsi_status launch_blk_u(const PassArgs &a, cudaStream_t st) {
   const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr;
-  if (horner && obs) return launch_blk_mode<T, true, true, U, RX, RY>(a, st);
-  if (horner) return launch_blk_mode<T, true, false, U, RX, RY>(a, st);
-  if (obs) return launch_blk_mode<T, false, true, U, RX, RY>(a, st);
-  return launch_blk_mode<T, false, false, U, RX, RY>(a, st);
+  if (horner && obs) return launch_blk_mode<T, true, true, U, RX, RY, CPLX>(a, st);
+  if (horner) return launch_blk_mode<T, true, false, U, RX, RY, CPLX>(a, st);
+  if (obs) return launch_blk_mode<T, false, true, U, RX, RY, CPLX>(a, st);
+  return launch_blk_mode<T, false, false, U, RX, RY, CPLX>(a, st);
 }
 
-template <typename T, int RX, int RY>
+template <typename T, int RX, int RY, bool CPLX>
 hpsi_status launch_blk_b(const PassArgs &a, int group, cudaStream_t st) {
-  if (group == 1) return launch_blk_u<T, 1, RX, RY>(a, st);
-  return launch_blk_u<T, 3, RX, RY>(a, st);
+  if (group == 1) return launch_blk_u<T, 1, RX, RY, CPLX>(a, st);
+  return launch_blk_u<T, 3, RX, RY, CPLX>(a, st);
 }
 
 }  // namespace
@@ -475,17 +532,18 @@ bool blk_pass_eligible(const PassArgs &a, long long ld) {
   return true;
 }
 
-// Thread blocks: FP64 2 x 4 cells (256 threads) or 2 x 2 (512); FP32 4 x 4
-// (256) or 2 x 4 (512).
+// Thread blocks (cells per thread, element, threads): FP64 2 x 2 real lanes
+// (512) or 2 x 2 complex (256); FP32 2 x 4 real lanes (512) or 2 x 2 complex
+// with packed multiply-adds (512).
 template <typename T>
-hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int group, cudaStream_t st) {
+hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int cplx, int group, cudaStream_t st) {
   if (a.nitems == 0) return HPSI_OK;
   if constexpr (sizeof(T) == 8) {
-    if (rx == 2 && ry == 4) return launch_blk_b<T, 2, 4>(a, group, st);
-    if (rx == 2 && ry == 2) return launch_blk_b<T, 2, 2>(a, group, st);
+    if (!cplx && rx == 2 && ry == 2) return launch_blk_b<T, 2, 2, false>(a, group, st);
+    if (cplx && rx == 2 && ry == 2) return launch_blk_b<T, 2, 2, true>(a, group, st);
   } else {
-    if (rx == 4 && ry == 4) return launch_blk_b<T, 4, 4>(a, group, st);
-    if (rx == 2 && ry == 4) return launch_blk_b<T, 2, 4>(a, group, st);
+    if (!cplx && rx == 2 && ry == 4) return launch_blk_b<T, 2, 4, false>(a, group, st);
+    if (cplx && rx == 2 && ry == 2) return launch_blk_b<T, 2, 2, true>(a, group, st);
   }
   set_error("launch_pass_blk: no kernel for this cell block");
   return HPSI_ERR_UNSUPPORTED;
@@ -495,7 +553,7 @@ template int blk_chunk_states<double>();
 template int blk_chunk_states<float>();
 template bool blk_pass_eligible<double>(const PassArgs &, long long);
 template bool blk_pass_eligible<float>(const PassArgs &, long long);
-template hpsi_status launch_pass_blk<double>(const PassArgs &, int, int, int, cudaStream_t);
-template hpsi_status launch_pass_blk<float>(const PassArgs &, int, int, int, cudaStream_t);
+template hpsi_status launch_pass_blk<double>(const PassArgs &, int, int, int, int, cudaStream_t);
+template hpsi_status launch_pass_blk<float>(const PassArgs &, int, int, int, int, cudaStream_t);
 
 }  // namespace hpsi

@@ -20,8 +20,9 @@ bool blk_pass_eligible(const PassArgs &a, long long ld);
 
 // a.chunks = ld / blk_chunk_states<T>(); a.items over 16 x 8 tiles;
 // observables, when requested, are written per item.  rx x ry: cells per
-// thread; group: planes per unrolled group of the z march (1 or 3).
+// thread; cplx: a thread owns a complex state (else one real lane); group:
+// planes per unrolled group of the z march (1 or 3).
 template <typename T>
-hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int group, cudaStream_t st);
+hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int cplx, int group, cudaStream_t st);
 
 }  // namespace hpsi

@@ -18,6 +18,10 @@ TOL64 = 1e-12
 TOL32 = 2e-5
 
 LEGACY = {"HPSI_PASS_SHAPE64": "4,2,0,0,0", "HPSI_PASS_SHAPE32": "8,4,0,0,0"}
+# blocked pass: "chunk,ry,zb,group,1,rx,complex"
+BLK_REAL = {"HPSI_PASS_SHAPE64": "8,2,{zb},3,1,2,0", "HPSI_PASS_SHAPE32": "16,4,{zb},1,1,2,0"}
+BLK_CPLX = {"HPSI_PASS_SHAPE64": "8,2,{zb},1,1,2,1", "HPSI_PASS_SHAPE32": "16,2,{zb},3,1,2,1"}
+PATHS = ["blk_real", "blk_cplx", "legacy"]
 
 
 def _setup(mesh, v=None, proj=None):
@@ -44,17 +48,12 @@ def _dev(x, cuda, ld, dtype):
 
 
 def _set_path(monkeypatch, path, zb=0):
-    for k in LEGACY:
-        monkeypatch.delenv(k, raising=False)
-    if path == "legacy":
-        for k, v in LEGACY.items():
-            monkeypatch.setenv(k, v)
-    elif zb:
-        monkeypatch.setenv("HPSI_PASS_SHAPE64", f"8,4,{zb},0,1")
-        monkeypatch.setenv("HPSI_PASS_SHAPE32", f"16,4,{zb},0,1")
+    env = {"legacy": LEGACY, "blk_real": BLK_REAL, "blk_cplx": BLK_CPLX}[path]
+    for k, v in env.items():
+        monkeypatch.setenv(k, v.format(zb=zb))
 
 
-@pytest.mark.parametrize("path", ["blk", "legacy"])
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("dtype,ld,nst", [(np.complex128, 16, 13), (np.complex128, 8, 8),
                                           (np.complex64, 16, 11), (np.complex64, 32, 20)])
 def test_apply_and_taylor(cuda, monkeypatch, path, dtype, ld, nst):
@@ -81,14 +80,15 @@ def test_apply_and_taylor(cuda, monkeypatch, path, dtype, ld, nst):
     assert np.max(np.abs(n - n_ref) / n_ref) <= (1e-12 if dtype == np.complex128 else 1e-6)
 
 
+@pytest.mark.parametrize("path", ["blk_real", "blk_cplx"])
 @pytest.mark.parametrize("zb", [0, 5, 9])
-def test_blk_zblocks_and_tiles(cuda, monkeypatch, zb):
+def test_blk_zblocks_and_tiles(cuda, monkeypatch, zb, path):
     """A box several tiles wide in x and y, cut into z blocks of several depths
     (the block edges re-read a 4-plane halo)."""
     import torch
     from hpsi import fixtures, lib
     from hpsi.mesh import index_box_mesh
-    _set_path(monkeypatch, "blk", zb=zb)
+    _set_path(monkeypatch, path, zb=zb)
     rng = np.random.default_rng(43)
     m = index_box_mesh((37, 21, 19), 0.3)
     v = fixtures.soft_coulomb(m, rng)
@@ -101,13 +101,14 @@ def test_blk_zblocks_and_tiles(cuda, monkeypatch, zb):
     assert rel_maxnorm_per_state(y.cpu().numpy(), ref) <= TOL64
 
 
-def test_blk_periodic_and_raw_boundary(cuda, monkeypatch):
+@pytest.mark.parametrize("path", ["blk_real", "blk_cplx"])
+def test_blk_periodic_and_raw_boundary(cuda, monkeypatch, path):
     """Periodic images without Bloch phase (map to inner rows) and set_bc=False
     (boundary rows read as stored: the input tensor spans np_part rows)."""
     import torch
     from hpsi import fixtures, lib
     from hpsi.mesh import index_box_mesh, sphere_mesh
-    _set_path(monkeypatch, "blk")
+    _set_path(monkeypatch, path)
     rng = np.random.default_rng(47)
     m = index_box_mesh((12, 10, 8), 0.3, periodic=True)
     v = fixtures.soft_coulomb(m, rng)
@@ -136,11 +137,32 @@ def test_paths_agree_fp32(cuda, monkeypatch):
     import torch
     m, v, proj, psi = small_sphere_system(seed=53, nst=16, radius=4.2, natoms=4)
     outs = []
-    for path in ("blk", "legacy"):
+    for path in PATHS:
         _set_path(monkeypatch, path)
         dm, ham, w, pts = _setup(m, v=v, proj=proj)
         x = _dev(psi, cuda, 16, np.complex64)
         y = torch.zeros((m.np, 16), dtype=x.dtype, device=cuda)
         ham.apply(x, y)
         outs.append(y.cpu().numpy().astype(np.complex128))
-    assert rel_maxnorm_per_state(outs[0], outs[1]) <= 2e-6
+    for o in outs[1:]:
+        assert rel_maxnorm_per_state(o, outs[0]) <= 2e-6
+
+
+@pytest.mark.parametrize("dtype,ld", [(np.complex128, 32), (np.complex64, 64), (np.complex128, 12)])
+@pytest.mark.parametrize("set_bc", [True, False])
+def test_host_batches_pipelined(cuda, dtype, ld, set_bc):
+    """Host (pinned) batches go through the slab pipeline (copy-in, passes,
+    copy-out on three streams) when the width splits into chunk-aligned slabs,
+    else through one staged pass; both equal the device-resident result."""
+    import torch
+    m, v, proj, psi = small_sphere_system(seed=59, nst=ld, radius=4.2, natoms=4)
+    dm, ham, w, pts = _setup(m, v=v, proj=proj)
+    x = _dev(psi, cuda, ld, dtype)
+    y = torch.zeros((m.np, ld), dtype=x.dtype, device=cuda)
+    ham.apply(x, y, set_bc=set_bc)
+    xh = x.cpu().pin_memory()
+    yh = torch.zeros((m.np, ld), dtype=x.dtype).pin_memory()
+    ham.apply(xh, yh, set_bc=set_bc)
+    # slabs change the projector split-K sums (rounding only)
+    tol = 1e-13 if dtype == np.complex128 else 1e-6
+    assert rel_maxnorm_per_state(yh.numpy().astype(np.complex128), y.cpu().numpy().astype(np.complex128)) <= tol
