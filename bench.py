@@ -76,20 +76,37 @@ def profile_traffic(path="profiles/pass_fp64_sphere128.md"):
 
 
 class Clocks:
-    """nvidia-smi sampler for the timed region."""
+    """SM clock and throttle-reason sampler for the timed region (NVML every
+    2 ms, read-only; nvidia-smi every 200 ms when NVML is unavailable)."""
 
-    def __init__(self, gpu_index=0):
-        self.samples = []
-        self.proc = None
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
+
+    def __init__(self, gpu_index=0, period=0.002):
         self.idx = gpu_index
+        self.period = period
+        self.samples = []  # (sm_mhz, reasons bitmask)
+        self.max_mhz = None
+        self.proc = None
+        self.nvml = None
+        self._stop = threading.Event()
 
     def __enter__(self):
         try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
+        try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}",
-                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
-                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap,utilization.gpu",
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -98,37 +115,48 @@ class Clocks:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv = self.nvml
+        while not self._stop.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((mhz, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+            try:
+                f = [x.strip() for x in line.split(",")]
+                self.max_mhz = float(f[1])
+                self.samples.append((float(f[0]), int(f[2], 16)))
+            except Exception:
+                continue
 
     def __exit__(self, *a):
+        self._stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        elif self.nvml is not None:
+            self.t.join(timeout=1)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
-            try:
-                util = float(s[6])
-                if util < 50:
-                    continue
-                sm.append(float(s[0]))
-                mx = float(s[1])
-                for n, v in zip(names, s[2:6]):
-                    if v.lower().startswith("active"):
-                        reasons.add(n)
-            except Exception:
-                continue
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(self.samples)}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        reasons = set()
+        for _, rs in self.samples:
+            for n, bit in self.REASONS.items():
+                if rs & bit:
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(self.samples),
+                "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 def build_system(small=False):

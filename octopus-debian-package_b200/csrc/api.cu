@@ -206,7 +206,7 @@ PassShape blk_shape(int dtype) {
   s.blk = 1;
   s.rx = 2;
   s.cplx = dtype == HPSI_C128 ? 0 : 1;
-  s.unroll = 3;  // planes per unrolled group of the z march
+  s.unroll = 9;  // planes per unrolled group of the z march (9: no rotation)
   return s;
 }
 
@@ -219,7 +219,7 @@ PassShape default_shape(int dtype, long long ld) {
     if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx) >= 2 && a > 0 && ld % a == 0) {
       if (t && ld % blk_shape(dtype).sc == 0) {
         s = blk_shape(dtype);  // fixed chunk: block, element, z depth and group are taken
-        if (u == 1 || u == 3) s.unroll = u;
+        if (u == 1 || u == 3 || u == 9) s.unroll = u;
         if (x > 0) s.rx = x;
         if (b > 0) s.ry = b;
         if (cx >= 0) s.cplx = cx;

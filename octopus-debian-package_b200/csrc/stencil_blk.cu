@@ -131,6 +131,11 @@ __device__ __forceinline__ float wsel_t<float>(const double *, const float *f, i
 __device__ __forceinline__ void zero16(void *d) {
   *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
 }
+// 16-byte cp.async that reads `bytes` (16 or 0) and zero-fills the rest
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, int bytes) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
 
 // grid: nitems (16 x 8 tiles x z blocks) * chunks.
 // Plane k of a CTA is halo plane zbeg + k: data stage k % NBUF, side slot
@@ -206,26 +211,36 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_, CPLX>::N
     const unsigned char *sd = side(k);
     const int *map = reinterpret_cast<const int *>(sd);
     T *halo = reinterpret_cast<T *>(st) + piece * EPP;
-#pragma unroll 1
-    for (int j = 0; j < LY::HROUNDS; ++j) {
-      const int cell = cpc + j * (LY::NT / PCS);
-      const int src = map[cell];
-      T *d = halo + cell * SL;
-      if (src >= 0) {
-        cp_async16(d, in_base + src * in_ld2);
-      } else if (src == -1) {
-        zero16(d);
-      } else {
-        // periodic image times the Bloch phase correction
-        const int b = -(src + 2);
-        const T *g = in_base + __ldg(p.per_inner + b) * in_ld2;
-        const T pr = static_cast<const T *>(p.phase_corr)[2 * b];
-        const T pi = static_cast<const T *>(p.phase_corr)[2 * b + 1];
+    if (p.phase_corr == nullptr) {
+      // every entry is a row or -1 (zero): one zero-filling copy per piece
 #pragma unroll
-        for (int e = 0; e < EPP; e += 2) {
-          const T xr = g[e], xi = g[e + 1];
-          d[e] = xr * pr - xi * pi;
-          d[e + 1] = xr * pi + xi * pr;
+      for (int j = 0; j < LY::HROUNDS; ++j) {
+        const int cell = cpc + j * (LY::NT / PCS);
+        const int src = map[cell];
+        cp_async16_zfill(halo + cell * SL, in_base + max(src, 0) * in_ld2, src >= 0 ? 16 : 0);
+      }
+    } else {
+#pragma unroll 1
+      for (int j = 0; j < LY::HROUNDS; ++j) {
+        const int cell = cpc + j * (LY::NT / PCS);
+        const int src = map[cell];
+        T *d = halo + cell * SL;
+        if (src >= 0) {
+          cp_async16(d, in_base + src * in_ld2);
+        } else if (src == -1) {
+          zero16(d);
+        } else {
+          // periodic image times the Bloch phase correction
+          const int b = -(src + 2);
+          const T *g = in_base + __ldg(p.per_inner + b) * in_ld2;
+          const T pr = static_cast<const T *>(p.phase_corr)[2 * b];
+          const T pi = static_cast<const T *>(p.phase_corr)[2 * b + 1];
+#pragma unroll
+          for (int e = 0; e < EPP; e += 2) {
+            const T xr = g[e], xi = g[e + 1];
+            d[e] = xr * pr - xi * pi;
+            d[e + 1] = xr * pi + xi * pr;
+          }
         }
       }
     }
@@ -237,7 +252,8 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_, CPLX>::N
       for (int j = 0; j < LY::IROUNDS; ++j) {
         const int cell = cpc + j * (LY::NT / PCS);
         const int row = rows[cell];
-        if (row >= 0 && row < p.np) cp_async16(x0 + cell * SL, x0_base + row * x0_ld2);
+        const bool ok = row >= 0 && row < p.np;
+        cp_async16_zfill(x0 + cell * SL, x0_base + (ok ? row : 0) * x0_ld2, ok ? 16 : 0);
       }
     }
     if (tid < LY::NVP) {
@@ -279,6 +295,7 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_, CPLX>::N
   const double fz = p.fld[2] * fscale * B.h[2];
   const double fx0 = fscale * p.fld[0] * B.h[0], fy0 = fscale * p.fld[1] * B.h[1];
   const double fxy0 = fx0 * double(cx0 + bx + B.lo[0]) + fy0 * double(cy0 + by + B.lo[1]);
+  const bool has_field = fz != 0.0 || fx0 != 0.0 || fy0 != 0.0;  // uniform over the grid
   const T are = static_cast<T>(p.a_re), aim = static_cast<T>(p.a_im);
   const bool odd = !CPLX && (l & 1) != 0;
   E *out = static_cast<E *>(p.out);
@@ -344,7 +361,8 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_, CPLX>::N
               acc[cx][r][S4] = fmae(wsel_t<T>(p.wy, p.wyf, d), val, acc[cx][r][S4]);
               continue;
             }
-            const double vv = vs[(by + r) * TX + bx + cx] + fxy0 + fx0 * double(cx) + fy0 * double(r) + vz;
+            double vv = vs[(by + r) * TX + bx + cx];
+            if (has_field) vv += fxy0 + fx0 * double(cx) + fy0 * double(r) + vz;
             acc[cx][r][S4] = fmae(wsel_t<T>(p.wx, p.wxf, 4) + static_cast<T>(vv), val, acc[cx][r][S4]);
 #pragma unroll
             for (int c2 = 0; c2 < RX; ++c2)
@@ -441,13 +459,21 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_, CPLX>::N
 #pragma unroll 1
   for (int k = 0; k < nplanes; k += U) {
     plane(std::integral_constant<int, 0>{}, k);
-    if constexpr (U > 1)
-      if (k + 1 < nplanes) plane(std::integral_constant<int, (U > 1 ? 1 : 0)>{}, k + 1);
-    if constexpr (U > 2)
-      if (k + 2 < nplanes) plane(std::integral_constant<int, (U > 2 ? 2 : 0)>{}, k + 2);
+#define HPSI_BLK_PLANE(J)                                                          \
+  if constexpr (U > J)                                                             \
+    if (k + J < nplanes) plane(std::integral_constant<int, (U > J ? J : 0)>{}, k + J);
+    HPSI_BLK_PLANE(1)
+    HPSI_BLK_PLANE(2)
+    HPSI_BLK_PLANE(3)
+    HPSI_BLK_PLANE(4)
+    HPSI_BLK_PLANE(5)
+    HPSI_BLK_PLANE(6)
+    HPSI_BLK_PLANE(7)
+    HPSI_BLK_PLANE(8)
+#undef HPSI_BLK_PLANE
     if constexpr (U % 9 != 0) rotate();
   }
-  static_assert(U >= 1 && U <= 3, "group of 1..3 planes");
+  static_assert(U == 1 || U == 3 || U == 9, "groups of 1, 3 or 9 planes");
   cp_async_wait<0>();
 
   if constexpr (OBS) {
@@ -510,12 +536,6 @@ hpsi_status launch_blk_u(const PassArgs &a, cudaStream_t st) {
   return launch_blk_mode<T, false, false, U, RX, RY, CPLX>(a, st);
 }
 
-template <typename T, int RX, int RY, bool CPLX>
-hpsi_status launch_blk_b(const PassArgs &a, int group, cudaStream_t st) {
-  if (group == 1) return launch_blk_u<T, 1, RX, RY, CPLX>(a, st);
-  return launch_blk_u<T, 3, RX, RY, CPLX>(a, st);
-}
-
 }  // namespace
 
 template <typename T>
@@ -532,18 +552,21 @@ bool blk_pass_eligible(const PassArgs &a, long long ld) {
   return true;
 }
 
-// Thread blocks (cells per thread, element, threads): FP64 2 x 2 real lanes
-// (512) or 2 x 2 complex (256); FP32 2 x 4 real lanes (512) or 2 x 2 complex
-// with packed multiply-adds (512).
+// Instantiated blocks (cells per thread, element, planes per group; all 512
+// threads): FP64 2 x 2 real lanes (group 9 or 3) or complex states (9);
+// FP32 2 x 2 complex states with packed multiply-adds (9 or 3) or 2 x 4 real
+// lanes (1).
 template <typename T>
 hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int cplx, int group, cudaStream_t st) {
   if (a.nitems == 0) return HPSI_OK;
   if constexpr (sizeof(T) == 8) {
-    if (!cplx && rx == 2 && ry == 2) return launch_blk_b<T, 2, 2, false>(a, group, st);
-    if (cplx && rx == 2 && ry == 2) return launch_blk_b<T, 2, 2, true>(a, group, st);
+    if (!cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_u<T, 9, 2, 2, false>(a, st);
+    if (!cplx && rx == 2 && ry == 2 && group == 3) return launch_blk_u<T, 3, 2, 2, false>(a, st);
+    if (cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_u<T, 9, 2, 2, true>(a, st);
   } else {
-    if (!cplx && rx == 2 && ry == 4) return launch_blk_b<T, 2, 4, false>(a, group, st);
-    if (cplx && rx == 2 && ry == 2) return launch_blk_b<T, 2, 2, true>(a, group, st);
+    if (cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_u<T, 9, 2, 2, true>(a, st);
+    if (cplx && rx == 2 && ry == 2 && group == 3) return launch_blk_u<T, 3, 2, 2, true>(a, st);
+    if (!cplx && rx == 2 && ry == 4 && group == 1) return launch_blk_u<T, 1, 2, 4, false>(a, st);
   }
   set_error("launch_pass_blk: no kernel for this cell block");
   return HPSI_ERR_UNSUPPORTED;

@@ -20,8 +20,8 @@ TOL32 = 2e-5
 LEGACY = {"HPSI_PASS_SHAPE64": "4,2,0,0,0", "HPSI_PASS_SHAPE32": "8,4,0,0,0"}
 # blocked pass: "chunk,ry,zb,group,1,rx,complex"
 BLK_REAL = {"HPSI_PASS_SHAPE64": "8,2,{zb},3,1,2,0", "HPSI_PASS_SHAPE32": "16,4,{zb},1,1,2,0"}
-BLK_CPLX = {"HPSI_PASS_SHAPE64": "8,2,{zb},1,1,2,1", "HPSI_PASS_SHAPE32": "16,2,{zb},3,1,2,1"}
-PATHS = ["blk_real", "blk_cplx", "legacy"]
+BLK_CPLX = {"HPSI_PASS_SHAPE64": "8,2,{zb},9,1,2,1", "HPSI_PASS_SHAPE32": "16,2,{zb},3,1,2,1"}
+PATHS = ["default", "blk_real", "blk_cplx", "legacy"]
 
 
 def _setup(mesh, v=None, proj=None):
@@ -48,6 +48,10 @@ def _dev(x, cuda, ld, dtype):
 
 
 def _set_path(monkeypatch, path, zb=0):
+    if path == "default":
+        for k in LEGACY:
+            monkeypatch.delenv(k, raising=False)
+        return
     env = {"legacy": LEGACY, "blk_real": BLK_REAL, "blk_cplx": BLK_CPLX}[path]
     for k, v in env.items():
         monkeypatch.setenv(k, v.format(zb=zb))
