@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--impl", default="hpsi", choices=["hpsi", "reference"])
     ap.add_argument("--small", action="store_true", help="small case (for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--configs", action="store_true",
+                    help="instead of the headline line, one line per other configuration "
+                         "(64^3 box, 2000-step TD, 64 grouped systems, adjoint gradient)")
     return ap.parse_args()
 
 
@@ -223,6 +226,144 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _cuda_ms(fn, reps, warm=2):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_configs(args):
+    """The configurations other than the headline, one JSON line each (1 GPU).
+
+    Time steps: the order-4 star Laplacian has E_max = 9.75 / h^2 Ha (244 Ha at
+    h = 0.2, 156 Ha at h = 0.25) and the 4th-order Taylor series is stable only
+    for dt * E_max <= 2 sqrt(2), so the TD run on the h = 0.2 sphere uses
+    dt = 0.005 and the adjoint run on the h = 0.25 box dt = 0.01 (dt = 0.02
+    diverges on these grids in any implementation of the method).
+    """
+    import torch
+    from hpsi import fixtures, lib
+    from hpsi.mesh import index_box_mesh
+    from hpsi.stencil import laplacian_weights, star_points
+    dev = torch.device("cuda", 0)
+
+    def emit(d):
+        print(json.dumps(d), flush=True)
+
+    # ---- 64^3 box, kinetic + local, 32 states ----------------------------------
+    s0 = fixtures.config0()
+    m = s0.mesh
+    dm = lib.DeviceMesh(m)
+    ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=s0.v)
+    x = torch.from_numpy(s0.psi).to(dev)
+    y = torch.zeros((m.np, 32), dtype=torch.complex128, device=dev)
+    ms64 = _cuda_ms(lambda: ham.apply(x, y), 20)
+    x32, y32 = x.to(torch.complex64), y.to(torch.complex64)
+    ms32 = _cuda_ms(lambda: ham.apply(x32, y32), 20)
+    emit({"config": "box 64^3 h=0.25, 32 states, kinetic + local (no KB)", "unit": UNIT,
+          "fp64": {"value": m.np * 32 / ms64 / 1e6, "ms": ms64}, "fp32": {"value": m.np * 32 / ms32 / 1e6, "ms": ms32},
+          "alg_bytes_fp64_per_apply": m.np * 32 * 32 + m.np * 8})
+    del ham, dm, x, y, x32, y32
+
+    # ---- TD: config-1 system, laser, 2000 steps, FP32 graph vs FP64 plain --------
+    s1 = build_system(args.small)
+    m = s1.mesh
+    dm = lib.DeviceMesh(m)
+    ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=s1.v, projectors=s1.proj)
+    nsteps = 200 if args.small else 2000
+    dt = 0.005
+    laser = dict(E0=0.01, omega=0.057, T=nsteps * dt)
+    res = {}
+    for name, dtype, graph in (("fp64_plain", torch.complex128, False), ("fp32_graph", torch.complex64, True)):
+        xs = torch.from_numpy(s1.psi).to(dev).to(dtype)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        E, D, N = ham.td_propagate(xs, nsteps, dt, graph=graph, **laser)
+        el = time.perf_counter() - t0
+        res[name] = (nsteps / el, E, D, N)
+        del xs
+    (r64, E64, D64, N64), (r32, E32, D32, N32) = res["fp64_plain"], res["fp32_graph"]
+    emit({"config": f"TD exp_mid, sphere R=12 h=0.2, 128 states, KB, laser E0=0.01 w=0.057 sin^2, "
+                    f"{nsteps} steps dt={dt}", "unit": "TD steps/s",
+          "fp64_plain": r64, "fp32_graph": r32, "speedup_fp32_graph": r32 / r64,
+          "energy_rel_err_max": float(np.max(np.abs(E32 - E64) / np.abs(E64))),
+          "dipole_abs_err_max": float(np.max(np.abs(D32 - D64))),
+          "dipole_rel_err_max": float(np.max(np.abs(D32 - D64)) / max(np.max(np.abs(D64)), 1e-300)),
+          "norm_rel_err_max": float(np.max(np.abs(N32 - N64) / N64))})
+    del ham, dm
+
+    # ---- 64 grouped systems of uneven size, 100 Taylor steps -----------------------
+    rng = np.random.default_rng(2024)
+    nsys = 16 if args.small else 64
+    sides = np.exp(rng.uniform(np.log(32), np.log(96), nsys)).astype(int)
+    nsts = np.exp(rng.uniform(np.log(4), np.log(64), nsys)).astype(int)
+    atoms = rng.integers(2, 17, nsys)
+    hams, dms, xs64 = [], [], []
+    pts = 0
+    for i in range(nsys):
+        n = int(sides[i])
+        mm = index_box_mesh((n, n, n), 0.25)
+        v = fixtures.soft_coulomb(mm, rng)
+        proj = fixtures.kb_projectors(mm, int(atoms[i]), rng, radius=2.0, min_dist=2.0,
+                                      place_radius=0.45 * n * 0.25)
+        d_ = lib.DeviceMesh(mm)
+        h_ = lib.Hamiltonian(d_, laplacian_weights(mm.spacing), star_points(), v=v, projectors=proj)
+        nst = int(nsts[i])
+        ld = 8 * ((nst + 7) // 8)
+        xx = torch.zeros((mm.np_part, ld), dtype=torch.complex128, device=dev)
+        f = rng.standard_normal((mm.np, nst)) + 1j * rng.standard_normal((mm.np, nst))
+        xx[: mm.np, :nst] = torch.from_numpy(f / np.sqrt(mm.np * mm.vol_pp))
+        dms.append(d_)
+        hams.append(h_)
+        xs64.append(xx)
+        pts += mm.np * nst
+    grp = lib.Group(hams)
+    out = {}
+    steps = 100
+    for name, dtype in (("fp64", torch.complex128), ("fp32", torch.complex64)):
+        ys = [xx.to(dtype) for xx in xs64]
+        grp.taylor_steps(ys, 2, 0.01)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        grp.taylor_steps(ys, steps, 0.01)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        out[name] = {"steps_per_s": steps / el, "Gpoint_states_per_s": pts * steps * 4 / el / 1e9}
+        del ys
+    emit({"config": f"{nsys} systems, cubic sides {int(sides.min())}..{int(sides.max())} (h=0.25), "
+                    f"{int(nsts.min())}..{int(nsts.max())} states, 2..16 KB atoms; {steps} Taylor-4 steps dt=0.01, "
+                    "persistent grouped launch + CUDA graph", "unit": "group steps/s (H.psi point-states/s: 4 per step)",
+          "total_point_states": int(pts), **out})
+    grp.close()
+    del hams, dms, xs64
+
+    # ---- adjoint gradient: 64^3, 16 states, 500 steps, checkpoint every 25 ----------
+    s0 = fixtures.config0(nst=16)
+    m = s0.mesh
+    dm = lib.DeviceMesh(m)
+    ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=s0.v)
+    nsteps = 100 if args.small else 500
+    eps = np.random.default_rng(7).normal(0.0, 0.005, nsteps)
+    psi0 = torch.from_numpy(s0.psi).to(dev)
+    tg = torch.from_numpy(fixtures.random_states(m, 16, np.random.default_rng(8))).to(dev)
+    ham.adjoint_gradient(psi0, tg, eps[:4], 0.01, ckpt=2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, ge, gv, gc = ham.adjoint_gradient(psi0, tg, eps, 0.01, ckpt=25)
+    el = time.perf_counter() - t0
+    emit({"config": f"adjoint gradient, box 64^3 h=0.25, 16 states, {nsteps} steps dt=0.01, checkpoint 25",
+          "unit": "s per gradient", "seconds": el, "forward_equiv_steps_per_s": nsteps / el, "J": J,
+          "grad_eps_norm": float(np.linalg.norm(ge)), "grad_v_norm": float(np.linalg.norm(gv))})
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -230,6 +371,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.configs:
+        if rank == 0:
+            run_configs(args)
+        return
 
     import torch
     import torch.distributed as dist

@@ -218,7 +218,8 @@ hpsi_status hpsi_group_taylor_steps(hpsi_group *group, hpsi_batch *psis,
 /* Autotuner: times the candidate shapes of the fused stencil pass (state chunk
  * width, z block depth) on scratch batches of width ld and storage dtype and
  * keeps the fastest for this Hamiltonian's later calls with that width.
- * shape_out (optional): {state chunk, rows per thread, z block, tile edge};
+ * shape_out (optional): {state chunk, rows per thread, z block, tile height
+ * (16: one-complex-per-thread pass, 8: register-blocked pass)};
  * ms_out: time of one pass with that shape. */
 hpsi_status hpsi_autotune(hpsi_hamiltonian *ham, int32_t dtype, int64_t ld,
                           int32_t shape_out[4], double *ms_out, void *stream);

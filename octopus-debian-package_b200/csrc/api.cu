@@ -1021,7 +1021,7 @@ hpsi_status prepare_taylor_workspaces(hpsi_hamiltonian *h, long long ld, size_t 
     p.nmat = h->nmat;
     p.psi_ld = ld;
     p.min_npoints = h->min_npoints;
-    s = h->bra_partial.ensure(size_t(bra_ksplit(p, m->num_sms)) * h->nprojections * ld * 2 * elem);
+    s = h->bra_partial.ensure(size_t(bra_ksplit(p, m->num_sms)) * h->nprojections * ld * 2 * sizeof(double));
     if (s) return s;
     if (obs) {
       s = h->ketobs.ensure(size_t(ket_row_blocks(h->nk)) * ld * 2 * sizeof(double));

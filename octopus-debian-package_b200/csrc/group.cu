@@ -19,14 +19,16 @@
 
 #include "api_internal.cuh"
 #include "projector.cuh"
+#include "stencil_blk.cuh"
 
 namespace hpsi {
 
 PassShape pass_shape(const hpsi_hamiltonian *h, int dtype, long long ld);
 PassShape default_shape(int dtype, long long ld);
 int pass_sc(int dtype, long long ld);
-int choose_zb(const hpsi_mesh *m, int chunks);
-hpsi_status mesh_items(hpsi_mesh *m, int zb, const int4 **items, int *nitems);
+int choose_zb(const hpsi_mesh *m, int chunks, int ty);
+hpsi_status mesh_items(hpsi_mesh *m, int zb, int ty, const int4 **items, int *nitems);
+PassShape blk_shape(int dtype);
 const int *load_map(const hpsi_hamiltonian *h, int set_bc);
 hpsi_status prepare_taylor_workspaces(hpsi_hamiltonian *h, long long ld, size_t elem, bool obs);
 template <typename T>
@@ -40,6 +42,8 @@ hpsi_status run_ket(hpsi_hamiltonian *h, const T *proj, long long ld, int nst, T
                     double a_re, double a_im, const T *psi0, long long psi0_ld, double *obs, cudaStream_t st);
 template <typename T>
 hpsi_status launch_pass(PassArgs a, const PassShape &shape, cudaStream_t st);
+template <typename T>
+hpsi_status launch_pass_any(const PassArgs &a, const PassShape &shape, long long in_rows, cudaStream_t st);
 
 namespace {
 template <typename T>
@@ -62,6 +66,7 @@ struct hpsi_group {
   std::vector<Launch> launches;
   long long built_ld_sig = -1;  // signature of the batch widths the units were built for
   int built_dtype = -1, sc = 0;
+  bool blk = false;             // every width fits the blocked pass's chunk
   std::vector<hpsi::PassShape> shapes;
   int *d_counter = nullptr;     // one counter per launch sub-group
   cudaStream_t cap = nullptr;
@@ -83,15 +88,28 @@ static hpsi_status group_build(hpsi_group *g, int dtype, const std::vector<long 
   if (sig == g->built_ld_sig && !g->launches.empty()) return HPSI_OK;
   group_free_units(g);
   const int n = int(g->hams.size());
-  // common state chunk: the smallest preferred chunk over the systems
-  int sc = dtype == HPSI_C128 ? 4 : 8;
   g->shapes.assign(n, PassShape{});
-  for (int s = 0; s < n; ++s) {
+  // the blocked pass when every width is a multiple of its chunk
+  const PassShape bs = blk_shape(dtype);
+  g->blk = true;
+  for (int s = 0; s < n; ++s) g->blk = g->blk && ld[s] % bs.sc == 0;
+  if (g->blk) {
+    for (int s = 0; s < n; ++s) g->shapes[s] = default_shape(dtype, ld[s]);
+    for (int s = 0; s < n; ++s)
+      if (!g->shapes[s].blk || g->shapes[s].rx != g->shapes[0].rx || g->shapes[s].ry != g->shapes[0].ry ||
+          g->shapes[s].cplx != g->shapes[0].cplx || g->shapes[s].unroll != g->shapes[0].unroll) {
+        g->blk = false;
+        break;
+      }
+  }
+  // common state chunk: the smallest preferred chunk over the systems
+  int sc = g->blk ? bs.sc : (dtype == HPSI_C128 ? 4 : 8);
+  for (int s = 0; s < n && !g->blk; ++s) {
     PassShape sh = pass_shape(g->hams[s], dtype, ld[s]);
-    sc = std::min(sc, sh.sc);
+    sc = std::min(sc, sh.blk ? (dtype == HPSI_C128 ? 4 : 8) : sh.sc);
     g->shapes[s] = sh;
   }
-  for (int s = 0; s < n; ++s) {
+  for (int s = 0; s < n && !g->blk; ++s) {
     if (ld[s] % sc) {
       set_error("hpsi_group: batch width incompatible with the common state chunk");
       return HPSI_ERR_UNSUPPORTED;
@@ -99,7 +117,8 @@ static hpsi_status group_build(hpsi_group *g, int dtype, const std::vector<long 
     g->shapes[s].sc = sc;
     g->shapes[s].ry = dtype == HPSI_C128 ? 2 : 4;
     g->shapes[s].tx = g->shapes[s].ty = 16;
-    g->shapes[s].blk = 0;  // the persistent group kernel is the one-complex-per-thread pass
+    g->shapes[s].blk = 0;  // the one-complex-per-thread pass
+    g->shapes[s].zb = 0;
   }
   g->sc = sc;
   for (int first = 0; first < n; first += GROUP_MAX) {
@@ -110,11 +129,12 @@ static hpsi_status group_build(hpsi_group *g, int dtype, const std::vector<long 
     for (int s = L.first; s < L.end; ++s) {
       hpsi_hamiltonian *h = g->hams[s];
       const int chunks = int(ld[s] / sc);
-      const int zb = g->shapes[s].zb > 0 ? g->shapes[s].zb : choose_zb(h->mesh, chunks);
+      const int ty = g->blk ? 8 : 16;
+      const int zb = g->shapes[s].zb > 0 ? g->shapes[s].zb : choose_zb(h->mesh, chunks, ty);
       g->shapes[s].zb = zb;
       const int4 *items;
       int nitems = 0;
-      hpsi_status st = mesh_items(h->mesh, zb, &items, &nitems);
+      hpsi_status st = mesh_items(h->mesh, zb, ty, &items, &nitems);
       if (st) return st;
       // the items live on the device; recompute their z extents on the host for the cost
       std::vector<int4> hi(nitems);
@@ -169,7 +189,9 @@ static hpsi_status group_step(hpsi_group *g, const std::vector<T *> &psi, const 
       ga.counter = g->d_counter + li;
       HPSI_TRY_CUDA(cudaMemsetAsync(ga.counter, 0, sizeof(int), st));
       ProfScope prof(sizeof(T) == 8 ? "group_pass_fp64" : "group_pass_fp32", st);
-      hpsi_status r = launch_pass_group<T>(ga, g->sc, g->num_sms, st);
+      const PassShape &s0 = g->shapes[L.first];
+      hpsi_status r = g->blk ? launch_pass_blk_group<T>(ga, s0.rx, s0.ry, s0.cplx, s0.unroll, g->num_sms, st)
+                             : launch_pass_group<T>(ga, g->sc, g->num_sms, st);
       if (r) return r;
     }
     for (int s = 0; s < n; ++s) {
@@ -268,6 +290,29 @@ static hpsi_status autotune_t(hpsi_hamiltonian *h, int dtype, long long ld, cuda
     if (ld % sc) continue;
     for (int zb : {0, 16, 24, 32, 48, 64, 96, 1 << 20}) cands.push_back(PassShape{sc, 16, 16, ry, zb});
   }
+  // blocked pass: the instantiated cell blocks x z block depths
+  const PassShape b0 = blk_shape(dtype);
+  if (ld % b0.sc == 0) {
+    std::vector<PassShape> blocks{b0};
+    PassShape b1 = b0, b2 = b0;
+    if (dtype == HPSI_C128) {
+      b1.unroll = 3;  // real lanes, groups of 3 planes
+      b2.cplx = 1;    // complex states, groups of 9
+    } else {
+      b1.unroll = 3;  // complex states, groups of 3
+      b2.cplx = 0;    // real lanes 2 x 4, groups of 1
+      b2.ry = 4;
+      b2.unroll = 1;
+    }
+    blocks.push_back(b1);
+    blocks.push_back(b2);
+    for (const auto &b : blocks)
+      for (int zb : {0, 16, 32, 48, 64, 1 << 20}) {
+        PassShape c = b;
+        c.zb = zb;
+        cands.push_back(c);
+      }
+  }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -279,10 +324,10 @@ static hpsi_status autotune_t(hpsi_hamiltonian *h, int dtype, long long ld, cuda
                            static_cast<const T *>(in), ld, static_cast<T *>(out), ld, ld, PASS_APPLY, nullptr, 0,
                            0.0, 0.0, sh, a);
     if (r) break;
-    for (int i = 0; i < 2 && !r; ++i) r = launch_pass<T>(a, sh, st);
+    for (int i = 0; i < 2 && !r; ++i) r = launch_pass_any<T>(a, sh, m->np, st);
     cudaEventRecord(e0, st);
     const int reps = 5;
-    for (int i = 0; i < reps && !r; ++i) r = launch_pass<T>(a, sh, st);
+    for (int i = 0; i < reps && !r; ++i) r = launch_pass_any<T>(a, sh, m->np, st);
     cudaEventRecord(e1, st);
     if (r) break;
     cudaEventSynchronize(e1);
@@ -372,7 +417,7 @@ hpsi_status hpsi_autotune(hpsi_hamiltonian *h, int32_t dtype, int64_t ld, int32_
     shape_out[0] = t.shape.sc;
     shape_out[1] = t.shape.ry;
     shape_out[2] = t.shape.zb;
-    shape_out[3] = t.shape.tx;
+    shape_out[3] = t.shape.ty;
   }
   if (ms_out) *ms_out = t.ms;
   return HPSI_OK;

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
     for (int i = tid; i < KB * CPR; i += 128) {
       const int k = i / CPR, part = i % CPR;
       T *d = &sA[b][k][part * EPC];
-      if (k0 + k < npts) {
+      if (k0 + k < npts && l0 + part * EPC < ld2) {
         const int row = __ldg(map + k0 + k);
         cp_async16(d, psi + row * ld2 + l0 + part * EPC);
       } else {
@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
   }
   // C fragment: row (lane) = ln >> 2, cols (projectors) = (ln & 3) * 2 + {0,1}
   const int lane = l0 + warp * 8 + (ln >> 2);
+  if (lane >= ld2) return;  // lanes past the batch width (zero-filled above)
   double *out = p.partial + ((long long)blockIdx.z * p.nprojections + p.proj_row[m]) * 2 * p.proj_ld;
 #pragma unroll
   for (int nt = 0; nt < 2; ++nt) {
@@ -173,8 +174,9 @@ template <typename T>
 hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStream_t st) {
   if (p.nmat == 0) return HPSI_OK;
   const long long ld2 = 2 * p.psi_ld;
-  if (use_tensor && p.max_nproj <= NMAX && ld2 % LANES == 0) {
-    dim3 grid(p.nmat, unsigned(ld2 / LANES), ksplit);
+  // the staged rows are copied in 16-byte pieces: FP32 needs an even width
+  if (use_tensor && p.max_nproj <= NMAX && ld2 % (16 / sizeof(T)) == 0) {
+    dim3 grid(p.nmat, unsigned((ld2 + LANES - 1) / LANES), ksplit);
     bra_dmma_kernel<T><<<grid, 128, 0, st>>>(p);
     HPSI_CHECK_LAUNCH();
     const long long n = (long long)p.nprojections * ld2;

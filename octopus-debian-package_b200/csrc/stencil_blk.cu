@@ -141,20 +141,17 @@ __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, i
 // Plane k of a CTA is halo plane zbeg + k: data stage k % NBUF, side slot
 // k % NSIDE.  Iteration k computes plane k and issues the data of plane
 // k + NBUF - 1 and the side data of plane k + 2 NBUF - 2 (one commit group).
+// One work unit: item ih (16 x 8 tile, z block) and state chunk `chunk`.
 template <typename T, bool HORNER, bool OBS, int U, int RX_, int RY_, bool CPLX>
-__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_, CPLX>::NT, 1)
-    pass_blk_kernel(const __grid_constant__ PassArgs p) {
+__device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const int chunk, unsigned char *smem) {
   constexpr bool X0 = HORNER || OBS;
   using LY = BlkLayout<T, X0, RX_, RY_, CPLX>;
   using E = typename BlkElem<T, CPLX>::E;
   constexpr int SLE = LY::SLE;
   constexpr int SL = LY::SL, RX = LY::RX, RY = LY::RY, TX = LY::TX, TY = LY::TY, HAL = LY::HAL;
   constexpr int HX = LY::HX, NBUF = LY::NBUF, NSIDE = LY::NSIDE, PCS = LY::PCS, EPP = LY::EPP;
-  extern __shared__ __align__(16) unsigned char smem[];
 
   const CellBox &B = p.box;
-  const int chunk = blockIdx.x % p.chunks;
-  const int ih = blockIdx.x / p.chunks;  // work item (16 x 8 tile, z block)
   const int4 it = p.items[ih];
   const int cx0 = HAL + it.x * TX, cy0 = HAL + it.y * TY;
   const int zs = it.z, ze = it.w;
@@ -512,6 +509,32 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX_, RY_, CPLX>::N
 }
 
 template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX>
+__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX>::NT, 1)
+    pass_blk_kernel(const __grid_constant__ PassArgs p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  blk_body<T, HORNER, OBS, U, RX, RY, CPLX>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem);
+}
+
+// Many systems in one persistent launch (Horner passes): each CTA takes
+// (system, item, chunk) units from a list sorted by cost until it is empty.
+template <typename T, int U, int RX, int RY, bool CPLX>
+__global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX>::NT, 1)
+    pass_blk_group_kernel(const __grid_constant__ GroupArgs g) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int unit_s;
+  for (;;) {
+    if (threadIdx.x == 0) unit_s = atomicAdd(g.counter, 1);
+    __syncthreads();
+    const int u = unit_s;
+    __syncthreads();
+    if (u >= g.nunits) break;
+    const int4 W = g.units[u];  // {system, item, chunk, -}
+    blk_body<T, true, false, U, RX, RY, CPLX>(g.sys[W.x], W.y, W.z, smem);
+    __syncthreads();
+  }
+}
+
+template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX>
 hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
   using LY = BlkLayout<T, HORNER || OBS, RX, RY, CPLX>;
   auto kern = pass_blk_kernel<T, HORNER, OBS, U, RX, RY, CPLX>;
@@ -536,7 +559,38 @@ hpsi_status launch_blk_u(const PassArgs &a, cudaStream_t st) {
   return launch_blk_mode<T, false, false, U, RX, RY, CPLX>(a, st);
 }
 
+template <typename T, int U, int RX, int RY, bool CPLX>
+hpsi_status launch_blk_group_v(const GroupArgs &g, int grid, cudaStream_t st) {
+  using LY = BlkLayout<T, true, RX, RY, CPLX>;
+  auto kern = pass_blk_group_kernel<T, U, RX, RY, CPLX>;
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [&] {
+    attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LY::bytes));
+  });
+  HPSI_TRY_CUDA(attr);
+  kern<<<grid, LY::NT, LY::bytes, st>>>(g);
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+
 }  // namespace
+
+template <typename T>
+hpsi_status launch_pass_blk_group(const GroupArgs &g, int rx, int ry, int cplx, int group, int num_sms,
+                                  cudaStream_t st) {
+  if (g.nunits == 0) return HPSI_OK;
+  const int grid = std::min(g.nunits, num_sms);
+  if constexpr (sizeof(T) == 8) {
+    if (!cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_group_v<T, 9, 2, 2, false>(g, grid, st);
+  } else {
+    if (cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_group_v<T, 9, 2, 2, true>(g, grid, st);
+  }
+  set_error("launch_pass_blk_group: no kernel for this cell block");
+  return HPSI_ERR_UNSUPPORTED;
+}
+template hpsi_status launch_pass_blk_group<double>(const GroupArgs &, int, int, int, int, int, cudaStream_t);
+template hpsi_status launch_pass_blk_group<float>(const GroupArgs &, int, int, int, int, int, cudaStream_t);
 
 template <typename T>
 int blk_chunk_states() {

@@ -25,4 +25,10 @@ bool blk_pass_eligible(const PassArgs &a, long long ld);
 template <typename T>
 hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int cplx, int group, cudaStream_t st);
 
+// Grouped systems in one persistent launch (Horner passes): every system's
+// arguments built with the blocked shape (items over 16 x 8 tiles).
+template <typename T>
+hpsi_status launch_pass_blk_group(const GroupArgs &g, int rx, int ry, int cplx, int group, int num_sms,
+                                  cudaStream_t st);
+
 }  // namespace hpsi

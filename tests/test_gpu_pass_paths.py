@@ -170,3 +170,30 @@ def test_host_batches_pipelined(cuda, dtype, ld, set_bc):
     # slabs change the projector split-K sums (rounding only)
     tol = 1e-13 if dtype == np.complex128 else 1e-6
     assert rel_maxnorm_per_state(yh.numpy().astype(np.complex128), y.cpu().numpy().astype(np.complex128)) <= tol
+
+
+@pytest.mark.parametrize("dtype,ld", [(np.complex128, 3), (np.complex64, 6), (np.complex64, 10), (np.complex128, 40)])
+def test_projector_bra_widths(cuda, dtype, ld):
+    """KB bra on the FP64 tensor cores for any batch width (lanes past the
+    width zero-filled; FP32 rows are 16-byte aligned only for even widths,
+    which the library requires)."""
+    import torch
+    m, v, proj, psi = small_sphere_system(seed=61, nst=ld, radius=4.2, natoms=4)
+    dm, ham, w, pts = _setup(m, v=v, proj=proj)
+    ref = _oracle(m, w, pts, v=v, proj=proj).apply(psi)
+    x = _dev(psi, cuda, ld, dtype)
+    y = torch.zeros((m.np, ld), dtype=x.dtype, device=cuda)
+    ham.apply(x, y)
+    tol = TOL64 if dtype == np.complex128 else TOL32
+    assert rel_maxnorm_per_state(y.cpu().numpy().astype(np.complex128), ref) <= tol
+
+
+def test_odd_fp32_width_rejected(cuda):
+    import torch
+    from hpsi import lib
+    m, v, proj, psi = small_sphere_system(seed=61, nst=5, radius=3.6, natoms=2)
+    dm, ham, w, pts = _setup(m, v=v, proj=proj)
+    x = _dev(psi, cuda, 5, np.complex64)
+    y = torch.zeros((m.np, 5), dtype=x.dtype, device=cuda)
+    with pytest.raises(lib.HpsiError, match="16-byte"):
+        ham.apply(x, y)
