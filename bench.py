@@ -66,7 +66,7 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(path="profiles/pass_fp64_sphere128.md"):
+def profile_traffic(path="profiles/pass_blk_fp64_sphere64.md"):
     """dram bytes per launch of the pass kernel from the committed ncu summary."""
     try:
         with open(os.path.join(ROOT, path)) as f:
@@ -442,7 +442,7 @@ def main():
 
     # roofline of the dominant kernel (fused stencil pass)
     S = 16
-    alg_bytes = m.np * nst * 2 * S + m.np * 8.0
+    alg_bytes = m.np * nst * 2 * S + m.np * 8.0  # read psi + write H psi, read v
     pass_avg_ms = pass_ms / max(npass, 1)
     achieved = alg_bytes / (pass_avg_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
@@ -514,7 +514,7 @@ def main():
                     "d2h_bytes_per_step": int(m.np * nst * S)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "pass_fp64 (fused stencil + local potential)",
+                         "kernel": "pass_blk_kernel FP64 (fused stencil + local potential)",
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": pass_avg_ms},
             "kernels": {"pass_fp64": {"launches": npass, "ms": pass_ms},
                         "bra_fp64": {"launches": nbra, "ms": bra_ms},

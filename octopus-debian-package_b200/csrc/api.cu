@@ -761,6 +761,14 @@ hpsi_status mesh_items(hpsi_mesh *m, int zb, int ty, const int4 **items, int *ni
         if (t.y < 0) continue;
         for (int z = t.x; z <= t.y; z += zb) v.push_back(make_int4(bx, by, z, std::min(z + zb, t.y + 1)));
       }
+    // launch order: by z band, then raster over the tiles, so that the CTAs in
+    // flight together are spatial neighbours and share their halo rows in L2
+    std::stable_sort(v.begin(), v.end(), [zb](const int4 &a, const int4 &b) {
+      const int za = a.z / zb, zbb = b.z / zb;
+      if (za != zbb) return za < zbb;
+      if (a.y != b.y) return a.y < b.y;
+      return a.x < b.x;
+    });
     int4 *d = nullptr;
     hpsi_status s = dev_alloc(reinterpret_cast<void **>(&d), std::max<size_t>(1, v.size()) * sizeof(int4));
     if (s) return s;
