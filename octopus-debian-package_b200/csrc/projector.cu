@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(128) bra_simt_kernel(const ProjArgs p) {
 int bra_ksplit(const ProjArgs &p, int num_sms) {
   const long long ld2 = 2 * p.psi_ld;
   const long long base = (long long)p.nmat * ((ld2 + LANES - 1) / LANES);
-  long long k = (4LL * num_sms + base - 1) / base;
+  long long k = (16LL * num_sms + base - 1) / base;
   k = std::min<long long>(k, std::max(1, p.min_npoints / 128));
   return int(std::max<long long>(1, std::min<long long>(k, 64)));
 }
@@ -210,7 +210,11 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
   C2 *out = static_cast<C2 *>(k.out);
   const C2 *psi0 = static_cast<const C2 *>(k.psi0);
   Kahan ke = {0, 0};
-  for (int i = blockIdx.y * 8 + threadIdx.y; i < k.nk; i += gridDim.y * 8) {
+  // each CTA row takes a contiguous range of covered rows: neighbouring rows
+  // lie in the same few spheres, so their projections stay in L1
+  const int per = (k.nk + gridDim.y - 1) / gridDim.y;
+  const int r0 = blockIdx.y * per, r1 = min(k.nk, r0 + per);
+  for (int i = r0 + threadIdx.y; i < r1; i += 8) {
     if (!active) continue;
     const int row = k.krows[i];
     C2 h;

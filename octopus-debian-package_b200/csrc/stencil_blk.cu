@@ -393,6 +393,10 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
     if (zo >= zs) {
       const int *rows = reinterpret_cast<const int *>(side(k) + LY::s_rows);
       const E *x0s = reinterpret_cast<const E *>(st + LY::o_psi0) + l;
+      double pe = 0.0, pn = 0.0, pd = 0.0;
+      (void)pe;
+      (void)pn;
+      (void)pd;
 #pragma unroll
       for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
@@ -426,12 +430,19 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
               eh = double(x0) * double(h);
               n2 = double(x0) * double(x0);
             }
-            kadd(ke, eh);
-            kadd(kn, n2);
-            kadd(kd, n2 * rr);
+            pe += eh;
+            pn += n2;
+            pd += n2 * rr;
           }
           out[row * out_lde + ocol] = val;
         }
+      if constexpr (OBS) {
+        // one compensated add per plane and quantity (the few cells of a
+        // plane are summed plainly first)
+        kadd(ke, pe);
+        kadd(kn, pn);
+        kadd(kd, pd);
+      }
     } else {
 #pragma unroll
       for (int cx = 0; cx < RX; ++cx)
