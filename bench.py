@@ -226,6 +226,29 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+class Ranks:
+    """One process per GPU: barrier and max over ranks (NCCL on the GPUs; the
+    CPU tests drive the same code over gloo)."""
+
+    def __init__(self, world, device):
+        self.world = world
+        self.device = device
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, v):
+        if self.world == 1:
+            return v
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+
 def _cuda_ms(fn, reps, warm=2):
     import torch
     for _ in range(warm):
@@ -396,16 +419,9 @@ def main():
     y = torch.zeros((m.np, nst), dtype=torch.complex128, device=dev)
     st = torch.cuda.current_stream()
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world, dev)
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):

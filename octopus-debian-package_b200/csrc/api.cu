@@ -217,8 +217,12 @@ PassShape default_shape(int dtype, long long ld) {
   if (env) {
     int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0, cx = -1;
     if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx) >= 2 && a > 0 && ld % a == 0) {
-      if (t && ld % blk_shape(dtype).sc == 0) {
-        s = blk_shape(dtype);  // fixed chunk: block, element, z depth and group are taken
+      if (t) {
+        s = blk_shape(dtype);  // chunk (128 or 64 bytes), block, element, z depth and group are taken
+        if (a == s.sc / 2) {
+          s.sc = a;  // 64-byte chunks ride 16 x 16 tiles
+          s.ty = 16;
+        }
         if (u == 1 || u == 3 || u == 9) s.unroll = u;
         if (x > 0) s.rx = x;
         if (b > 0) s.ry = b;
@@ -892,7 +896,7 @@ hpsi_status build_pass_args(hpsi_hamiltonian *h, int terms, const int *src_map, 
   a.a_re = a_re;
   a.a_im = a_im;
   a.chunks = int(ld / shape.sc);
-  const int ty = shape.blk ? 8 : 16;
+  const int ty = shape.blk ? shape.ty : 16;
   a.zb = shape.zb > 0 ? shape.zb : choose_zb(h->mesh, a.chunks, ty);
   return mesh_items(h->mesh, a.zb, ty, &a.items, &a.nitems);
 }
@@ -907,7 +911,7 @@ long long pass_in_rows(const hpsi_hamiltonian *h, const int *src_map) {
 template <typename T>
 hpsi_status launch_pass_any(const PassArgs &a, const PassShape &shape, long long in_rows, cudaStream_t st) {
   (void)in_rows;
-  if (shape.blk) return launch_pass_blk<T>(a, shape.rx, shape.ry, shape.cplx, shape.unroll, st);
+  if (shape.blk) return launch_pass_blk<T>(a, shape, st);
   return launch_pass<T>(a, shape, st);
 }
 template hpsi_status launch_pass_any<double>(const PassArgs &, const PassShape &, long long, cudaStream_t);
@@ -928,7 +932,7 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
     PassArgs chk = a;
     if (obs_partial) chk.obs = obs_partial;
     if (obs_partial && !psi0) chk.psi0 = in, chk.psi0_ld = in_ld;
-    if (!blk_pass_eligible<T>(chk, ld)) {
+    if (!blk_pass_eligible<T>(chk, ld, shape.sc)) {
       shape = legacy_shape(dtype, ld);
       si = build_pass_args<T>(h, terms, src_map, in, in_ld, out, out_ld, ld, mode, psi0, psi0_ld, a_re, a_im, shape,
                               a);
@@ -995,7 +999,7 @@ size_t obs_partial_bytes(hpsi_hamiltonian *h, long long ld) {
     const PassShape sh = pass_shape(h, dt, ld);
     const int4 *items;
     int nitems = 0;
-    const int ty = sh.blk ? 8 : 16;
+    const int ty = sh.blk ? sh.ty : 16;
     const int zb = sh.zb > 0 ? sh.zb : choose_zb(h->mesh, int(ld / sh.sc), ty);
     if (mesh_items(h->mesh, zb, ty, &items, &nitems) == HPSI_OK)
       n = std::max(n, size_t(nitems));

@@ -97,13 +97,14 @@ static hpsi_status group_build(hpsi_group *g, int dtype, const std::vector<long 
     for (int s = 0; s < n; ++s) g->shapes[s] = default_shape(dtype, ld[s]);
     for (int s = 0; s < n; ++s)
       if (!g->shapes[s].blk || g->shapes[s].rx != g->shapes[0].rx || g->shapes[s].ry != g->shapes[0].ry ||
-          g->shapes[s].cplx != g->shapes[0].cplx || g->shapes[s].unroll != g->shapes[0].unroll) {
+          g->shapes[s].cplx != g->shapes[0].cplx || g->shapes[s].unroll != g->shapes[0].unroll ||
+          g->shapes[s].sc != g->shapes[0].sc || g->shapes[s].ty != g->shapes[0].ty || ld[s] % g->shapes[s].sc) {
         g->blk = false;
         break;
       }
   }
   // common state chunk: the smallest preferred chunk over the systems
-  int sc = g->blk ? bs.sc : (dtype == HPSI_C128 ? 4 : 8);
+  int sc = g->blk ? g->shapes[0].sc : (dtype == HPSI_C128 ? 4 : 8);
   for (int s = 0; s < n && !g->blk; ++s) {
     PassShape sh = pass_shape(g->hams[s], dtype, ld[s]);
     sc = std::min(sc, sh.blk ? (dtype == HPSI_C128 ? 4 : 8) : sh.sc);
@@ -129,7 +130,7 @@ static hpsi_status group_build(hpsi_group *g, int dtype, const std::vector<long 
     for (int s = L.first; s < L.end; ++s) {
       hpsi_hamiltonian *h = g->hams[s];
       const int chunks = int(ld[s] / sc);
-      const int ty = g->blk ? 8 : 16;
+      const int ty = g->blk ? g->shapes[s].ty : 16;
       const int zb = g->shapes[s].zb > 0 ? g->shapes[s].zb : choose_zb(h->mesh, chunks, ty);
       g->shapes[s].zb = zb;
       const int4 *items;
@@ -190,7 +191,7 @@ static hpsi_status group_step(hpsi_group *g, const std::vector<T *> &psi, const 
       HPSI_TRY_CUDA(cudaMemsetAsync(ga.counter, 0, sizeof(int), st));
       ProfScope prof(sizeof(T) == 8 ? "group_pass_fp64" : "group_pass_fp32", st);
       const PassShape &s0 = g->shapes[L.first];
-      hpsi_status r = g->blk ? launch_pass_blk_group<T>(ga, s0.rx, s0.ry, s0.cplx, s0.unroll, g->num_sms, st)
+      hpsi_status r = g->blk ? launch_pass_blk_group<T>(ga, s0, g->num_sms, st)
                              : launch_pass_group<T>(ga, g->sc, g->num_sms, st);
       if (r) return r;
     }
@@ -292,8 +293,9 @@ static hpsi_status autotune_t(hpsi_hamiltonian *h, int dtype, long long ld, cuda
   }
   // blocked pass: the instantiated cell blocks x z block depths
   const PassShape b0 = blk_shape(dtype);
-  if (ld % b0.sc == 0) {
-    std::vector<PassShape> blocks{b0};
+  if (ld % (b0.sc / 2) == 0) {
+    std::vector<PassShape> blocks;
+    if (ld % b0.sc == 0) blocks.push_back(b0);
     PassShape b1 = b0, b2 = b0;
     if (dtype == HPSI_C128) {
       b1.unroll = 3;  // real lanes, groups of 3 planes
@@ -304,8 +306,20 @@ static hpsi_status autotune_t(hpsi_hamiltonian *h, int dtype, long long ld, cuda
       b2.ry = 4;
       b2.unroll = 1;
     }
-    blocks.push_back(b1);
-    blocks.push_back(b2);
+    if (ld % b0.sc == 0) {
+      blocks.push_back(b1);
+      blocks.push_back(b2);
+    }
+    {
+      PassShape b3 = b0;  // 64-byte chunks, 16 x 16 tiles, 1 x 4 cells
+      b3.sc = b0.sc / 2;
+      b3.ty = 16;
+      b3.rx = 1;
+      b3.ry = 4;
+      b3.cplx = dtype == HPSI_C128 ? 0 : 1;
+      b3.unroll = 9;
+      blocks.push_back(b3);
+    }
     for (const auto &b : blocks)
       for (int zb : {0, 16, 32, 48, 64, 1 << 20}) {
         PassShape c = b;

@@ -82,23 +82,25 @@ __device__ __forceinline__ float2 fmae(float w, float2 v, float2 a) {
   return __ffma2_rn(make_float2(w, w), v, a);  // packed FP32 multiply-add (sm_100)
 }
 
-template <typename T, bool X0, int RX_, int RY_, bool CPLX_>
+template <typename T, bool X0, int RX_, int RY_, bool CPLX_, int TY_ = 8, int CB_ = 128>
 struct BlkLayout {
   static constexpr bool CPLX = CPLX_;
-  static constexpr int SL = blk_lanes<T>(), RX = RX_, RY = RY_;
+  static constexpr int SL = CB_ / int(sizeof(T)), RX = RX_, RY = RY_;
   static constexpr int LW = CPLX ? 2 : 1;  // reals per thread element
   static constexpr int SLE = SL / LW;      // thread elements per cell chunk
-  static constexpr int TX = BLK_TILE_X, TY = BLK_TILE_Y, HAL = 4;
+  static constexpr int TX = BLK_TILE_X, TY = TY_, HAL = 4;
   static constexpr int HX = TX + 2 * HAL, HY = TY + 2 * HAL;
   static constexpr int HC = HX * HY, IC = TX * TY;
   static constexpr int CELLB = SL * int(sizeof(T));  // bytes of one cell chunk
   static constexpr int PCS = CELLB / 16;             // 16-byte pieces per cell chunk
   static constexpr int EPP = 16 / int(sizeof(T));    // elements per piece
-  static_assert(CELLB == 128, "one cell chunk is 128 bytes");
+  static_assert(CELLB == 128 || CELLB == 64, "cell chunks of 64 or 128 bytes");
   static constexpr int NT = SLE * (TX / RX) * (TY / RY);
   static_assert(NT == 256 || NT == 512, "256 or 512 threads");
-  static_assert((HC * PCS) % NT == 0 && (IC * PCS) % NT == 0, "copy rounds tile the threads");
-  static constexpr int HROUNDS = HC * PCS / NT, IROUNDS = IC * PCS / NT;
+  // 16-byte copy rounds of a halo plane / an interior plane (the last round
+  // may be partial)
+  static constexpr int HROUNDS = (HC * PCS + NT - 1) / NT, IROUNDS = (IC * PCS + NT - 1) / NT;
+  static constexpr bool HPART = (HC * PCS) % NT != 0, IPART = (IC * PCS) % NT != 0;
   static constexpr int NBUF = X0 ? 3 : 4;   // data stages
   static constexpr int NSIDE = 2 * NBUF - 1;  // side slots (issued 2 NBUF - 2 planes ahead)
   static constexpr int SIDE_AHEAD = 2 * NBUF - 2;
@@ -142,10 +144,10 @@ __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, i
 // k % NSIDE.  Iteration k computes plane k and issues the data of plane
 // k + NBUF - 1 and the side data of plane k + 2 NBUF - 2 (one commit group).
 // One work unit: item ih (16 x 8 tile, z block) and state chunk `chunk`.
-template <typename T, bool HORNER, bool OBS, int U, int RX_, int RY_, bool CPLX>
+template <typename T, bool HORNER, bool OBS, int U, int RX_, int RY_, bool CPLX, int TY_, int CB_>
 __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const int chunk, unsigned char *smem) {
   constexpr bool X0 = HORNER || OBS;
-  using LY = BlkLayout<T, X0, RX_, RY_, CPLX>;
+  using LY = BlkLayout<T, X0, RX_, RY_, CPLX, TY_, CB_>;
   using E = typename BlkElem<T, CPLX>::E;
   constexpr int SLE = LY::SLE;
   constexpr int SL = LY::SL, RX = LY::RX, RY = LY::RY, TX = LY::TX, TY = LY::TY, HAL = LY::HAL;
@@ -213,6 +215,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 #pragma unroll
       for (int j = 0; j < LY::HROUNDS; ++j) {
         const int cell = cpc + j * (LY::NT / PCS);
+        if (LY::HPART && j == LY::HROUNDS - 1 && cell >= LY::HC) break;
         const int src = map[cell];
         cp_async16_zfill(halo + cell * SL, in_base + max(src, 0) * in_ld2, src >= 0 ? 16 : 0);
       }
@@ -220,6 +223,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 #pragma unroll 1
       for (int j = 0; j < LY::HROUNDS; ++j) {
         const int cell = cpc + j * (LY::NT / PCS);
+        if (LY::HPART && j == LY::HROUNDS - 1 && cell >= LY::HC) break;
         const int src = map[cell];
         T *d = halo + cell * SL;
         if (src >= 0) {
@@ -248,6 +252,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 #pragma unroll
       for (int j = 0; j < LY::IROUNDS; ++j) {
         const int cell = cpc + j * (LY::NT / PCS);
+        if (LY::IPART && j == LY::IROUNDS - 1 && cell >= LY::IC) break;
         const int row = rows[cell];
         const bool ok = row >= 0 && row < p.np;
         cp_async16_zfill(x0 + cell * SL, x0_base + (ok ? row : 0) * x0_ld2, ok ? 16 : 0);
@@ -519,17 +524,17 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   }
 }
 
-template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX>
-__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX>::NT, 1)
+template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX, int TY, int CB>
+__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::NT, 1)
     pass_blk_kernel(const __grid_constant__ PassArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
-  blk_body<T, HORNER, OBS, U, RX, RY, CPLX>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem);
+  blk_body<T, HORNER, OBS, U, RX, RY, CPLX, TY, CB>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem);
 }
 
 // Many systems in one persistent launch (Horner passes): each CTA takes
 // (system, item, chunk) units from a list sorted by cost until it is empty.
-template <typename T, int U, int RX, int RY, bool CPLX>
-__global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX>::NT, 1)
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
+__global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT, 1)
     pass_blk_group_kernel(const __grid_constant__ GroupArgs g) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int unit_s;
@@ -540,15 +545,15 @@ __global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX>::NT, 1)
     __syncthreads();
     if (u >= g.nunits) break;
     const int4 W = g.units[u];  // {system, item, chunk, -}
-    blk_body<T, true, false, U, RX, RY, CPLX>(g.sys[W.x], W.y, W.z, smem);
+    blk_body<T, true, false, U, RX, RY, CPLX, TY, CB>(g.sys[W.x], W.y, W.z, smem);
     __syncthreads();
   }
 }
 
-template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX>
+template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX, int TY, int CB>
 hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
-  using LY = BlkLayout<T, HORNER || OBS, RX, RY, CPLX>;
-  auto kern = pass_blk_kernel<T, HORNER, OBS, U, RX, RY, CPLX>;
+  using LY = BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>;
+  auto kern = pass_blk_kernel<T, HORNER, OBS, U, RX, RY, CPLX, TY, CB>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
@@ -561,19 +566,19 @@ hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
   return HPSI_OK;
 }
 
-template <typename T, int U, int RX, int RY, bool CPLX>
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
 hpsi_status launch_blk_u(const PassArgs &a, cudaStream_t st) {
   const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr;
-  if (horner && obs) return launch_blk_mode<T, true, true, U, RX, RY, CPLX>(a, st);
-  if (horner) return launch_blk_mode<T, true, false, U, RX, RY, CPLX>(a, st);
-  if (obs) return launch_blk_mode<T, false, true, U, RX, RY, CPLX>(a, st);
-  return launch_blk_mode<T, false, false, U, RX, RY, CPLX>(a, st);
+  if (horner && obs) return launch_blk_mode<T, true, true, U, RX, RY, CPLX, TY, CB>(a, st);
+  if (horner) return launch_blk_mode<T, true, false, U, RX, RY, CPLX, TY, CB>(a, st);
+  if (obs) return launch_blk_mode<T, false, true, U, RX, RY, CPLX, TY, CB>(a, st);
+  return launch_blk_mode<T, false, false, U, RX, RY, CPLX, TY, CB>(a, st);
 }
 
-template <typename T, int U, int RX, int RY, bool CPLX>
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
 hpsi_status launch_blk_group_v(const GroupArgs &g, int grid, cudaStream_t st) {
-  using LY = BlkLayout<T, true, RX, RY, CPLX>;
-  auto kern = pass_blk_group_kernel<T, U, RX, RY, CPLX>;
+  using LY = BlkLayout<T, true, RX, RY, CPLX, TY, CB>;
+  auto kern = pass_blk_group_kernel<T, U, RX, RY, CPLX, TY, CB>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
@@ -585,53 +590,72 @@ hpsi_status launch_blk_group_v(const GroupArgs &g, int grid, cudaStream_t st) {
   return HPSI_OK;
 }
 
+// chunk bytes of a shape: sc complex states of the storage type
+template <typename T>
+int shape_cb(const PassShape &s) {
+  return s.sc * 2 * int(sizeof(T));
+}
+
 }  // namespace
 
 template <typename T>
-hpsi_status launch_pass_blk_group(const GroupArgs &g, int rx, int ry, int cplx, int group, int num_sms,
-                                  cudaStream_t st) {
+hpsi_status launch_pass_blk_group(const GroupArgs &g, const PassShape &s, int num_sms, cudaStream_t st) {
   if (g.nunits == 0) return HPSI_OK;
   const int grid = std::min(g.nunits, num_sms);
+  const int cb = shape_cb<T>(s);
   if constexpr (sizeof(T) == 8) {
-    if (!cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_group_v<T, 9, 2, 2, false>(g, grid, st);
+    if (!s.cplx && s.rx == 2 && s.ry == 2 && s.unroll == 9 && s.ty == 8 && cb == 128)
+      return launch_blk_group_v<T, 9, 2, 2, false, 8, 128>(g, grid, st);
   } else {
-    if (cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_group_v<T, 9, 2, 2, true>(g, grid, st);
+    if (s.cplx && s.rx == 2 && s.ry == 2 && s.unroll == 9 && s.ty == 8 && cb == 128)
+      return launch_blk_group_v<T, 9, 2, 2, true, 8, 128>(g, grid, st);
   }
   set_error("launch_pass_blk_group: no kernel for this cell block");
   return HPSI_ERR_UNSUPPORTED;
 }
-template hpsi_status launch_pass_blk_group<double>(const GroupArgs &, int, int, int, int, int, cudaStream_t);
-template hpsi_status launch_pass_blk_group<float>(const GroupArgs &, int, int, int, int, int, cudaStream_t);
+template hpsi_status launch_pass_blk_group<double>(const GroupArgs &, const PassShape &, int, cudaStream_t);
+template hpsi_status launch_pass_blk_group<float>(const GroupArgs &, const PassShape &, int, cudaStream_t);
 
 template <typename T>
 int blk_chunk_states() {
-  return blk_lanes<T>() / 2;
+  return 128 / int(sizeof(T)) / 2;
 }
 
 template <typename T>
-bool blk_pass_eligible(const PassArgs &a, long long ld) {
-  if (ld % blk_chunk_states<T>() != 0) return false;
+bool blk_pass_eligible(const PassArgs &a, long long ld, int sc) {
+  if (ld % sc != 0) return false;
   if (reinterpret_cast<uintptr_t>(a.in) % 16 != 0 || reinterpret_cast<uintptr_t>(a.out) % 16 != 0) return false;
   if ((a.mode == PASS_HORNER || a.obs) && reinterpret_cast<uintptr_t>(a.psi0) % 16 != 0) return false;
   if ((2 * a.in_ld * sizeof(T)) % 16 != 0 || (2 * a.psi0_ld * sizeof(T)) % 16 != 0) return false;
   return true;
 }
 
-// Instantiated blocks (cells per thread, element, planes per group; all 512
-// threads): FP64 2 x 2 real lanes (group 9 or 3) or complex states (9);
-// FP32 2 x 2 complex states with packed multiply-adds (9 or 3) or 2 x 4 real
-// lanes (1).
+// Instantiated blocks (512 threads each):
+//   128-byte chunks, 16 x 8 tiles: FP64 2 x 2 real lanes (groups of 9 or 3)
+//     or complex states (9); FP32 2 x 2 complex states with packed
+//     multiply-adds (9 or 3) or 2 x 4 real lanes (1);
+//   64-byte chunks, 16 x 16 tiles (halo 2.25x instead of 3x): 1 x 4 cells,
+//     FP64 real lanes, FP32 complex states (groups of 9).
 template <typename T>
-hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int cplx, int group, cudaStream_t st) {
+hpsi_status launch_pass_blk(const PassArgs &a, const PassShape &s, cudaStream_t st) {
   if (a.nitems == 0) return HPSI_OK;
-  if constexpr (sizeof(T) == 8) {
-    if (!cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_u<T, 9, 2, 2, false>(a, st);
-    if (!cplx && rx == 2 && ry == 2 && group == 3) return launch_blk_u<T, 3, 2, 2, false>(a, st);
-    if (cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_u<T, 9, 2, 2, true>(a, st);
-  } else {
-    if (cplx && rx == 2 && ry == 2 && group == 9) return launch_blk_u<T, 9, 2, 2, true>(a, st);
-    if (cplx && rx == 2 && ry == 2 && group == 3) return launch_blk_u<T, 3, 2, 2, true>(a, st);
-    if (!cplx && rx == 2 && ry == 4 && group == 1) return launch_blk_u<T, 1, 2, 4, false>(a, st);
+  const int cb = shape_cb<T>(s), g = s.unroll;
+  if (s.ty == 8 && cb == 128) {
+    if constexpr (sizeof(T) == 8) {
+      if (!s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, false, 8, 128>(a, st);
+      if (!s.cplx && s.rx == 2 && s.ry == 2 && g == 3) return launch_blk_u<T, 3, 2, 2, false, 8, 128>(a, st);
+      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, true, 8, 128>(a, st);
+    } else {
+      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, true, 8, 128>(a, st);
+      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 3) return launch_blk_u<T, 3, 2, 2, true, 8, 128>(a, st);
+      if (!s.cplx && s.rx == 2 && s.ry == 4 && g == 1) return launch_blk_u<T, 1, 2, 4, false, 8, 128>(a, st);
+    }
+  } else if (s.ty == 16 && cb == 64 && s.rx == 1 && s.ry == 4 && g == 9) {
+    if constexpr (sizeof(T) == 8) {
+      if (!s.cplx) return launch_blk_u<T, 9, 1, 4, false, 16, 64>(a, st);
+    } else {
+      if (s.cplx) return launch_blk_u<T, 9, 1, 4, true, 16, 64>(a, st);
+    }
   }
   set_error("launch_pass_blk: no kernel for this cell block");
   return HPSI_ERR_UNSUPPORTED;
@@ -639,9 +663,9 @@ hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int cplx, int gro
 
 template int blk_chunk_states<double>();
 template int blk_chunk_states<float>();
-template bool blk_pass_eligible<double>(const PassArgs &, long long);
-template bool blk_pass_eligible<float>(const PassArgs &, long long);
-template hpsi_status launch_pass_blk<double>(const PassArgs &, int, int, int, int, cudaStream_t);
-template hpsi_status launch_pass_blk<float>(const PassArgs &, int, int, int, int, cudaStream_t);
+template bool blk_pass_eligible<double>(const PassArgs &, long long, int);
+template bool blk_pass_eligible<float>(const PassArgs &, long long, int);
+template hpsi_status launch_pass_blk<double>(const PassArgs &, const PassShape &, cudaStream_t);
+template hpsi_status launch_pass_blk<float>(const PassArgs &, const PassShape &, cudaStream_t);
 
 }  // namespace hpsi

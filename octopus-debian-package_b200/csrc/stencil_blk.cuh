@@ -5,30 +5,28 @@
 
 namespace hpsi {
 
-// Cell tile of one CTA: 16 x 8 (work items over 16 x 8 tiles).
+// Cell tiles of one CTA: 16 x 8 (128-byte chunks) or 16 x 16 (64-byte chunks).
 constexpr int BLK_TILE_X = 16;
-constexpr int BLK_TILE_Y = 8;
 
-// Complex states per chunk of the blocked pass (FP64 8, FP32 16).
+// Complex states per 128-byte chunk of the blocked pass (FP64 8, FP32 16).
 template <typename T>
 int blk_chunk_states();
 
-// The blocked pass serves a call when its chunk divides ld and the batches
-// are 16-byte aligned.
+// The blocked pass serves a call when its chunk (sc complex states) divides
+// ld and the batches are 16-byte aligned.
 template <typename T>
-bool blk_pass_eligible(const PassArgs &a, long long ld);
+bool blk_pass_eligible(const PassArgs &a, long long ld, int sc);
 
-// a.chunks = ld / blk_chunk_states<T>(); a.items over 16 x 8 tiles;
-// observables, when requested, are written per item.  rx x ry: cells per
-// thread; cplx: a thread owns a complex state (else one real lane); group:
-// planes per unrolled group of the z march (1 or 3).
+// a.chunks = ld / shape.sc; a.items over 16 x shape.ty tiles; observables,
+// when requested, are written per item.  The shape names the cell block
+// (rx x ry), the element (cplx: a complex state per thread, else one real
+// lane) and the planes per unrolled group (unroll).
 template <typename T>
-hpsi_status launch_pass_blk(const PassArgs &a, int rx, int ry, int cplx, int group, cudaStream_t st);
+hpsi_status launch_pass_blk(const PassArgs &a, const PassShape &shape, cudaStream_t st);
 
 // Grouped systems in one persistent launch (Horner passes): every system's
 // arguments built with the blocked shape (items over 16 x 8 tiles).
 template <typename T>
-hpsi_status launch_pass_blk_group(const GroupArgs &g, int rx, int ry, int cplx, int group, int num_sms,
-                                  cudaStream_t st);
+hpsi_status launch_pass_blk_group(const GroupArgs &g, const PassShape &shape, int num_sms, cudaStream_t st);
 
 }  // namespace hpsi
