@@ -255,25 +255,43 @@ __global__ void __launch_bounds__(256) trsm_apply_kernel(T *psi, long long ld, i
   }
 }
 
-// observables: partial [ncta][ld][3][2] -> out[3][nst] (energy, norm2, dipole) * dv
-__global__ void obs_finalize_kernel(const double *partial, int ncta, int ld, int nst, double dv,
-                                    const double *ket_partial, int nket, double *out) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nst) return;
-  for (int q = 0; q < 3; ++q) {
-    Kahan a = {0, 0};
-    for (int c = 0; c < ncta; ++c) {
-      const double *p = partial + ((long long)c * ld + s) * 6 + 2 * q;
-      kadd(a, p[0]);
-      a.c += p[1];
+// observables: partial [ncta][ld][3][2] -> out[3][nst] (energy, norm2, dipole) * dv.
+// One CTA per state: its threads take strided slices of the CTA partials
+// (compensated sums), then fold them in shared memory.
+__global__ void __launch_bounds__(128) obs_finalize_kernel(const double *partial, int ncta, int ld, int nst,
+                                                           double dv, const double *ket_partial, int nket,
+                                                           double *out) {
+  const int s = blockIdx.x;
+  __shared__ double red[3][2][128];
+  Kahan a[3] = {{0, 0}, {0, 0}, {0, 0}};
+  for (int c = threadIdx.x; c < ncta; c += blockDim.x) {
+    const double *p = partial + ((long long)c * ld + s) * 6;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      kadd(a[q], p[2 * q]);
+      a[q].c += p[2 * q + 1];
     }
-    if (q == 0 && ket_partial)
-      for (int c = 0; c < nket; ++c) {
-        const double *p = ket_partial + ((long long)c * ld + s) * 2;
-        kadd(a, p[0]);
-        a.c += p[1];
-      }
-    out[q * nst + s] = (a.s + a.c) * dv;
+  }
+  if (ket_partial)
+    for (int c = threadIdx.x; c < nket; c += blockDim.x) {
+      const double *p = ket_partial + ((long long)c * ld + s) * 2;
+      kadd(a[0], p[0]);
+      a[0].c += p[1];
+    }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    red[q][0][threadIdx.x] = a[q].s;
+    red[q][1][threadIdx.x] = a[q].c;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int q = threadIdx.x;
+    Kahan t = {0, 0};
+    for (int i = 0; i < int(blockDim.x); ++i) {
+      kadd(t, red[q][0][i]);
+      t.c += red[q][1][i];
+    }
+    out[q * nst + s] = (t.s + t.c) * dv;
   }
 }
 
@@ -339,7 +357,8 @@ hpsi_status launch_trsm_apply(T *psi, long long ld, int np, int nst, const doubl
 
 hpsi_status launch_obs_finalize(const double *partial, int ncta, int ld, int nst, double dv,
                                 const double *ket_partial, int nket, double *out, cudaStream_t st) {
-  obs_finalize_kernel<<<(nst + 127) / 128, 128, 0, st>>>(partial, ncta, ld, nst, dv, ket_partial, nket, out);
+  if (nst < 1) return HPSI_OK;
+  obs_finalize_kernel<<<nst, 128, 0, st>>>(partial, ncta, ld, nst, dv, ket_partial, nket, out);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
 }

@@ -102,7 +102,7 @@ struct BlkLayout {
   static constexpr int HROUNDS = (HC * PCS + NT - 1) / NT, IROUNDS = (IC * PCS + NT - 1) / NT;
   static constexpr bool HPART = (HC * PCS) % NT != 0, IPART = (IC * PCS) % NT != 0;
   static constexpr int NBUF = X0 ? 3 : 4;   // data stages
-  static constexpr int NSIDE = 2 * NBUF - 1;  // side slots (issued 2 NBUF - 2 planes ahead)
+  static constexpr int NSIDE = 8;  // side slots: >= 2 NBUF - 1 (issued 2 NBUF - 2 planes ahead), power of 2
   static constexpr int SIDE_AHEAD = 2 * NBUF - 2;
   // data stage: halo plane, psi0 rows of the output plane, potential
   static constexpr size_t o_psi0 = size_t(HC) * CELLB;
@@ -117,6 +117,7 @@ struct BlkLayout {
   static_assert(STAGE % 16 == 0 && SIDEB % 16 == 0, "16-byte copies");
   static constexpr int NMAPP = HC / 4, NROWP = IC / 4, NVP = IC / 2;  // 16-byte side/v pieces
   static_assert(NMAPP + NROWP <= NT && NVP <= NT, "one side piece per thread");
+  static_assert(NSIDE >= 2 * NBUF - 1, "side slot lifetime");
 };
 
 template <typename T>
@@ -304,6 +305,12 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   const long long out_lde = 2 * p.out_ld / LY::LW;  // elements per output row
   const int ocol = col / LY::LW + l;
   Kahan ke = {0, 0}, kn = {0, 0}, kd = {0, 0};
+  double n2c[RX][RY];  // observables: per-cell sums of |psi|^2 over the z march
+#pragma unroll
+  for (int cx = 0; cx < RX; ++cx)
+#pragma unroll
+    for (int r = 0; r < RY; ++r) n2c[cx][r] = 0.0;
+  (void)n2c;
   (void)lane;
 
   // z range of the inner points under this thread's cells: planes more than
@@ -398,10 +405,25 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
     if (zo >= zs) {
       const int *rows = reinterpret_cast<const int *>(side(k) + LY::s_rows);
       const E *x0s = reinterpret_cast<const E *>(st + LY::o_psi0) + l;
-      double pe = 0.0, pn = 0.0, pd = 0.0;
+      // output rows of the owned cells (pairs of x-adjacent cells in one load)
+      int rowv[RX][RY];
+#pragma unroll
+      for (int r = 0; r < RY; ++r) {
+        if constexpr (RX % 2 == 0) {
+#pragma unroll
+          for (int cx = 0; cx < RX; cx += 2) {
+            const int2 rr = *reinterpret_cast<const int2 *>(rows + (by + r) * TX + bx + cx);
+            rowv[cx][r] = rr.x;
+            rowv[cx + 1][r] = rr.y;
+          }
+        } else {
+#pragma unroll
+          for (int cx = 0; cx < RX; ++cx) rowv[cx][r] = rows[(by + r) * TX + bx + cx];
+        }
+      }
+      double pe = 0.0, pn = 0.0;
       (void)pe;
       (void)pn;
-      (void)pd;
 #pragma unroll
       for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
@@ -420,13 +442,10 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
               val = odd ? x0 + are * h + aim * hp : x0 + are * h - aim * hp;
             }
           }
-          const int row = rows[cell];
+          const int row = rowv[cx][r];
           if (row < 0 || row >= p.np) continue;
           if constexpr (OBS) {
             const E x0 = x0s[cell * SLE];
-            const double rr = p.obs_pol[0] * B.h[0] * double(cx0 + bx + cx + B.lo[0]) +
-                              p.obs_pol[1] * B.h[1] * double(cy0 + by + r + B.lo[1]) +
-                              p.obs_pol[2] * B.h[2] * double(zo + B.lo[2]);
             double eh, n2;
             if constexpr (CPLX) {
               eh = double(x0.x) * double(h.x) + double(x0.y) * double(h.y);
@@ -437,16 +456,16 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
             }
             pe += eh;
             pn += n2;
-            pd += n2 * rr;
+            n2c[cx][r] += n2;
           }
           out[row * out_lde + ocol] = val;
         }
       if constexpr (OBS) {
-        // one compensated add per plane and quantity (the few cells of a
-        // plane are summed plainly first)
+        // energy: one compensated add per plane (the plane's few cells summed
+        // plainly first); norm: per-cell sums of positive terms, folded at
+        // the end; dipole: z part per plane, x/y parts from the cell sums
         kadd(ke, pe);
-        kadd(kn, pn);
-        kadd(kd, pd);
+        kadd(kd, pn * (p.obs_pol[2] * B.h[2] * double(zo + B.lo[2])));
       }
     } else {
 #pragma unroll
@@ -490,6 +509,14 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   cp_async_wait<0>();
 
   if constexpr (OBS) {
+#pragma unroll
+    for (int cx = 0; cx < RX; ++cx)
+#pragma unroll
+      for (int r = 0; r < RY; ++r) {
+        kadd(kn, n2c[cx][r]);
+        kadd(kd, n2c[cx][r] * (p.obs_pol[0] * B.h[0] * double(cx0 + bx + cx + B.lo[0]) +
+                               p.obs_pol[1] * B.h[1] * double(cy0 + by + r + B.lo[1])));
+      }
     // per-state sums over the threads of this chunk; the two lanes of a state
     // fold into one entry
     __syncthreads();
