@@ -342,9 +342,9 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
     constexpr int S4 = (4 + K) % 9;  // running sum of output plane zbeg + k
     cp_async_wait<NBUF - 2>();
     __syncthreads();
-    issue_data(k + NBUF - 1);
-    issue_side(k + LY::SIDE_AHEAD);
-    cp_async_commit();
+    // the refill of the stage read in plane k - 1 is issued after this
+    // plane's arithmetic (every thread passed the barrier above, so the stage
+    // is free): the arithmetic starts right after the barrier
 
     const unsigned char *st = stage(k);
     const E *P = reinterpret_cast<const E *>(st) + l;
@@ -473,6 +473,9 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 #pragma unroll
         for (int r = 0; r < RY; ++r) acc[cx][r][K] = ezero<E>();
     }
+    issue_data(k + NBUF - 1);
+    issue_side(k + LY::SIDE_AHEAD);
+    cp_async_commit();
   };
 
   auto rotate = [&]() {
