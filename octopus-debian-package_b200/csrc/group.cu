@@ -71,6 +71,11 @@ struct hpsi_group {
   int *d_counter = nullptr;     // one counter per launch sub-group
   cudaStream_t cap = nullptr;
   cudaEvent_t ev = nullptr;
+  // side streams: the per-system KB bras and kets run concurrently (forked
+  // from and joined back to the step's stream; branches of the captured graph)
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
   int num_sms = 148;
 };
 
@@ -162,19 +167,37 @@ template <typename T>
 static hpsi_status group_step(hpsi_group *g, const std::vector<T *> &psi, const std::vector<long long> &ld,
                               const std::vector<int> &nst, double dt, int order, cudaStream_t st) {
   const int n = int(g->hams.size());
+  const int ns = int(g->side.size());
+  auto fork = [&]() -> hpsi_status {
+    HPSI_TRY_CUDA(cudaEventRecord(g->fork, st));
+    for (int i = 0; i < ns; ++i) HPSI_TRY_CUDA(cudaStreamWaitEvent(g->side[i], g->fork, 0));
+    return HPSI_OK;
+  };
+  auto join = [&]() -> hpsi_status {
+    for (int i = 0; i < ns; ++i) {
+      HPSI_TRY_CUDA(cudaEventRecord(g->join[i], g->side[i]));
+      HPSI_TRY_CUDA(cudaStreamWaitEvent(st, g->join[i], 0));
+    }
+    return HPSI_OK;
+  };
+  auto sst = [&](int s) { return ns ? g->side[s % ns] : st; };
   std::vector<const T *> in(psi.begin(), psi.end());
   for (int k = order; k >= 1; --k) {
     const double are = 0.0 / k, aim = -dt / k;  // a_k = -i dt / k (real dt)
     std::vector<T *> out(n);
+    hpsi_status r0 = fork();
+    if (r0) return r0;
     for (int s = 0; s < n; ++s) {
       hpsi_hamiltonian *h = g->hams[s];
       T *u0 = static_cast<T *>(h->u[0].ptr), *u1 = static_cast<T *>(h->u[1].ptr);
       out[s] = (k == 1 && order > 1) ? psi[s] : ((order - k) % 2 == 0 ? u0 : u1);
       if (h->nmat > 0) {
-        hpsi_status r = run_bra<T>(h, in[s], ld[s], static_cast<T *>(h->projbuf.ptr), st);
+        hpsi_status r = run_bra<T>(h, in[s], ld[s], static_cast<T *>(h->projbuf.ptr), sst(s));
         if (r) return r;
       }
     }
+    r0 = join();
+    if (r0) return r0;
     for (size_t li = 0; li < g->launches.size(); ++li) {
       const auto &L = g->launches[li];
       GroupArgs ga;
@@ -195,14 +218,18 @@ static hpsi_status group_step(hpsi_group *g, const std::vector<T *> &psi, const 
                              : launch_pass_group<T>(ga, g->sc, g->num_sms, st);
       if (r) return r;
     }
+    r0 = fork();
+    if (r0) return r0;
     for (int s = 0; s < n; ++s) {
       hpsi_hamiltonian *h = g->hams[s];
       if (h->nmat > 0) {
         hpsi_status r = run_ket<T>(h, static_cast<const T *>(h->projbuf.ptr), ld[s], int(ld[s]), out[s], ld[s],
-                                   PASS_HORNER, are, aim, psi[s], ld[s], nullptr, st);
+                                   PASS_HORNER, are, aim, psi[s], ld[s], nullptr, sst(s));
         if (r) return r;
       }
     }
+    r0 = join();
+    if (r0) return r0;
     for (int s = 0; s < n; ++s) in[s] = out[s];
   }
   if (order == 1)
@@ -229,6 +256,16 @@ static hpsi_status group_run(hpsi_group *g, hpsi_batch *b, int nsteps, double dt
   }
   hpsi_status r = group_build(g, b[0].dtype, ld);
   if (r) return r;
+  if (!g->fork) {
+    constexpr int NSIDE = 8;
+    HPSI_TRY_CUDA(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
+    g->side.resize(NSIDE);
+    g->join.resize(NSIDE);
+    for (int i = 0; i < NSIDE; ++i) {
+      HPSI_TRY_CUDA(cudaStreamCreateWithFlags(&g->side[i], cudaStreamNonBlocking));
+      HPSI_TRY_CUDA(cudaEventCreateWithFlags(&g->join[i], cudaEventDisableTiming));
+    }
+  }
   for (int s = 0; s < n; ++s) {
     r = prepare_taylor_workspaces(g->hams[s], ld[s], sizeof(T), false);
     if (r) return r;
@@ -399,6 +436,9 @@ hpsi_status hpsi_group_destroy(hpsi_group *g) {
   dev_free(g->d_counter);
   if (g->cap) cudaStreamDestroy(g->cap);
   if (g->ev) cudaEventDestroy(g->ev);
+  for (auto s : g->side) cudaStreamDestroy(s);
+  for (auto e : g->join) cudaEventDestroy(e);
+  if (g->fork) cudaEventDestroy(g->fork);
   delete g;
   return HPSI_OK;
 }
