@@ -66,3 +66,41 @@ def test_autotune_keeps_results(cuda):
     x32 = x.to(torch.complex64)
     shape32, _ = ham.autotune(lib.HPSI_C64, 8)
     assert shape32["sc"] in (2, 4, 8)
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_group_blocked_pass_matches_single_systems(cuda, dtype):
+    """Every width a multiple of the blocked pass's chunk (8 complex128 / 16
+    complex64 states): the grouped launch runs the blocked pass kernel."""
+    import torch
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    chunk = 8 if dtype == "c128" else 16
+    specs = [(11, 13, 5, 2), (12, 18, chunk + 3, 0), (13, 10, 2 * chunk, 3), (14, 22, 3, 1)]
+    hams, xs, refs, nsts = [], [], [], []
+    for seed, n, nst, natoms in specs:
+        m, v, proj, psi = _system(seed, n, nst, natoms)
+        dm = lib.DeviceMesh(m)
+        ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=v, projectors=proj)
+        ld = chunk * ((nst + chunk - 1) // chunk)
+        x = torch.zeros((m.np_part, ld), dtype=tdt, device=cuda)
+        x[:, :nst] = torch.from_numpy(psi).to(tdt)
+        r = x.clone()
+        for _ in range(3):
+            ham.taylor_step(r, 0.02)
+        hams.append((dm, ham))
+        xs.append(x)
+        refs.append(r)
+        nsts.append(nst)
+    g = lib.Group([h for _, h in hams])
+    tol = 1e-13 if dtype == "c128" else 1e-6
+    for graph in (False, True):
+        ys = [x.clone() for x in xs]
+        g.taylor_steps(ys, 3, 0.02, graph=graph)
+        torch.cuda.synchronize()
+        for y, r, nst in zip(ys, refs, nsts):
+            a = y.cpu().numpy()[:, :nst].astype(np.complex128)
+            b = r.cpu().numpy()[:, :nst].astype(np.complex128)
+            assert rel_maxnorm_per_state(a, b) <= tol
+    g.close()

@@ -199,3 +199,28 @@ def test_odd_fp32_width_rejected(cuda):
     y = torch.zeros((m.np, 5), dtype=x.dtype, device=cuda)
     with pytest.raises(lib.HpsiError, match="16-byte"):
         ham.apply(x, y)
+
+
+@pytest.mark.parametrize("path", ["default", "blk_real", "blk_cplx", "blk_64b"])
+@pytest.mark.parametrize("dtype,ld", [(np.complex128, 8), (np.complex64, 16)])
+def test_blk_bloch_phase(cuda, monkeypatch, path, dtype, ld):
+    """Bloch-phase periodic images (phase multiplied on load) in the blocked pass."""
+    import torch
+    from hpsi import fixtures
+    from hpsi.mesh import index_box_mesh
+    _set_path(monkeypatch, path)
+    rng = np.random.default_rng(67)
+    m = index_box_mesh((12, 10, 8), 0.3, periodic=True)
+    v = fixtures.soft_coulomb(m, rng)
+    psi = fixtures.random_states(m, ld, rng, orthonormal=False)
+    k = np.array([0.3, -0.2, 0.5])
+    pc = np.exp(1j * ((m.x[m.np:] - m.x[m.per_inner]) @ k))
+    dm, ham, w, pts = _setup(m, v=v)
+    ham.set_phase_corr(pc)
+    from oracle import oracle as O
+    ref = O.Hamiltonian(m, w, pts, v=v, bc="periodic", phase_corr=pc).apply(psi)
+    x = _dev(psi, cuda, ld, dtype)
+    y = torch.zeros((m.np, ld), dtype=x.dtype, device=cuda)
+    ham.apply(x, y)
+    tol = TOL64 if dtype == np.complex128 else TOL32
+    assert rel_maxnorm_per_state(y.cpu().numpy().astype(np.complex128), ref) <= tol
