@@ -212,16 +212,17 @@ PassShape blk_shape(int dtype) {
 
 PassShape default_shape(int dtype, long long ld) {
   PassShape s = ld % blk_shape(dtype).sc == 0 ? blk_shape(dtype) : legacy_shape(dtype, ld);
-  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx,cplx"
+  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx,cplx,ty"
   const char *env = std::getenv(dtype == HPSI_C128 ? "HPSI_PASS_SHAPE64" : "HPSI_PASS_SHAPE32");
   if (env) {
-    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0, cx = -1;
-    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx) >= 2 && a > 0 && ld % a == 0) {
+    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0, cx = -1, ty = 0;
+    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx, &ty) >= 2 && a > 0 &&
+        ld % a == 0) {
       if (t) {
         s = blk_shape(dtype);  // chunk (128 or 64 bytes), block, element, z depth and group are taken
         if (a == s.sc / 2) {
-          s.sc = a;  // 64-byte chunks ride 16 x 16 tiles
-          s.ty = 16;
+          s.sc = a;  // 64-byte chunks ride 16 x 16 tiles unless ty = 8 is given
+          s.ty = ty == 8 ? 8 : 16;
         }
         if (u == 1 || u == 3 || u == 9) s.unroll = u;
         if (x > 0) s.rx = x;

@@ -356,6 +356,9 @@ static hpsi_status autotune_t(hpsi_hamiltonian *h, int dtype, long long ld, cuda
       b3.cplx = dtype == HPSI_C128 ? 0 : 1;
       b3.unroll = 9;
       blocks.push_back(b3);
+      PassShape b4 = b3;  // 64-byte chunks, 16 x 8 tiles, 256 threads, two CTAs per SM
+      b4.ty = 8;
+      blocks.push_back(b4);
     }
     for (const auto &b : blocks)
       for (int zb : {0, 16, 32, 48, 64, 1 << 20}) {

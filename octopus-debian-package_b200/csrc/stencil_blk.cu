@@ -101,8 +101,12 @@ struct BlkLayout {
   // may be partial)
   static constexpr int HROUNDS = (HC * PCS + NT - 1) / NT, IROUNDS = (IC * PCS + NT - 1) / NT;
   static constexpr bool HPART = (HC * PCS) % NT != 0, IPART = (IC * PCS) % NT != 0;
-  static constexpr int NBUF = X0 ? 3 : 4;   // data stages
-  static constexpr int NSIDE = 8;  // side slots: >= 2 NBUF - 1 (issued 2 NBUF - 2 planes ahead), power of 2
+  // two CTAs per SM for 256-thread blocks (shared memory <= 113 KB each)
+  static constexpr int CTAS = (NT == 256 && CB_ == 64) ? 2 : 1;
+  static constexpr int NBUF = (X0 || CTAS == 2) ? 3 : 4;  // data stages
+  // side slots: >= 2 NBUF - 1 (issued 2 NBUF - 2 planes ahead); a power of 2
+  // unless shared memory is short
+  static constexpr int NSIDE = CTAS == 2 ? 2 * NBUF - 1 : 8;
   static constexpr int SIDE_AHEAD = 2 * NBUF - 2;
   // data stage: halo plane, psi0 rows of the output plane, potential
   static constexpr size_t o_psi0 = size_t(HC) * CELLB;
@@ -113,7 +117,7 @@ struct BlkLayout {
   static constexpr size_t SIDEB = s_rows + size_t(IC) * sizeof(int);
   static constexpr size_t o_side = NBUF * STAGE;
   static constexpr size_t bytes = o_side + NSIDE * SIDEB;
-  static_assert(bytes <= 232448, "shared memory per CTA");
+  static_assert(bytes * CTAS <= 232448 - 2048, "shared memory per CTA");
   static_assert(STAGE % 16 == 0 && SIDEB % 16 == 0, "16-byte copies");
   static constexpr int NMAPP = HC / 4, NROWP = IC / 4, NVP = IC / 2;  // 16-byte side/v pieces
   static_assert(NMAPP + NROWP <= NT && NVP <= NT, "one side piece per thread");
@@ -555,7 +559,8 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 }
 
 template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX, int TY, int CB>
-__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::NT, 1)
+__global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::NT,
+                                  BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::CTAS)
     pass_blk_kernel(const __grid_constant__ PassArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
   blk_body<T, HORNER, OBS, U, RX, RY, CPLX, TY, CB>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem);
@@ -564,7 +569,8 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, 
 // Many systems in one persistent launch (Horner passes): each CTA takes
 // (system, item, chunk) units from a list sorted by cost until it is empty.
 template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
-__global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT, 1)
+__global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT,
+                                  BlkLayout<T, true, RX, RY, CPLX, TY, CB>::CTAS)
     pass_blk_group_kernel(const __grid_constant__ GroupArgs g) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int unit_s;
@@ -588,6 +594,8 @@ hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
     attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LY::bytes));
+    if (attr == cudaSuccess && LY::CTAS > 1)
+      attr = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   });
   HPSI_TRY_CUDA(attr);
   const unsigned nblocks = unsigned(a.nitems) * unsigned(a.chunks);
@@ -665,7 +673,9 @@ bool blk_pass_eligible(const PassArgs &a, long long ld, int sc) {
 //     or complex states (9); FP32 2 x 2 complex states with packed
 //     multiply-adds (9 or 3) or 2 x 4 real lanes (1);
 //   64-byte chunks, 16 x 16 tiles (halo 2.25x instead of 3x): 1 x 4 cells,
-//     FP64 real lanes, FP32 complex states (groups of 9).
+//     FP64 real lanes, FP32 complex states (groups of 9);
+//   64-byte chunks, 16 x 8 tiles, 1 x 4 cells, 256 threads and two CTAs per
+//     SM (faster on small meshes: twice the CTAs per state chunk).
 template <typename T>
 hpsi_status launch_pass_blk(const PassArgs &a, const PassShape &s, cudaStream_t st) {
   if (a.nitems == 0) return HPSI_OK;
@@ -679,6 +689,13 @@ hpsi_status launch_pass_blk(const PassArgs &a, const PassShape &s, cudaStream_t 
       if (s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, true, 8, 128>(a, st);
       if (s.cplx && s.rx == 2 && s.ry == 2 && g == 3) return launch_blk_u<T, 3, 2, 2, true, 8, 128>(a, st);
       if (!s.cplx && s.rx == 2 && s.ry == 4 && g == 1) return launch_blk_u<T, 1, 2, 4, false, 8, 128>(a, st);
+    }
+  } else if (s.ty == 8 && cb == 64 && s.rx == 1 && s.ry == 4 && g == 9) {
+    // 256-thread blocks, two CTAs per SM
+    if constexpr (sizeof(T) == 8) {
+      if (!s.cplx) return launch_blk_u<T, 9, 1, 4, false, 8, 64>(a, st);
+    } else {
+      if (s.cplx) return launch_blk_u<T, 9, 1, 4, true, 8, 64>(a, st);
     }
   } else if (s.ty == 16 && cb == 64 && s.rx == 1 && s.ry == 4 && g == 9) {
     if constexpr (sizeof(T) == 8) {

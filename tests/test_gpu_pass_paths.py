@@ -23,7 +23,9 @@ BLK_REAL = {"HPSI_PASS_SHAPE64": "8,2,{zb},3,1,2,0", "HPSI_PASS_SHAPE32": "16,4,
 BLK_CPLX = {"HPSI_PASS_SHAPE64": "8,2,{zb},9,1,2,1", "HPSI_PASS_SHAPE32": "16,2,{zb},3,1,2,1"}
 # 64-byte chunks on 16 x 16 tiles, 1 x 4 cells
 BLK_64B = {"HPSI_PASS_SHAPE64": "4,4,{zb},9,1,1,0", "HPSI_PASS_SHAPE32": "8,4,{zb},9,1,1,1"}
-PATHS = ["default", "blk_real", "blk_cplx", "blk_64b", "legacy"]
+# 64-byte chunks on 16 x 8 tiles, 1 x 4 cells, 256 threads (two CTAs per SM)
+BLK_2CTA = {"HPSI_PASS_SHAPE64": "4,4,{zb},9,1,1,0,8", "HPSI_PASS_SHAPE32": "8,4,{zb},9,1,1,1,8"}
+PATHS = ["default", "blk_real", "blk_cplx", "blk_64b", "blk_2cta", "legacy"]
 
 
 def _setup(mesh, v=None, proj=None):
@@ -54,7 +56,8 @@ def _set_path(monkeypatch, path, zb=0):
         for k in LEGACY:
             monkeypatch.delenv(k, raising=False)
         return
-    env = {"legacy": LEGACY, "blk_real": BLK_REAL, "blk_cplx": BLK_CPLX, "blk_64b": BLK_64B}[path]
+    env = {"legacy": LEGACY, "blk_real": BLK_REAL, "blk_cplx": BLK_CPLX, "blk_64b": BLK_64B,
+           "blk_2cta": BLK_2CTA}[path]
     for k, v in env.items():
         monkeypatch.setenv(k, v.format(zb=zb))
 
@@ -86,7 +89,7 @@ def test_apply_and_taylor(cuda, monkeypatch, path, dtype, ld, nst):
     assert np.max(np.abs(n - n_ref) / n_ref) <= (1e-12 if dtype == np.complex128 else 1e-6)
 
 
-@pytest.mark.parametrize("path", ["blk_real", "blk_cplx", "blk_64b"])
+@pytest.mark.parametrize("path", ["blk_real", "blk_cplx", "blk_64b", "blk_2cta"])
 @pytest.mark.parametrize("zb", [0, 5, 9])
 def test_blk_zblocks_and_tiles(cuda, monkeypatch, zb, path):
     """A box several tiles wide in x and y, cut into z blocks of several depths
@@ -107,7 +110,7 @@ def test_blk_zblocks_and_tiles(cuda, monkeypatch, zb, path):
     assert rel_maxnorm_per_state(y.cpu().numpy(), ref) <= TOL64
 
 
-@pytest.mark.parametrize("path", ["blk_real", "blk_cplx", "blk_64b"])
+@pytest.mark.parametrize("path", ["blk_real", "blk_cplx", "blk_64b", "blk_2cta"])
 def test_blk_periodic_and_raw_boundary(cuda, monkeypatch, path):
     """Periodic images without Bloch phase (map to inner rows) and set_bc=False
     (boundary rows read as stored: the input tensor spans np_part rows)."""
@@ -201,7 +204,7 @@ def test_odd_fp32_width_rejected(cuda):
         ham.apply(x, y)
 
 
-@pytest.mark.parametrize("path", ["default", "blk_real", "blk_cplx", "blk_64b"])
+@pytest.mark.parametrize("path", ["default", "blk_real", "blk_cplx", "blk_64b", "blk_2cta"])
 @pytest.mark.parametrize("dtype,ld", [(np.complex128, 8), (np.complex64, 16)])
 def test_blk_bloch_phase(cuda, monkeypatch, path, dtype, ld):
     """Bloch-phase periodic images (phase multiplied on load) in the blocked pass."""
