@@ -266,6 +266,9 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
 }
 }  // namespace
 
+// At most 1024 CTA rows, each over a contiguous range of covered rows: one
+// row per thread (up to 65535 CTA rows) measured 45 % slower on the R = 12
+// sphere, the projections of neighbouring rows no longer sharing L1.
 int ket_row_blocks(int nk) { return std::max(1, std::min(1024, (nk + 7) / 8)); }
 
 template <typename T>
