@@ -232,7 +232,6 @@ PassShape default_shape(int dtype, long long ld) {
         s = legacy_shape(dtype, ld);
         s.sc = a;
         s.ry = b;
-        s.unroll = u;
       }
       s.zb = c;
     }

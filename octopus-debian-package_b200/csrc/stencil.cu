@@ -356,7 +356,7 @@ __device__ __forceinline__ void pass_body(const PassArgs &p, const int item, con
     const int zo = pz - HAL;
     if (zo >= zs) {
       const int *ro = rowring + ((K + 5) % RING) * TY * TX;
-      const C2 *x0s = psi0ring + DB * INNER;
+      [[maybe_unused]] const C2 *x0s = psi0ring + DB * INNER;
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
         const int ty = tyg * RY + r;
@@ -470,7 +470,7 @@ hpsi_status launch_mode(const PassArgs &a, cudaStream_t st) {
   return HPSI_OK;
 }
 
-template <typename T, int SC, int TX, int TY, int RY, bool UNR = false>
+template <typename T, int SC, int TX, int TY, int RY>
 hpsi_status launch_variant(const PassArgs &a, cudaStream_t st) {
   const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr;
   if (horner && obs) return launch_mode<T, SC, TX, TY, RY, true, true>(a, st);

@@ -54,7 +54,7 @@ struct PassShape {
   int sc;   // complex states per CTA
   int tx, ty, ry;
   int zb = 0;  // output planes per work item (0: chosen from the wave count)
-  int unroll = 0;  // 1: nine-plane unrolled ring, 0: switch-selected ring
+  int unroll = 0;  // blocked pass: planes per unrolled group of the z march (1, 3 or 9)
   int blk = 0;     // 1: register-blocked real-lane pass (sc = its chunk, tiles 16 x 8)
   int rx = 0;      // blocked pass: cells per thread along x (ry along y)
   int cplx = 0;    // blocked pass: 1 = a thread owns a complex state, 0 = one real lane

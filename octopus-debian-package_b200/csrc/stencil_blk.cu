@@ -408,7 +408,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
     const int zo = pz - HAL;
     if (zo >= zs) {
       const int *rows = reinterpret_cast<const int *>(side(k) + LY::s_rows);
-      const E *x0s = reinterpret_cast<const E *>(st + LY::o_psi0) + l;
+      [[maybe_unused]] const E *x0s = reinterpret_cast<const E *>(st + LY::o_psi0) + l;
       // output rows of the owned cells (pairs of x-adjacent cells in one load)
       int rowv[RX][RY];
 #pragma unroll
@@ -432,7 +432,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
       for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
-          const int cell = (by + r) * TX + bx + cx;
+          [[maybe_unused]] const int cell = (by + r) * TX + bx + cx;
           const E h = acc[cx][r][K];
           acc[cx][r][K] = ezero<E>();
           E val = h;
