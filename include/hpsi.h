@@ -261,6 +261,16 @@ hpsi_status hpsi_dotp_matrix(hpsi_mesh *mesh, const hpsi_batch *a,
 hpsi_status hpsi_orthonormalize_cholesky(hpsi_mesh *mesh, hpsi_batch *psi,
                                          void *stream);
 
+/* Density accumulation of a propagated batch: replaces density_calc_accumulate
+ * for unpolarised / spin-polarised packed batches
+ * (src/states/density.F90:279-362):
+ *   rho[ip] = (accumulate ? rho[ip] : 0) + sum_i weight[i] |psi_i(ip)|^2
+ * over the np inner points.  weight: nst host doubles (kweight x occupation);
+ * psi and rho (np doubles) on the device; FP64 sums in a fixed order. */
+hpsi_status hpsi_density_accumulate(hpsi_mesh *mesh, const hpsi_batch *psi,
+                                    const double *weight, double *rho,
+                                    int32_t accumulate, void *stream);
+
 /* Allocation-free variant of hpsi_nrm2 (no counterpart in the reference).
  * For callers that must not make the library allocate device memory at this
  * point (an application that owns the whole device-memory budget or pool, or

@@ -1322,6 +1322,27 @@ hpsi_status hpsi_taylor_step(hpsi_hamiltonian *h, hpsi_batch *psi, double dt_re,
 }
 
 // ---------------------------------------------------------------------------
+hpsi_status hpsi_density_accumulate(hpsi_mesh *m, const hpsi_batch *psi, const double *weight, double *rho,
+                                    int32_t accumulate, void *stream) {
+  if (!m || !weight || !rho) return HPSI_ERR_ARG;
+  hpsi_status s = check_batch(m, psi, m->np, "hpsi_density_accumulate");
+  if (s) return s;
+  if (!is_device_ptr(psi->ptr) || !is_device_ptr(rho)) {
+    set_error("hpsi_density_accumulate: device batch and density expected");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  s = m->scratch2.ensure(size_t(psi->nst) * sizeof(double));
+  if (s) return s;
+  double *w = static_cast<double *>(m->scratch2.ptr);
+  HPSI_TRY_CUDA(cudaMemcpyAsync(w, weight, size_t(psi->nst) * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (psi->dtype == HPSI_C128)
+    return launch_density<double>(static_cast<const double *>(psi->ptr), psi->ld, m->np, psi->nst, w, rho,
+                                  accumulate != 0, st);
+  return launch_density<float>(static_cast<const float *>(psi->ptr), psi->ld, m->np, psi->nst, w, rho,
+                               accumulate != 0, st);
+}
+
 hpsi_status hpsi_nrm2(hpsi_mesh *m, const hpsi_batch *psi, double *out, void *stream) {
   if (!m || !out) return HPSI_ERR_ARG;
   hpsi_status s = check_batch(m, psi, m->np, "hpsi_nrm2");

@@ -8,6 +8,8 @@
 // X(mesh_batch_dotp_matrix) (src/grid/mesh_batch_inc.F90:20-263, 379-552,
 // 970-1167) and the cholesky_serial branch of
 // X(states_elec_orthogonalization_full) (src/states/states_elec_calc_inc.F90:66-98).
+#include <algorithm>
+
 #include "reduce.cuh"
 
 namespace hpsi {
@@ -295,7 +297,40 @@ __global__ void __launch_bounds__(128) obs_finalize_kernel(const double *partial
   }
 }
 
+// rho[ip] (+)= sum_s w[s] |psi_s(ip)|^2 over the np inner points: one warp per
+// row, lanes over the states, FP64 sums folded in a fixed order (deterministic).
+template <typename T>
+__global__ void __launch_bounds__(256) density_kernel(const T *psi, long long ld, int np, int nst, const double *w,
+                                                      double *rho, int accumulate) {
+  const int lane = threadIdx.x & 31;
+  for (long long row = blockIdx.x * 8LL + (threadIdx.x >> 5); row < np; row += gridDim.x * 8LL) {
+    const T *r = psi + row * 2 * ld;
+    double acc = 0.0;
+    for (int s = lane; s < nst; s += 32) {
+      const double re = double(r[2 * s]), im = double(r[2 * s + 1]);
+      acc += __ldg(w + s) * (re * re + im * im);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) rho[row] = accumulate ? rho[row] + acc : acc;
+  }
+}
+
 }  // namespace
+
+template <typename T>
+hpsi_status launch_density(const T *psi, long long ld, int np, int nst, const double *w, double *rho, int accumulate,
+                           cudaStream_t st) {
+  if (np < 1) return HPSI_OK;
+  const int grid = std::min((np + 7) / 8, 148 * 16);
+  density_kernel<T><<<grid, 256, 0, st>>>(psi, ld, np, nst, w, rho, accumulate);
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+template hpsi_status launch_density<double>(const double *, long long, int, int, const double *, double *, int,
+                                            cudaStream_t);
+template hpsi_status launch_density<float>(const float *, long long, int, int, const double *, double *, int,
+                                           cudaStream_t);
 
 int reduce_blocks(int np) {
   int nb = (np + 4095) / 4096;

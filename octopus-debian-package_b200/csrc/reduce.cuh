@@ -27,6 +27,11 @@ hpsi_status launch_trsm_apply(T *psi, long long ld, int np, int nst, const doubl
 
 // partial [ncta][ld][3][2] -> out[3][nst] = (energy, norm2, dipole) * dv;
 // ket_partial [nket][ld][2] (may be null) adds the KB part of the energy
+// rho[ip] (+)= sum_s w[s] |psi_s(ip)|^2 (w on the device, nst entries)
+template <typename T>
+hpsi_status launch_density(const T *psi, long long ld, int np, int nst, const double *w, double *rho, int accumulate,
+                           cudaStream_t st);
+
 hpsi_status launch_obs_finalize(const double *partial, int ncta, int ld, int nst, double dv,
                                 const double *ket_partial, int nket, double *out, cudaStream_t st);
 

@@ -87,6 +87,8 @@ SIGNATURES = {
                                           C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_nrm2": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_density_accumulate": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(C.c_double), C.c_void_p,
+                                            C.c_int32, C.c_void_p]),
     "hpsi_dotp_matrix": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(C.c_double),
                                      C.c_void_p]),
     "hpsi_orthonormalize_cholesky": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_void_p]),
@@ -215,6 +217,18 @@ class DeviceMesh:
         out = np.zeros(b.nst)
         check(load().hpsi_nrm2(self.handle, C.byref(b), _dp(out), _stream_ptr(stream)))
         return out
+
+    def density(self, psi, weight, rho=None, accumulate=False, nst=None, stream=None):
+        """rho (+)= sum_i weight[i] |psi_i|^2 on the inner points (density_calc_accumulate);
+        rho: a float64 device tensor of np entries (allocated when None)."""
+        import torch
+        b = as_batch(psi, nst=nst)
+        w = np.ascontiguousarray(np.asarray(weight, dtype=np.float64)[: b.nst])
+        if rho is None:
+            rho = torch.zeros(self.mesh.np, dtype=torch.float64, device=psi.device)
+        check(load().hpsi_density_accumulate(self.handle, C.byref(b), _dp(w), C.c_void_p(rho.data_ptr()),
+                                             1 if accumulate else 0, _stream_ptr(stream)))
+        return rho
 
     def dotp_matrix(self, a, b, nst=None, stream=None) -> np.ndarray:
         ba, bb = as_batch(a, nst=nst), as_batch(b, nst=nst)

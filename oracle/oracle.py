@@ -261,6 +261,16 @@ def mesh_batch_nrm2(mesh, psi):
     return np.sqrt(mesh.vol_pp * np.sum(np.abs(a) ** 2, axis=0))
 
 
+def density_accumulate(mesh, psi, weight, rho=None):
+    """rho + sum_i weight_i |psi_i|^2 on the inner points: the packed,
+    unpolarised branch of density_calc_accumulate
+    (src/states/density.F90:337-357, weights from :295-298)."""
+    a = np.asarray(psi)[: mesh.np]
+    w = np.asarray(weight, dtype=np.float64)
+    d = (np.abs(a) ** 2) @ w
+    return d if rho is None else np.asarray(rho) + d
+
+
 def mesh_batch_dotp_matrix(mesh, a, b):
     a = np.asarray(a)[: mesh.np]
     b = np.asarray(b)[: mesh.np]

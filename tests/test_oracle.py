@@ -160,3 +160,21 @@ def test_oracle_projector_matches_dense_formula():
         pr = sc[:, None] * (mat.T @ psi[mp])
         ref[mp] += mat @ pr
     assert np.max(np.abs(got - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+def test_density_restatement_matches_reference_loop():
+    """oracle.density_accumulate against an explicit point/state double loop in
+    the order of the reference's packed branch (density.F90:337-357)."""
+    import numpy as np
+    from hpsi.mesh import index_box_mesh
+    from oracle import oracle as O
+    m = index_box_mesh((5, 4, 3), 0.5)
+    rng = np.random.default_rng(5)
+    psi = rng.standard_normal((m.np_part, 3)) + 1j * rng.standard_normal((m.np_part, 3))
+    w = rng.uniform(0, 2, 3)
+    ref = np.zeros(m.np)
+    for ip in range(m.np):
+        for ist in range(3):
+            ref[ip] += w[ist] * (np.conj(psi[ip, ist]) * psi[ip, ist]).real
+    got = O.density_accumulate(m, psi, w)
+    assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(ref)
