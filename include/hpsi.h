@@ -196,6 +196,16 @@ hpsi_status hpsi_td_propagate(hpsi_hamiltonian *ham, hpsi_batch *psi, int32_t ns
                               double t0, int32_t use_graph, double *energy,
                               double *dipole, double *norm2, void *stream);
 
+/* The same driver with the enforced-time-reversal-symmetry propagator
+ * (td_etrs for independent particles, src/td/propagator_etrs.F90:70-152):
+ * each step is exp(-i dt/2 H(t_n+1)) exp(-i dt/2 H(t_n)) psi (two Taylor
+ * exponentials, 2 * order H.psi); the observables of step n are those of
+ * psi(t_n) under H(t_n). */
+hpsi_status hpsi_td_propagate_etrs(hpsi_hamiltonian *ham, hpsi_batch *psi, int32_t nsteps,
+                                   double dt, int32_t order, const hpsi_laser *laser,
+                                   double t0, int32_t use_graph, double *energy,
+                                   double *dipole, double *norm2, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Independent systems advanced together (no reference counterpart: the
  * reference loops over state blocks on the host,

@@ -10,6 +10,10 @@
 // H(t_n + dt/2) and the laser difference is removed exactly,
 // E(t_n) = E_mid - (eps(t_n + dt/2) - eps(t_n)) * <pol.r>, since H depends on the
 // field only through eps * pol.r.
+//
+// ETRS (td_etrs, src/td/propagator_etrs.F90:70-152, independent particles):
+// exp(-i dt/2 H(t_n+1)) exp(-i dt/2 H(t_n)); the observables are measured by
+// the first half step, with H(t_n) exactly.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -54,32 +58,45 @@ double laser_field(const hpsi_laser &L, double t) {
   return L.E0 * s * s * std::cos(L.omega * t);
 }
 
+// ETRS: the second half step of step *step runs with the field of t_n+1.
+__global__ void td_set_second_half(const double *amp_b, const int *step, double *cur_amp) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *cur_amp = amp_b[*step];
+}
+
 }  // namespace
 
+// propagator: 0 exponential midpoint, 1 ETRS
 template <typename T>
 hpsi_status td_run(hpsi_hamiltonian *h, T *psi, long long ld, int nst, int nsteps, double dt, int order,
                    const hpsi_laser *las, double t0, bool graph, double *e_out, double *d_out, double *n_out,
-                   cudaStream_t st) {
+                   cudaStream_t st, int propagator = 0) {
   // device layout of the driver buffer (doubles):
   // amp_mid[nsteps+1] amp_n[nsteps+1] cur_amp step(int) E[nsteps] D[nsteps] N[nsteps] obs_state[3*nst]
-  const size_t nd = 2 * size_t(nsteps + 1) + 2 + 3 * size_t(nsteps) + 3 * size_t(nst);
+  // amp_b[nsteps+1]
+  // (ETRS: amp_mid = amp_n = E(t_n), the first half step; amp_b = E(t_n+1))
+  const bool etrs = propagator == 1;
+  const size_t nd = 2 * size_t(nsteps + 1) + 2 + 3 * size_t(nsteps) + 3 * size_t(nst) + size_t(nsteps + 1);
   hpsi_status s = h->tdbuf.ensure(nd * sizeof(double));
   if (s) return s;
   double *base = static_cast<double *>(h->tdbuf.ptr);
   double *amp_mid = base, *amp_n = base + (nsteps + 1), *cur_amp = amp_n + (nsteps + 1);
   int *step = reinterpret_cast<int *>(cur_amp + 1);
   double *E = cur_amp + 2, *D = E + nsteps, *N = D + nsteps, *obs_state = N + nsteps;
-  std::vector<double> host(2 * size_t(nsteps + 1) + 2, 0.0);
+  double *amp_b = obs_state + 3 * size_t(nst);
+  std::vector<double> host(2 * size_t(nsteps + 1) + 2, 0.0), hostb(size_t(nsteps + 1), 0.0);
   const hpsi_laser none = {0.0, 0.0, 0.0, {0.0, 0.0, 1.0}};
   const hpsi_laser &L = las ? *las : none;
   for (int i = 0; i <= nsteps; ++i) {
-    host[i] = laser_field(L, t0 + (i + 0.5) * dt);
+    host[i] = laser_field(L, t0 + (etrs ? i : i + 0.5) * dt);
     host[nsteps + 1 + i] = laser_field(L, t0 + i * dt);
+    hostb[i] = laser_field(L, t0 + (i + 1) * dt);
   }
   host[2 * size_t(nsteps + 1)] = host[0];  // cur_amp
   int zero = 0;
   std::memcpy(&host[2 * size_t(nsteps + 1) + 1], &zero, sizeof(int));
   HPSI_TRY_CUDA(cudaMemcpyAsync(base, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (etrs)
+    HPSI_TRY_CUDA(cudaMemcpyAsync(amp_b, hostb.data(), hostb.size() * sizeof(double), cudaMemcpyHostToDevice, st));
 
   // the field enters the pass as pol * (*cur_amp)
   const double save_fld[3] = {h->fld[0], h->fld[1], h->fld[2]};
@@ -93,8 +110,14 @@ hpsi_status td_run(hpsi_hamiltonian *h, T *psi, long long ld, int nst, int nstep
   h->fld_scale_dev = cur_amp;
 
   auto one_step = [&]() -> hpsi_status {
-    hpsi_status r = taylor_dev<T>(h, psi, ld, nst, dt, 0.0, order, obs_state, st);
+    hpsi_status r = taylor_dev<T>(h, psi, ld, nst, etrs ? 0.5 * dt : dt, 0.0, order, obs_state, st);
     if (r) return r;
+    if (etrs) {
+      td_set_second_half<<<1, 32, 0, st>>>(amp_b, step, cur_amp);
+      HPSI_CHECK_LAUNCH();
+      r = taylor_dev<T>(h, psi, ld, nst, 0.5 * dt, 0.0, order, nullptr, st);
+      if (r) return r;
+    }
     td_step_finalize<<<1, 32, 0, st>>>(obs_state, nst, amp_mid, amp_n, cur_amp, step, E, D, N);
     HPSI_CHECK_LAUNCH();
     return HPSI_OK;
@@ -189,28 +212,43 @@ hpsi_status td_run(hpsi_hamiltonian *h, T *psi, long long ld, int nst, int nstep
 
 using namespace hpsi;
 
-extern "C" hpsi_status hpsi_td_propagate(hpsi_hamiltonian *h, hpsi_batch *psi, int32_t nsteps, double dt,
-                                         int32_t order, const hpsi_laser *laser, double t0, int32_t use_graph,
-                                         double *energy, double *dipole, double *norm2, void *stream) {
+static hpsi_status td_entry(const char *name, hpsi_hamiltonian *h, hpsi_batch *psi, int32_t nsteps, double dt,
+                            int32_t order, const hpsi_laser *laser, double t0, int32_t use_graph, double *energy,
+                            double *dipole, double *norm2, void *stream, int propagator) {
   if (!h || !psi || nsteps < 0 || !(dt > 0.0) || order < 1 || order > 32) {
-    set_error("hpsi_td_propagate: bad argument");
+    set_error(std::string(name) + ": bad argument");
     return HPSI_ERR_ARG;
   }
   if (!h->have_kinetic) {
-    set_error("hpsi_td_propagate: kinetic weights not set");
+    set_error(std::string(name) + ": kinetic weights not set");
     return HPSI_ERR_STATE;
   }
   if (!psi->ptr || psi->npts < h->mesh->np || psi->nst < 1 || psi->ld < psi->nst || !is_device_ptr(psi->ptr)) {
-    set_error("hpsi_td_propagate: device batch with at least np points expected");
+    set_error(std::string(name) + ": device batch with at least np points expected");
     return HPSI_ERR_ARG;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (psi->dtype == HPSI_C128)
     return td_run<double>(h, static_cast<double *>(psi->ptr), psi->ld, psi->nst, nsteps, dt, order, laser, t0,
-                          use_graph != 0, energy, dipole, norm2, st);
+                          use_graph != 0, energy, dipole, norm2, st, propagator);
   if (psi->dtype == HPSI_C64)
     return td_run<float>(h, static_cast<float *>(psi->ptr), psi->ld, psi->nst, nsteps, dt, order, laser, t0,
-                         use_graph != 0, energy, dipole, norm2, st);
-  set_error("hpsi_td_propagate: unknown dtype");
+                         use_graph != 0, energy, dipole, norm2, st, propagator);
+  set_error(std::string(name) + ": unknown dtype");
   return HPSI_ERR_ARG;
+}
+
+extern "C" hpsi_status hpsi_td_propagate(hpsi_hamiltonian *h, hpsi_batch *psi, int32_t nsteps, double dt,
+                                         int32_t order, const hpsi_laser *laser, double t0, int32_t use_graph,
+                                         double *energy, double *dipole, double *norm2, void *stream) {
+  return td_entry("hpsi_td_propagate", h, psi, nsteps, dt, order, laser, t0, use_graph, energy, dipole, norm2,
+                  stream, 0);
+}
+
+extern "C" hpsi_status hpsi_td_propagate_etrs(hpsi_hamiltonian *h, hpsi_batch *psi, int32_t nsteps, double dt,
+                                              int32_t order, const hpsi_laser *laser, double t0,
+                                              int32_t use_graph, double *energy, double *dipole, double *norm2,
+                                              void *stream) {
+  return td_entry("hpsi_td_propagate_etrs", h, psi, nsteps, dt, order, laser, t0, use_graph, energy, dipole, norm2,
+                  stream, 1);
 }

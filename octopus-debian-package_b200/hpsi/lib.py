@@ -76,6 +76,9 @@ SIGNATURES = {
     "hpsi_td_propagate": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
                                       C.POINTER(Laser), C.c_double, C.c_int32, C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_td_propagate_etrs": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
+                                           C.POINTER(Laser), C.c_double, C.c_int32, C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_group_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "hpsi_group_destroy": (C.c_int32, [C.c_void_p]),
     "hpsi_group_taylor_steps": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
@@ -308,15 +311,17 @@ class Hamiltonian:
 
     # exponential-midpoint time propagation (td_run with TDPropagator = exp_mid)
     def td_propagate(self, psi, nsteps, dt, order=4, E0=0.0, omega=0.0, T=0.0, pol=(0.0, 0.0, 1.0), t0=0.0,
-                     graph=True, nst=None, stream=None):
+                     graph=True, nst=None, stream=None, propagator="exp_mid"):
+        """propagator: "exp_mid" (hpsi_td_propagate) or "etrs" (hpsi_td_propagate_etrs)."""
         b = as_batch(psi, nst=nst)
         las = Laser()
         las.E0, las.omega, las.T = float(E0), float(omega), float(T)
         for a in range(3):
             las.pol[a] = float(pol[a])
         e, d, n = np.zeros(nsteps), np.zeros(nsteps), np.zeros(nsteps)
-        check(load().hpsi_td_propagate(self.handle, C.byref(b), int(nsteps), float(dt), int(order), C.byref(las),
-                                       float(t0), 1 if graph else 0, _dp(e), _dp(d), _dp(n), _stream_ptr(stream)))
+        fn = {"exp_mid": load().hpsi_td_propagate, "etrs": load().hpsi_td_propagate_etrs}[propagator]
+        check(fn(self.handle, C.byref(b), int(nsteps), float(dt), int(order), C.byref(las), float(t0),
+                 1 if graph else 0, _dp(e), _dp(d), _dp(n), _stream_ptr(stream)))
         return e, d, n
 
     def close(self):

@@ -227,9 +227,12 @@ def laser_field(E0, omega, T, t):
     return E0 * np.sin(np.pi * t / T) ** 2 * np.cos(omega * t)
 
 
-def td_propagate(H, v0, psi, nsteps, dt, E0, omega, T, pol=(0.0, 0.0, 1.0), order=4, t0=0.0):
+def td_propagate(H, v0, psi, nsteps, dt, E0, omega, T, pol=(0.0, 0.0, 1.0), order=4, t0=0.0,
+                 propagator="exp_mid"):
     """Exponential-midpoint propagation with the laser folded into v
-    (src/td/propagator_expmid.F90:52-100, src/hamiltonian/hamiltonian_elec.F90:1028).
+    (src/td/propagator_expmid.F90:52-100, src/hamiltonian/hamiltonian_elec.F90:1028),
+    or, with propagator="etrs", the independent-particle ETRS step
+    exp(-i dt/2 H(t_n+1)) exp(-i dt/2 H(t_n)) (src/td/propagator_etrs.F90:70-152).
 
     Returns (psi_final (np, nst), energy[n], dipole[n], norm2[n]) where the
     observables are those of psi(t_n) under H(t_n), summed over the states."""
@@ -246,8 +249,15 @@ def td_propagate(H, v0, psi, nsteps, dt, E0, omega, T, pol=(0.0, 0.0, 1.0), orde
         E.append(dv * float(np.sum(np.real(a.conj() * h))))
         D.append(dv * float(np.sum(np.abs(a) ** 2 * r[:, None])))
         N.append(dv * float(np.sum(np.abs(a) ** 2)))
-        H.v[:] = v0 + laser_field(E0, omega, T, tn + 0.5 * dt) * r
-        y = H.taylor(x, dt, order=order)
+        if propagator == "etrs":
+            y = H.taylor(x, 0.5 * dt, order=order)  # H(t_n) is in place
+            x = np.zeros_like(x)
+            x[: m.np] = y
+            H.v[:] = v0 + laser_field(E0, omega, T, tn + dt) * r
+            y = H.taylor(x, 0.5 * dt, order=order)
+        else:
+            H.v[:] = v0 + laser_field(E0, omega, T, tn + 0.5 * dt) * r
+            y = H.taylor(x, dt, order=order)
         x = np.zeros_like(x)
         x[: m.np] = y
     H.v[:] = v0

@@ -59,3 +59,20 @@ def test_td_runaway_detected(cuda):
     with pytest.raises(lib.HpsiError) as e:
         ham.td_propagate(x, 5, 1.0, graph=False)  # dt far beyond the Taylor stability limit
     assert e.value.status == 8
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_td_etrs_matches_oracle(cuda, graph):
+    """ETRS steps (two half-step exponentials with the fields of t_n and t_n+1)."""
+    import torch
+    from oracle import oracle as O
+    m, v, psi, dm, ham, H = _systems(seed=47)
+    nsteps, dt = 30, 0.02
+    ref, Er, Dr, Nr = O.td_propagate(H, v, psi, nsteps, dt, propagator="etrs", **LASER)
+    x = torch.from_numpy(psi.copy()).to(cuda)
+    E, D, N = ham.td_propagate(x, nsteps, dt, graph=graph, propagator="etrs", **LASER)
+    got = x.cpu().numpy()[: m.np]
+    assert rel_maxnorm_per_state(got, ref) <= 1e-11
+    assert np.max(np.abs(E - Er) / np.abs(Er)) <= 1e-11
+    assert np.max(np.abs(N - Nr) / Nr) <= 1e-12
+    assert np.max(np.abs(D - Dr)) <= 1e-11 * np.max(np.abs(Nr))
