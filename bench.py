@@ -313,6 +313,19 @@ def run_configs(args):
         el = time.perf_counter() - t0
         res[name] = (nsteps / el, E, D, N)
         del xs
+    # ETRS (two half-step exponentials per step) and the density of the
+    # propagated states, FP64, same system
+    xs = torch.from_numpy(s1.psi).to(dev)
+    ham.td_propagate(xs, 2, dt, graph=True, propagator="etrs", **laser)
+    torch.cuda.synchronize()
+    ns_e = 100 if args.small else 400
+    t0 = time.perf_counter()
+    ham.td_propagate(xs, ns_e, dt, graph=True, propagator="etrs", **laser)
+    r_etrs = ns_e / (time.perf_counter() - t0)
+    w = np.full(s1.psi.shape[1], 2.0)
+    rho = dm.density(xs, w)
+    ms_rho = _cuda_ms(lambda: dm.density(xs, w, rho=rho, accumulate=True), 20)
+    del xs
     (r64, E64, D64, N64), (r32, E32, D32, N32) = res["fp64_plain"], res["fp32_graph"]
     emit({"config": f"TD exp_mid, sphere R=12 h=0.2, 128 states, KB, laser E0=0.01 w=0.057 sin^2, "
                     f"{nsteps} steps dt={dt}", "unit": "TD steps/s",
@@ -320,7 +333,9 @@ def run_configs(args):
           "energy_rel_err_max": float(np.max(np.abs(E32 - E64) / np.abs(E64))),
           "dipole_abs_err_max": float(np.max(np.abs(D32 - D64))),
           "dipole_rel_err_max": float(np.max(np.abs(D32 - D64)) / max(np.max(np.abs(D64)), 1e-300)),
-          "norm_rel_err_max": float(np.max(np.abs(N32 - N64) / N64))})
+          "norm_rel_err_max": float(np.max(np.abs(N32 - N64) / N64)),
+          "etrs_fp64_graph_steps_per_s": r_etrs,
+          "density_accumulate_fp64": {"ms": ms_rho, "GB_per_s": m.np * s1.psi.shape[1] * 16 / ms_rho / 1e6}})
     del ham, dm
 
     # ---- 64 grouped systems of uneven size, 100 Taylor steps -----------------------

@@ -234,6 +234,18 @@ hpsi_status hpsi_group_taylor_steps(hpsi_group *group, hpsi_batch *psis,
 hpsi_status hpsi_autotune(hpsi_hamiltonian *ham, int32_t dtype, int64_t ld,
                           int32_t shape_out[4], double *ms_out, void *stream);
 
+/* Lanczos exponential psi <- exp(-i dt H) psi of a complex128 device batch
+ * (exponential_lanczos_batch, src/electrons/exponential.F90:766-901):
+ * Krylov spaces of dimension up to max_order (TDExpOrder, 2..64) built per
+ * state with classical Gram-Schmidt against the last two vectors, stopped
+ * once every state's error estimate is below tol (TDLanczosTol) after more
+ * than 3 iterations, or on breakdown.  iters_out: the dimension used;
+ * res_out: the largest error estimate (above tol when the expansion did not
+ * converge, which the reference reports as a warning). */
+hpsi_status hpsi_lanczos_step(hpsi_hamiltonian *ham, hpsi_batch *psi, double dt,
+                              int32_t max_order, double tol, int32_t *iters_out,
+                              double *res_out, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Exact discrete adjoint of the Taylor propagator for optimal control
  * (served to opt_control's backward propagation, bwd_step / bwd_step_2,

@@ -487,6 +487,8 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   h->ketobs.release();
   h->tdbuf.release();
   h->adjbuf.release();
+  h->lzbuf.release();
+  h->lzsmall.release();
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   if (h->capture_event) cudaEventDestroy(h->capture_event);
   if (h->xfer_in) cudaStreamDestroy(h->xfer_in);

@@ -95,5 +95,6 @@ struct hpsi_hamiltonian {
   hpsi::Workspace slab_in, slab_out;
   // workspaces
   hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small, tdbuf, adjbuf;
+  hpsi::Workspace lzbuf, lzsmall;  // Lanczos: Krylov vectors, reductions and coefficients
   void proj_free();
 };

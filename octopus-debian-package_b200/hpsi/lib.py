@@ -79,6 +79,8 @@ SIGNATURES = {
     "hpsi_td_propagate_etrs": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
                                            C.POINTER(Laser), C.c_double, C.c_int32, C.POINTER(C.c_double),
                                            C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_lanczos_step": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_double, C.c_int32, C.c_double,
+                                      C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_group_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "hpsi_group_destroy": (C.c_int32, [C.c_void_p]),
     "hpsi_group_taylor_steps": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
@@ -345,6 +347,16 @@ class Hamiltonian:
     def boundaries_set(self, psi, nst=None, stream=None):
         b = as_batch(psi, nst=nst)
         check(load().hpsi_boundaries_set(self.handle, C.byref(b), _stream_ptr(stream)))
+
+    # Lanczos branch of exponential_apply_batch
+    def lanczos_step(self, psi, dt, max_order=30, tol=1e-5, nst=None, stream=None):
+        """psi <- exp(-i dt H) psi by Lanczos; returns (Krylov dimension, error estimate)."""
+        b = as_batch(psi, nst=nst)
+        it = C.c_int32()
+        res = C.c_double()
+        check(load().hpsi_lanczos_step(self.handle, C.byref(b), float(dt), int(max_order), float(tol), C.byref(it),
+                                       C.byref(res), _stream_ptr(stream)))
+        return int(it.value), float(res.value)
 
     # Taylor branch of exponential_apply_batch
     def taylor_step(self, psi, dt, order=4, nst=None, observables=False, stream=None):

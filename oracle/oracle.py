@@ -264,6 +264,56 @@ def td_propagate(H, v0, psi, nsteps, dt, E0, omega, T, pol=(0.0, 0.0, 1.0), orde
     return x[: m.np], np.array(E), np.array(D), np.array(N)
 
 
+def lanczos(H, psi, dt, max_order=30, tol=1e-5):
+    """exp(-i dt H) psi by the Lanczos method of exponential_lanczos_batch
+    (src/electrons/exponential.F90:766-901): Krylov vectors orthogonalised by
+    classical Gram-Schmidt against the last two (X(mesh_batch_orthogonalization),
+    src/grid/mesh_batch_inc.F90:1168-1274), exp of the projected Hermitian matrix
+    by eigendecomposition (zlalg_exp), stop when every error estimate
+    |h(m+1,m) expo(m,1)| < tol after more than 3 iterations or on breakdown.
+    Returns (psi_new (np, nst), dimension used, largest error estimate)."""
+    m = H.mesh
+    dv = m.vol_pp
+    eps = np.finfo(np.float64).eps
+    x = np.array(np.asarray(psi)[: m.np], dtype=np.complex128)
+    nst = x.shape[1]
+    beta = np.sqrt(dv * np.sum(np.abs(x) ** 2, axis=0))
+    if np.all(np.abs(beta) <= 1e-12):
+        return x, 0, 0.0
+    V = [x / np.where(beta > 0, beta, 1.0)]
+    K = max_order
+    Hm = np.zeros((nst, K + 1, K + 1), dtype=np.complex128)
+    expo, res, it = None, np.zeros(nst), 1
+    for it in range(1, K + 1):
+        pad = np.zeros((m.np_part, nst), dtype=np.complex128)
+        pad[: m.np] = V[it - 1]
+        w = H.apply(pad)
+        lo = max(1, it - 1)
+        ov = [dv * np.sum(V[j - 1].conj() * w, axis=0) for j in range(lo, it + 1)]
+        for j, o in zip(range(lo, it + 1), ov):
+            Hm[:, j - 1, it - 1] = o
+        for j, o in zip(range(lo, it + 1), ov):
+            w = w - o[None, :] * V[j - 1]
+        nrm = np.sqrt(dv * np.sum(np.abs(w) ** 2, axis=0))
+        Hm[:, it, it - 1] = nrm
+        expo = []
+        for i in range(nst):
+            lam, Q = np.linalg.eigh(Hm[i, :it, :it], UPLO="U")
+            expo.append((Q * np.exp(-1j * dt * lam)[None, :]) @ Q.conj().T)
+        res = np.abs(nrm) * np.array([abs(e[it - 1, 0]) for e in expo])
+        if np.all(np.abs(nrm) < 1e4 * eps):
+            break
+        w = w / np.where(np.abs(nrm) >= 1e4 * eps, np.abs(nrm), 1.0)[None, :]
+        V.append(w)
+        if it > 3 and np.all(res < tol):
+            break
+    mdim = min(it, K)
+    out = np.zeros_like(x)
+    for j in range(mdim):
+        out += (beta * np.array([e[j, 0] for e in expo]))[None, :] * V[j]
+    return out, mdim, float(np.max(res))
+
+
 # ---------------------------------------------------------------------------
 # dense FP64 pieces
 def mesh_batch_nrm2(mesh, psi):

@@ -178,3 +178,28 @@ def test_density_restatement_matches_reference_loop():
             ref[ip] += w[ist] * (np.conj(psi[ip, ist]) * psi[ip, ist]).real
     got = O.density_accumulate(m, psi, w)
     assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(ref)
+
+
+def test_lanczos_restatement_matches_dense_exponential():
+    """The Lanczos restatement converges to exp(-i dt H) psi computed from the
+    eigendecomposition of the dense oracle H (Hermitian on the inner points)."""
+    from oracle import oracle as O
+    from hpsi import fixtures
+    from hpsi.mesh import index_box_mesh
+    from hpsi.stencil import laplacian_weights, star_points
+    rng = np.random.default_rng(7)
+    m = index_box_mesh((5, 4, 4), 0.3)
+    v = fixtures.soft_coulomb(m, rng)
+    proj = fixtures.kb_projectors(m, 1, rng, radius=0.5, min_dist=0.1, place_radius=0.1)
+    P = O.Projectors(proj.maps, proj.mats, proj.scals)
+    H = O.Hamiltonian(m, laplacian_weights(m.spacing), star_points(), v=v, projectors=P)
+    Hd = _dense_h(H, m.np)[: m.np]
+    Hd = 0.5 * (Hd + Hd.conj().T)
+    lam, Q = np.linalg.eigh(Hd)
+    psi = np.zeros((m.np_part, 3), dtype=np.complex128)
+    psi[: m.np] = rng.standard_normal((m.np, 3)) + 1j * rng.standard_normal((m.np, 3))
+    for dt in (0.01, 0.2):
+        ref = (Q * np.exp(-1j * dt * lam)[None, :]) @ (Q.conj().T @ psi[: m.np])
+        got, mdim, res = O.lanczos(H, psi, dt, max_order=60, tol=1e-11)
+        assert res < 1e-11 and mdim > 3
+        assert rel_maxnorm_per_state(got, ref) <= 1e-9
