@@ -325,6 +325,14 @@ def run_configs(args):
     w = np.full(s1.psi.shape[1], 2.0)
     rho = dm.density(xs, w)
     ms_rho = _cuda_ms(lambda: dm.density(xs, w, rho=rho, accumulate=True), 20)
+    # Lanczos step (TDLanczosTol = 1e-5, TDExpOrder 30) at dt = 0.05, ten times
+    # the Taylor-4 limit on this grid; host-synchronised every Krylov iteration
+    ham.lanczos_step(xs, 0.05, max_order=30, tol=1e-5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lz_it, lz_res = ham.lanczos_step(xs, 0.05, max_order=30, tol=1e-5)
+    torch.cuda.synchronize()
+    ms_lz = (time.perf_counter() - t0) * 1e3
     del xs
     (r64, E64, D64, N64), (r32, E32, D32, N32) = res["fp64_plain"], res["fp32_graph"]
     emit({"config": f"TD exp_mid, sphere R=12 h=0.2, 128 states, KB, laser E0=0.01 w=0.057 sin^2, "
@@ -335,7 +343,8 @@ def run_configs(args):
           "dipole_rel_err_max": float(np.max(np.abs(D32 - D64)) / max(np.max(np.abs(D64)), 1e-300)),
           "norm_rel_err_max": float(np.max(np.abs(N32 - N64) / N64)),
           "etrs_fp64_graph_steps_per_s": r_etrs,
-          "density_accumulate_fp64": {"ms": ms_rho, "GB_per_s": m.np * s1.psi.shape[1] * 16 / ms_rho / 1e6}})
+          "density_accumulate_fp64": {"ms": ms_rho, "GB_per_s": m.np * s1.psi.shape[1] * 16 / ms_rho / 1e6},
+          "lanczos_fp64_dt0.05": {"ms": ms_lz, "krylov_dim": lz_it, "error_estimate": lz_res}})
     del ham, dm
 
     # ---- 64 grouped systems of uneven size, 100 Taylor steps -----------------------
