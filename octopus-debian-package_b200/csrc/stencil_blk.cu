@@ -99,8 +99,14 @@ struct BlkLayout {
   static_assert(NT == 256 || NT == 512, "256 or 512 threads");
   // 16-byte copy rounds of a halo plane / an interior plane (the last round
   // may be partial)
-  static constexpr int HROUNDS = (HC * PCS + NT - 1) / NT, IROUNDS = (IC * PCS + NT - 1) / NT;
-  static constexpr bool HPART = (HC * PCS) % NT != 0, IPART = (IC * PCS) % NT != 0;
+  static constexpr int IROUNDS = (IC * PCS + NT - 1) / NT;
+  static constexpr bool IPART = (IC * PCS) % NT != 0;
+  // the 25-point star reads no cell of the four HAL x HAL corners of the halo
+  // plane: the fill gathers the SC star cells only (rows of the top and
+  // bottom halo over the tile's columns, full halo rows beside the tile)
+  static constexpr int SC = 2 * HAL * TX + TY * HX;
+  static constexpr int SROUNDS = (SC * PCS + NT - 1) / NT;
+  static constexpr bool SPART = (SC * PCS) % NT != 0;
   // two CTAs per SM for 256-thread blocks (shared memory <= 113 KB each)
   static constexpr int CTAS = (NT == 256 && CB_ == 64) ? 2 : 1;
   static constexpr int NBUF = (X0 || CTAS == 2) ? 3 : 4;  // data stages
@@ -138,6 +144,18 @@ __device__ __forceinline__ float wsel_t<float>(const double *, const float *f, i
 __device__ __forceinline__ void zero16(void *d) {
   *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
 }
+// Halo-plane cell (row-major in the HX x HY plane) of star cell i: i < HAL TX
+// top rows over the tile's columns, then TY full rows, then the bottom rows.
+template <class LY>
+__device__ __forceinline__ int star_cell(int i) {
+  constexpr int TX = LY::TX, TY = LY::TY, HX = LY::HX, HAL = LY::HAL;
+  if (i < HAL * TX) return (i / TX) * HX + HAL + i % TX;
+  i -= HAL * TX;
+  if (i < TY * HX) return (HAL + i / HX) * HX + i % HX;
+  i -= TY * HX;
+  return (HAL + TY + i / TX) * HX + HAL + i % TX;
+}
+
 // 16-byte cp.async that reads `bytes` (16 or 0) and zero-fills the rest
 __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, int bytes) {
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -171,7 +189,8 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   auto side = [&](int k) { return smem + LY::o_side + size_t(k % NSIDE) * LY::SIDEB; };
 
   // ---- copy roles ---------------------------------------------------------------
-  const int cpc = tid / PCS, piece = tid % PCS;  // cell (+ 32 per round) and 16-byte piece
+  const int cpc = tid / PCS, piece = tid % PCS;  // cell (+ NT / PCS per round) and 16-byte piece
+  __builtin_assume(cpc >= 0 && cpc < LY::NT / PCS);
   const T *in_base = static_cast<const T *>(p.in) + col + piece * EPP;
   const long long in_ld2 = 2 * p.in_ld;
   const T *x0_base = static_cast<const T *>(p.psi0) + col + piece * EPP;
@@ -218,17 +237,19 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
     if (p.phase_corr == nullptr) {
       // every entry is a row or -1 (zero): one zero-filling copy per piece
 #pragma unroll
-      for (int j = 0; j < LY::HROUNDS; ++j) {
-        const int cell = cpc + j * (LY::NT / PCS);
-        if (LY::HPART && j == LY::HROUNDS - 1 && cell >= LY::HC) break;
+      for (int j = 0; j < LY::SROUNDS; ++j) {
+        const int i = cpc + j * (LY::NT / PCS);
+        if (LY::SPART && j == LY::SROUNDS - 1 && i >= LY::SC) break;
+        const int cell = star_cell<LY>(i);
         const int src = map[cell];
         cp_async16_zfill(halo + cell * SL, in_base + max(src, 0) * in_ld2, src >= 0 ? 16 : 0);
       }
     } else {
 #pragma unroll 1
-      for (int j = 0; j < LY::HROUNDS; ++j) {
-        const int cell = cpc + j * (LY::NT / PCS);
-        if (LY::HPART && j == LY::HROUNDS - 1 && cell >= LY::HC) break;
+      for (int j = 0; j < LY::SROUNDS; ++j) {
+        const int i = cpc + j * (LY::NT / PCS);
+        if (LY::SPART && j == LY::SROUNDS - 1 && i >= LY::SC) break;
+        const int cell = star_cell<LY>(i);
         const int src = map[cell];
         T *d = halo + cell * SL;
         if (src >= 0) {
@@ -356,7 +377,9 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
     const int pz = zbeg + k;
     const double vz = fz * double(pz + B.lo[2]);
 
-    if (pz >= gz0 - HAL && pz <= gz1 + HAL) {
+    // warp-uniform test: a plane no cell of the warp needs is skipped by the
+    // whole warp (its contributions would only reach non-inner outputs)
+    if (__any_sync(0xffffffffu, pz >= gz0 - HAL && pz <= gz1 + HAL)) {
       // rows of the owned columns: y arms of every owned cell; the owned
       // cells themselves carry the centre (+ potential), the z arms and the x
       // arms of their siblings.  Columns innermost: consecutive multiply-adds
