@@ -325,6 +325,21 @@ def run_configs(args):
     w = np.full(s1.psi.shape[1], 2.0)
     rho = dm.density(xs, w)
     ms_rho = _cuda_ms(lambda: dm.density(xs, w, rho=rho, accumulate=True), 20)
+    # ghost rows of a two-slab partition of this mesh: device pack of the rows
+    # partition 0 sends (hpsi_ghost_pack), compared with the H psi it feeds
+    from hpsi.domain import partition_z
+    doms = partition_z(m, 2)
+    d0 = doms[0]
+    smap, _ = d0.device_maps(dev)
+    sbuf = torch.empty((smap.numel(), xs.shape[1]), dtype=xs.dtype, device=dev)
+    lp = torch.zeros((d0.mesh.np_part, xs.shape[1]), dtype=xs.dtype, device=dev)
+    lp[: d0.np_local + d0.np_ghost] = xs[torch.from_numpy(d0.global_rows[: d0.np_local + d0.np_ghost]).to(dev)]
+    ms_pack = _cuda_ms(lambda: lib.ghost_pack(lp, smap, sbuf), 20)
+    ghost_info = {"partitions": 2, "np_local": d0.np_local, "ghost_rows": d0.np_ghost,
+                  "rows_sent": int(smap.numel()), "pack_ms": ms_pack,
+                  "pack_GB_per_s": 2 * sbuf.numel() * sbuf.element_size() / ms_pack / 1e6,
+                  "message_MB": sbuf.numel() * sbuf.element_size() / 1e6}
+    del lp, sbuf
     # Lanczos step (TDLanczosTol = 1e-5, TDExpOrder 30) at dt = 0.05, ten times
     # the Taylor-4 limit on this grid; host-synchronised every Krylov iteration
     ham.lanczos_step(xs, 0.05, max_order=30, tol=1e-5)
@@ -344,7 +359,8 @@ def run_configs(args):
           "norm_rel_err_max": float(np.max(np.abs(N32 - N64) / N64)),
           "etrs_fp64_graph_steps_per_s": r_etrs,
           "density_accumulate_fp64": {"ms": ms_rho, "GB_per_s": m.np * s1.psi.shape[1] * 16 / ms_rho / 1e6},
-          "lanczos_fp64_dt0.05": {"ms": ms_lz, "krylov_dim": lz_it, "error_estimate": lz_res}})
+          "lanczos_fp64_dt0.05": {"ms": ms_lz, "krylov_dim": lz_it, "error_estimate": lz_res},
+          "ghost_pack_fp64": ghost_info})
     del ham, dm
 
     # ---- 64 grouped systems of uneven size, 100 Taylor steps -----------------------

@@ -312,6 +312,24 @@ hpsi_status hpsi_nrm2_noalloc(int32_t np, double vol_pp, const hpsi_batch *psi,
                               double *out, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* Ghost rows of a domain-parallel mesh (X(ghost_update_batch_start/finish),
+ * src/grid/boundaries_inc.F90:57-231, par_vec_t layout: local points, then
+ * ghost rows grouped by source partition, then boundary points).
+ * hpsi_ghost_pack: sendbuf[i][s] = psi[sendmap[i]][s] for i < count, s < nst
+ * (sendbuf contiguous, count x nst complex of psi's dtype; the reference's
+ * ghost_reorder kernel).  hpsi_ghost_unpack: psi[pos[i]][s] = recvbuf[i][s],
+ * for batches whose rows are not contiguous (ld > nst); with ld == nst the
+ * received message can land in the ghost rows directly.  Maps and buffers
+ * are device memory; map entries outside [0, npts) are skipped.  Stream
+ * ordered, no synchronisation.  After the exchange, hpsi_apply_h with
+ * set_bc = 0 reads the ghost rows as stored (boundary points must hold
+ * their boundary values, zero for a zero boundary). */
+hpsi_status hpsi_ghost_pack(const hpsi_batch *psi, const int32_t *sendmap,
+                            int32_t count, void *sendbuf, void *stream);
+hpsi_status hpsi_ghost_unpack(const void *recvbuf, const int32_t *pos,
+                              int32_t count, hpsi_batch *psi, void *stream);
+
+/* ------------------------------------------------------------------ */
 /* Library-wide controls and diagnostics. */
 const char *hpsi_last_error_string(void);
 /* Number of this library's kernels launched since load (diagnostic). */

@@ -1,0 +1,237 @@
+"""Domain-parallel meshes: partitions, ghost rows and their exchange.
+
+The host side of the reference's par_vec_t (src/grid/par_vec.F90:196-420,
+par_vec_init) and of X(ghost_update_batch_start/finish)
+(src/grid/boundaries_inc.F90:57-231):
+
+* ``partition_z`` splits the inner points of a mesh into ``nparts`` slabs of
+  consecutive z planes with about the same number of points (the reference
+  takes its partition from METIS or a similar library; a slab partition keeps
+  every partition's neighbours to the one below and the one above).
+* Each ``Domain`` holds the local mesh of one partition in the par_vec_t row
+  order -- its own inner points (in global order), then its ghost points
+  grouped by source partition (``ghost_rcounts``/``ghost_rdispls``), then the
+  boundary points its stencil reaches -- and the send map: the local rows that
+  each other partition holds as ghosts, grouped by destination
+  (``ghost_sendmap``, ``ghost_scounts``, ``ghost_sdispls``).
+* ``ghost_update`` packs the send rows on the device (``hpsi_ghost_pack``),
+  posts one receive and one send per neighbour through ``torch.distributed``
+  (NCCL between GPUs) and lands each message in the ghost rows (directly when
+  rows are contiguous, through ``hpsi_ghost_unpack`` otherwise).
+
+After the update, H psi of the partition's inner points is ``hpsi_apply_h``
+with ``set_bc = 0`` on the local mesh: ghost rows hold the neighbours' values
+and boundary rows zeros.  Kinetic and local terms only: KB spheres that cross
+partitions need a sum of the projections over the partitions
+(mesh%allreduce of hamiltonian_elec_base_inc.F90:836), which this module does
+not do; ``DomainHamiltonian`` refuses projectors.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .mesh import Mesh
+from .stencil import star_points
+
+
+@dataclass
+class Domain:
+    rank: int
+    nparts: int
+    mesh: Mesh                  # local mesh: inner | ghosts by source | boundary
+    global_rows: np.ndarray     # global row of every local row
+    np_ghost: int
+    ghost_rcounts: np.ndarray   # (nparts,) ghost rows received from each partition
+    ghost_rdispls: np.ndarray   # (nparts,) their offsets after the inner rows
+    ghost_sendmap: np.ndarray   # local rows sent, grouped by destination
+    ghost_scounts: np.ndarray   # (nparts,)
+    ghost_sdispls: np.ndarray   # (nparts,)
+    _dev: dict = field(default_factory=dict, repr=False)
+
+    @property
+    def np_local(self) -> int:
+        return self.mesh.np
+
+    @property
+    def inner_rows(self) -> np.ndarray:
+        """Global rows of this partition's inner points."""
+        return self.global_rows[: self.mesh.np]
+
+    def local_batch(self, psi_global: np.ndarray) -> np.ndarray:
+        """Local rows of a global (np_part, ld) batch: inner and ghost rows
+        copied, boundary rows zero (the zero boundary)."""
+        out = np.zeros((self.mesh.np_part,) + psi_global.shape[1:], dtype=psi_global.dtype)
+        n = self.mesh.np + self.np_ghost
+        out[:n] = psi_global[self.global_rows[:n]]
+        return out
+
+    def device_maps(self, device):
+        """int32 device copies of the send map and the ghost row positions."""
+        import torch
+        key = str(device)
+        if key not in self._dev:
+            ghost_pos = np.arange(self.mesh.np, self.mesh.np + self.np_ghost, dtype=np.int32)
+            self._dev[key] = (torch.from_numpy(self.ghost_sendmap.astype(np.int32)).to(device),
+                              torch.from_numpy(ghost_pos).to(device))
+        return self._dev[key]
+
+
+def _lookup(lxyz: np.ndarray):
+    lo = lxyz.min(0)
+    ext = lxyz.max(0) - lo + 1
+    lut = -np.ones(int(np.prod(ext)), dtype=np.int64)
+    def flat(c):
+        c = c - lo
+        return (c[..., 2] * ext[1] + c[..., 1]) * ext[0] + c[..., 0]
+    lut[flat(lxyz)] = np.arange(len(lxyz))
+    def find(c):
+        inside = np.all((c >= lo) & (c < lo + ext), axis=-1)
+        out = -np.ones(c.shape[:-1], dtype=np.int64)
+        out[inside] = lut[flat(c[inside])]
+        return out
+    return find
+
+
+def partition_z(mesh: Mesh, nparts: int, order: int = 4) -> list[Domain]:
+    """Slab partition of the inner points along z and the ghost layout of
+    every partition (par_vec_init, src/grid/par_vec.F90:196-420)."""
+    if mesh.periodic:
+        raise ValueError("partition_z: periodic meshes are not partitioned here")
+    if nparts < 1:
+        raise ValueError("partition_z: nparts must be >= 1")
+    L = np.asarray(mesh.lxyz, dtype=np.int64)
+    npi = mesh.np
+    z = L[:npi, 2]
+    zs, cnt = np.unique(z, return_counts=True)
+    if nparts > len(zs):
+        raise ValueError("partition_z: more partitions than z planes")
+    # cut after the plane where the cumulative count passes k/nparts of the points
+    cum = np.cumsum(cnt)
+    cuts, prev = [], -1
+    for k in range(1, nparts):
+        i = int(np.searchsorted(cum, k * npi / nparts))
+        # at least one plane in this partition and in each of the remaining ones
+        i = min(max(i, prev + 1), len(zs) - 1 - (nparts - k))
+        cuts.append(i)
+        prev = i
+    zcut = np.array([zs[i] for i in cuts], dtype=np.int64)   # last plane of partitions 0..nparts-2
+    part = np.searchsorted(zcut, z, side="left").astype(np.int64)
+    find = _lookup(L)
+    pts = star_points(order).astype(np.int64)
+
+    inner = [np.nonzero(part == p)[0] for p in range(nparts)]
+    needed = []
+    for p in range(nparts):
+        nb = find(L[inner[p]][:, None, :] + pts[None, :, :]).ravel()
+        if (nb < 0).any():
+            raise ValueError("partition_z: a stencil neighbour of an inner point is not in the mesh")
+        nb = np.unique(nb)
+        mine = np.zeros(L.shape[0], dtype=bool)
+        mine[inner[p]] = True
+        needed.append(nb[~mine[nb]])
+
+    ghosts = [[np.zeros(0, dtype=np.int64)] * nparts for _ in range(nparts)]  # ghosts[p][q]
+    bnds = []
+    for p in range(nparts):
+        nd = needed[p]
+        gi = nd[nd < npi]
+        for q in range(nparts):
+            if q != p:
+                ghosts[p][q] = np.sort(gi[part[gi] == q])
+        bnds.append(np.sort(nd[nd >= npi]))
+
+    doms = []
+    for p in range(nparts):
+        rc = np.array([len(ghosts[p][q]) for q in range(nparts)], dtype=np.int64)
+        rd = np.concatenate([[0], np.cumsum(rc)[:-1]]).astype(np.int64)
+        grow = np.concatenate([inner[p]] + [ghosts[p][q] for q in range(nparts)] + [bnds[p]]).astype(np.int64)
+        sc = np.array([len(ghosts[d][p]) for d in range(nparts)], dtype=np.int64)
+        sd = np.concatenate([[0], np.cumsum(sc)[:-1]]).astype(np.int64)
+        # rows of partition p that partition d holds as ghosts, in d's order,
+        # as local rows of p (its inner rows are in ascending global order)
+        smap = [np.searchsorted(inner[p], ghosts[d][p]) for d in range(nparts)]
+        smap = np.concatenate(smap).astype(np.int64) if smap else np.zeros(0, dtype=np.int64)
+        local = Mesh(lxyz=np.ascontiguousarray(L[grow].astype(np.int32)), np=len(inner[p]),
+                     spacing=np.asarray(mesh.spacing, dtype=np.float64).copy(),
+                     label=f"{mesh.label} part {p}/{nparts}")
+        doms.append(Domain(rank=p, nparts=nparts, mesh=local, global_rows=grow, np_ghost=int(rc.sum()),
+                           ghost_rcounts=rc, ghost_rdispls=rd, ghost_sendmap=smap,
+                           ghost_scounts=sc, ghost_sdispls=sd))
+    for p in range(nparts):
+        for d in range(nparts):
+            assert doms[p].ghost_scounts[d] == doms[d].ghost_rcounts[p]
+    return doms
+
+
+def ghost_update(dom: Domain, psi, nst=None, group=None, pack=None, unpack=None, sendbuf=None, recvbuf=None):
+    """Fill the ghost rows of the local batch ``psi`` (npts, ld) from the
+    neighbouring partitions; every rank of ``group`` calls it together.
+
+    ``pack(psi, sendmap, out, nst)`` and ``unpack(buf, pos, psi, nst)`` default
+    to the device kernels (hpsi_ghost_pack / hpsi_ghost_unpack); ``sendbuf`` and
+    ``recvbuf`` may pass preallocated (rows, nst) buffers.  Receives are posted
+    for every partition with ghost rows here, sends for every partition that
+    holds rows of this one, all at once (torch.distributed.batch_isend_irecv,
+    the reference's ring of irecv/isend), then waited for."""
+    import torch
+    import torch.distributed as dist
+    from . import lib
+    pack = pack or lib.ghost_pack
+    unpack = unpack or lib.ghost_unpack
+    nst = psi.shape[1] if nst is None else nst
+    ld = psi.shape[1]
+    dev = psi.device
+    nsend = int(dom.ghost_scounts.sum())
+    sendmap, ghost_pos = dom.device_maps(dev)
+    if sendbuf is None:
+        sendbuf = torch.empty((nsend, nst), dtype=psi.dtype, device=dev)
+    if nsend:
+        pack(psi, sendmap, sendbuf, nst=nst)
+        if dev.type == "cuda":
+            torch.cuda.current_stream(dev).synchronize()
+    direct = ld == nst
+    if not direct and recvbuf is None:
+        recvbuf = torch.empty((dom.np_ghost, nst), dtype=psi.dtype, device=dev)
+    ops = []
+    # receives first, counting upwards from this rank (the reference's ring order)
+    for k in range(dom.nparts):
+        q = (dom.rank + k) % dom.nparts
+        n = int(dom.ghost_rcounts[q])
+        if q == dom.rank or n == 0:
+            continue
+        off = int(dom.ghost_rdispls[q])
+        tgt = psi[dom.np_local + off: dom.np_local + off + n] if direct else recvbuf[off: off + n]
+        ops.append(dist.P2POp(dist.irecv, torch.view_as_real(tgt), q, group=group))
+    for k in range(dom.nparts):
+        q = (dom.rank - k) % dom.nparts
+        n = int(dom.ghost_scounts[q])
+        if q == dom.rank or n == 0:
+            continue
+        off = int(dom.ghost_sdispls[q])
+        ops.append(dist.P2POp(dist.isend, torch.view_as_real(sendbuf[off: off + n]), q, group=group))
+    if ops:
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()
+    if not direct and dom.np_ghost:
+        unpack(recvbuf, ghost_pos, psi, nst=nst)
+
+
+class DomainHamiltonian:
+    """Kinetic + local H psi of one partition on its local mesh."""
+
+    def __init__(self, dom: Domain, weights, points, v_global=None, projectors=None):
+        from . import lib
+        if projectors is not None:
+            raise ValueError("DomainHamiltonian: KB projectors across partitions are not supported")
+        self.dom = dom
+        self.dmesh = lib.DeviceMesh(dom.mesh)
+        v = None if v_global is None else np.asarray(v_global)[dom.inner_rows]
+        self.ham = lib.Hamiltonian(self.dmesh, weights, points, v=v)
+
+    def apply(self, psi, hpsi, nst=None, group=None):
+        """Ghost update of ``psi`` (boundary rows must be zero), then H psi of
+        the inner rows into ``hpsi`` (hpsi_apply_h, set_bc = 0)."""
+        ghost_update(self.dom, psi, nst=nst, group=group)
+        self.ham.apply(psi, hpsi, nst=nst, set_bc=False)

@@ -81,6 +81,8 @@ SIGNATURES = {
                                            C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_lanczos_step": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_double, C.c_int32, C.c_double,
                                       C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_ghost_pack": (C.c_int32, [C.POINTER(Batch), C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "hpsi_ghost_unpack": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(Batch), C.c_void_p]),
     "hpsi_group_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "hpsi_group_destroy": (C.c_int32, [C.c_void_p]),
     "hpsi_group_taylor_steps": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
@@ -423,3 +425,20 @@ def profile_query(label: str):
     ms = C.c_double()
     check(load().hpsi_profile_query(label.encode(), C.byref(n), C.byref(ms)))
     return int(n.value), float(ms.value)
+
+
+def ghost_pack(psi, sendmap, out, nst=None, stream=None):
+    """out[i, :nst] = psi[sendmap[i], :nst] on the device (hpsi_ghost_pack).
+
+    ``sendmap`` an int32 device tensor, ``out`` a contiguous (count, nst) device
+    tensor of psi's dtype."""
+    b = as_batch(psi, nst=nst)
+    check(load().hpsi_ghost_pack(C.byref(b), sendmap.data_ptr(), int(sendmap.numel()), out.data_ptr(),
+                                 _stream_ptr(stream)))
+
+
+def ghost_unpack(buf, pos, psi, nst=None, stream=None):
+    """psi[pos[i], :nst] = buf[i, :nst] on the device (hpsi_ghost_unpack)."""
+    b = as_batch(psi, nst=nst)
+    check(load().hpsi_ghost_unpack(buf.data_ptr(), pos.data_ptr(), int(pos.numel()), C.byref(b),
+                                   _stream_ptr(stream)))

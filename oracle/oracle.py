@@ -316,6 +316,24 @@ def lanczos(H, psi, dt, max_order=30, tol=1e-5):
 
 # ---------------------------------------------------------------------------
 # dense FP64 pieces
+def ghost_exchange(domains, batches):
+    """Ghost rows of every partition from the owners' inner rows, in place:
+    X(ghost_update_batch_start/finish) (src/grid/boundaries_inc.F90:57-231)
+    with the send map packed as the ghost_reorder kernel does and each message
+    landing at np_local + ghost_rdispls(source).  ``batches[p]`` is partition
+    p's local (npts, ld) array."""
+    for p, dp in enumerate(domains):
+        for q, dq in enumerate(domains):
+            n = int(dp.ghost_rcounts[q])
+            if q == p or n == 0:
+                continue
+            so = int(dq.ghost_sdispls[p])
+            rows = dq.ghost_sendmap[so: so + n]
+            ro = dp.np_local + int(dp.ghost_rdispls[q])
+            batches[p][ro: ro + n] = batches[q][rows]
+    return batches
+
+
 def mesh_batch_nrm2(mesh, psi):
     a = np.asarray(psi)[: mesh.np]
     return np.sqrt(mesh.vol_pp * np.sum(np.abs(a) ** 2, axis=0))

@@ -1,0 +1,118 @@
+"""Domain-parallel meshes on the CPU: partition layout, the oracle's ghost
+exchange, H psi of the partitions against the global H psi, and the
+torch.distributed exchange protocol over gloo with two ranks."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from helpers import small_sphere_system
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize("nparts", [2, 3, 5])
+def test_partition_layout_and_partitioned_hpsi(nparts):
+    from hpsi.domain import partition_z
+    from hpsi.stencil import laplacian_weights, star_points
+    from oracle import oracle as O
+    m, v, proj, psi = small_sphere_system(seed=11, nst=3)
+    doms = partition_z(m, nparts)
+    inner = np.concatenate([d.inner_rows for d in doms])
+    assert np.array_equal(np.sort(inner), np.arange(m.np))
+    w = laplacian_weights(m.spacing)
+    Hg = O.Hamiltonian(m, w, star_points(), v=v)
+    ref = Hg.apply(psi)
+    # local batches with the ghost rows still empty, then the oracle exchange
+    locs = []
+    for d in doms:
+        b = d.local_batch(psi)
+        b[d.np_local: d.np_local + d.np_ghost] = 0.0
+        locs.append(b)
+    O.ghost_exchange(doms, locs)
+    for d, b in zip(doms, locs):
+        n = d.np_local + d.np_ghost
+        assert np.array_equal(b[:n], psi[d.global_rows[:n]])
+        assert not b[n:].any()
+        H = O.Hamiltonian(d.mesh, w, star_points(), v=v[d.inner_rows], bc="none")
+        got = H.apply(b)
+        assert np.max(np.abs(got - ref[d.inner_rows])) <= 1e-13 * np.max(np.abs(ref))
+    for p, d in enumerate(doms):
+        assert d.ghost_rcounts[p] == 0 and d.ghost_scounts[p] == 0
+        if nparts > 1:
+            assert d.np_ghost > 0
+
+
+def test_partition_rejects_periodic_and_too_many_parts():
+    from hpsi.domain import partition_z
+    from hpsi.mesh import index_box_mesh
+    m = index_box_mesh((6, 5, 4), 0.3)
+    with pytest.raises(ValueError):
+        partition_z(m, 5)
+    m.periodic = True
+    with pytest.raises(ValueError):
+        partition_z(m, 2)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "octopus-debian-package_b200"))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    from helpers import small_sphere_system
+    from hpsi.domain import ghost_update, partition_z
+
+    # CPU stand-ins for the device pack/unpack kernels (the test checks the
+    # exchange protocol: counts, offsets, ring order, direct and buffered receives)
+    def pack(psi, sendmap, out, nst):
+        out.copy_(psi[sendmap.long(), :nst])
+
+    def unpack(buf, pos, psi, nst):
+        psi[pos.long(), :nst] = buf
+
+    m, v, proj, psi = small_sphere_system(seed=13, nst=4)
+    d = partition_z(m, world)[rank]
+    ok = []
+    for ld in (4, 8):
+        g = np.zeros((m.np_part, ld), dtype=np.complex128)
+        g[:, :4] = psi
+        b = d.local_batch(g)
+        b[d.np_local: d.np_local + d.np_ghost] = 0.0
+        t = torch.from_numpy(b)
+        ghost_update(d, t, nst=4, pack=pack, unpack=unpack)
+        n = d.np_local + d.np_ghost
+        ok.append(bool(np.array_equal(t.numpy()[:n], g[d.global_rows[:n]])))
+    dist.barrier()
+    dist.destroy_process_group()
+    out.put((rank, ok))
+
+
+def test_ghost_update_gloo_two_ranks():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res == {0: [True, True], 1: [True, True]}

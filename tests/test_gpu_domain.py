@@ -1,0 +1,84 @@
+"""Domain-parallel H psi on one GPU: the partitions run one after another in
+this process, their ghost rows packed by hpsi_ghost_pack and delivered by
+device copies (the part NCCL does between GPUs) or hpsi_ghost_unpack; the
+partitions' H psi must equal the global H psi of the same states."""
+import numpy as np
+import pytest
+
+from helpers import small_sphere_system
+
+pytestmark = pytest.mark.gpu
+
+
+def _exchange_on_one_gpu(doms, locs, nst):
+    import torch
+    from hpsi import lib
+    sends = []
+    for d, b in zip(doms, locs):
+        smap, _ = d.device_maps(b.device)
+        buf = torch.empty((int(d.ghost_scounts.sum()), nst), dtype=b.dtype, device=b.device)
+        if buf.shape[0]:
+            lib.ghost_pack(b, smap, buf, nst=nst)
+        sends.append(buf)
+    for p, d in enumerate(doms):
+        ld = locs[p].shape[1]
+        recv = torch.empty((d.np_ghost, nst), dtype=locs[p].dtype, device=locs[p].device)
+        for q, dq in enumerate(doms):
+            n = int(d.ghost_rcounts[q])
+            if n == 0:
+                continue
+            so, ro = int(dq.ghost_sdispls[p]), int(d.ghost_rdispls[q])
+            if ld == nst:  # contiguous rows: the message lands in the ghost rows
+                locs[p][d.np_local + ro: d.np_local + ro + n].copy_(sends[q][so: so + n])
+            else:
+                recv[ro: ro + n].copy_(sends[q][so: so + n])
+        if ld != nst and d.np_ghost:
+            _, pos = d.device_maps(locs[p].device)
+            lib.ghost_unpack(recv, pos, locs[p], nst=nst)
+
+
+@pytest.mark.parametrize("nparts,ld,dtype", [(2, 16, "c128"), (3, 16, "c128"), (3, 24, "c128"), (4, 32, "c64")])
+def test_partitioned_hpsi_equals_global(cuda, nparts, ld, dtype):
+    import torch
+    from hpsi import lib
+    from hpsi.domain import DomainHamiltonian, partition_z
+    from hpsi.stencil import laplacian_weights, star_points
+    nst = 16 if dtype == "c128" else 32
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    m, v, proj, psi = small_sphere_system(seed=17, nst=nst, radius=4.5)
+    g = np.zeros((m.np_part, ld), dtype=np.complex128)
+    g[:, :nst] = psi
+    g[m.np:] = 0.0
+    w = laplacian_weights(m.spacing)
+    dm = lib.DeviceMesh(m)
+    H = lib.Hamiltonian(dm, w, star_points(), v=v)
+    x = torch.from_numpy(g).to(cuda).to(tdt)
+    y = torch.zeros((m.np, ld), dtype=tdt, device=cuda)
+    H.apply(x, y, nst=nst)
+    ref = y.cpu().numpy()[:, :nst]
+    doms = partition_z(m, nparts)
+    hams = [DomainHamiltonian(d, w, star_points(), v_global=v) for d in doms]
+    locs = []
+    for d in doms:
+        b = d.local_batch(g)
+        b[d.np_local: d.np_local + d.np_ghost] = 0.0  # filled by the exchange
+        locs.append(torch.from_numpy(b).to(cuda).to(tdt))
+    _exchange_on_one_gpu(doms, locs, nst)
+    tol = 1e-13 if dtype == "c128" else 2e-6
+    for d, hm, b in zip(doms, hams, locs):
+        n = d.np_local + d.np_ghost
+        assert np.array_equal(b.cpu().numpy()[:n, :nst], g[d.global_rows[:n], :nst].astype(b.cpu().numpy().dtype))
+        out = torch.zeros((d.np_local, ld), dtype=tdt, device=cuda)
+        hm.ham.apply(b, out, nst=nst, set_bc=False)
+        got = out.cpu().numpy()[:, :nst]
+        assert np.max(np.abs(got - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+
+
+def test_ghost_pack_rejects_host_buffers(cuda):
+    import torch
+    from hpsi import lib
+    x = torch.zeros((10, 4), dtype=torch.complex128, device=cuda)
+    smap = torch.arange(3, dtype=torch.int32)
+    out = torch.zeros((3, 4), dtype=torch.complex128)
+    with pytest.raises(lib.HpsiError):
+        lib.ghost_pack(x, smap, out)
