@@ -171,6 +171,17 @@ hpsi_status hpsi_taylor_step(hpsi_hamiltonian *ham, hpsi_batch *psi, double dt_r
                              double dt_im, int32_t order, double *energy,
                              double *dipole, double *norm2, void *stream);
 
+/* exponential_apply_batch with its second output (psib2 / deltat2,
+ * src/electrons/exponential.F90:695-744, used by the self-consistent ETRS
+ * predictor): psi2 <- exp(-i dt2 H) psi, psi <- exp(-i dt H) psi, both by the
+ * order-`order` Taylor series (dt = dt_re + i dt_im, likewise dt2).  Device
+ * batches with at least np points, same dtype and nst, distinct storage;
+ * rows np.. of psi2 are not written.  No observables, no synchronisation. */
+hpsi_status hpsi_taylor_step_dual(hpsi_hamiltonian *ham, hpsi_batch *psi,
+                                  hpsi_batch *psi2, double dt_re, double dt_im,
+                                  double dt2_re, double dt2_im, int32_t order,
+                                  void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Time propagation with exponential-midpoint steps
  * (TDPropagator = exp_mid, src/td/propagator_expmid.F90:52-100, driven by

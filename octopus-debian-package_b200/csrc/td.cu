@@ -252,3 +252,54 @@ extern "C" hpsi_status hpsi_td_propagate_etrs(hpsi_hamiltonian *h, hpsi_batch *p
   return td_entry("hpsi_td_propagate_etrs", h, psi, nsteps, dt, order, laser, t0, use_graph, energy, dipole, norm2,
                   stream, 1);
 }
+
+// exponential_apply_batch with a second output (psib2, deltat2;
+// src/electrons/exponential.F90:695-744): psi2 <- exp(-i dt2 H) psi and
+// psi <- exp(-i dt H) psi, both by the order-`order` Taylor series of the same
+// H.  The reference accumulates both sums from one sequence H^k psi (power
+// form: per term one H apply and two axpys); here psi is copied into psi2 and
+// each output gets its own Horner sweep.  On an HBM-bound pass the two move
+// the same bytes (power form: read H^(k-1) psi, write H^k psi, update psi and
+// psi2 = 6 batch passes per term; two Horner chains: 2 x 3), while the Horner
+// form needs no extra batch for H^k psi.
+extern "C" hpsi_status hpsi_taylor_step_dual(hpsi_hamiltonian *h, hpsi_batch *psi, hpsi_batch *psi2, double dt_re,
+                                             double dt_im, double dt2_re, double dt2_im, int32_t order,
+                                             void *stream) {
+  if (!h || !psi || !psi2 || order < 1 || order > 32 || !std::isfinite(dt_re) || !std::isfinite(dt_im) ||
+      !std::isfinite(dt2_re) || !std::isfinite(dt2_im)) {
+    set_error("hpsi_taylor_step_dual: bad argument");
+    return HPSI_ERR_ARG;
+  }
+  if (!h->have_kinetic) {
+    set_error("hpsi_taylor_step_dual: kinetic weights not set");
+    return HPSI_ERR_STATE;
+  }
+  const int np = h->mesh->np;
+  for (const hpsi_batch *b : {static_cast<const hpsi_batch *>(psi), static_cast<const hpsi_batch *>(psi2)})
+    if (!b->ptr || b->npts < np || b->nst < 1 || b->ld < b->nst || !is_device_ptr(b->ptr)) {
+      set_error("hpsi_taylor_step_dual: device batches with at least np points expected");
+      return HPSI_ERR_ARG;
+    }
+  if (psi->dtype != psi2->dtype || psi->nst != psi2->nst || (psi->dtype != HPSI_C128 && psi->dtype != HPSI_C64) ||
+      psi->ptr == psi2->ptr) {
+    set_error("hpsi_taylor_step_dual: psi and psi2 must be distinct batches of one dtype and width");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t esz = psi->dtype == HPSI_C128 ? 16 : 8;
+  HPSI_TRY_CUDA(cudaMemcpy2DAsync(psi2->ptr, size_t(psi2->ld) * esz, psi->ptr, size_t(psi->ld) * esz,
+                                  size_t(psi->nst) * esz, np, cudaMemcpyDeviceToDevice, st));
+  hpsi_status s;
+  if (psi->dtype == HPSI_C128) {
+    s = taylor_dev<double>(h, static_cast<double *>(psi2->ptr), psi2->ld, psi2->nst, dt2_re, dt2_im, order, nullptr,
+                           st);
+    if (!s)
+      s = taylor_dev<double>(h, static_cast<double *>(psi->ptr), psi->ld, psi->nst, dt_re, dt_im, order, nullptr, st);
+  } else {
+    s = taylor_dev<float>(h, static_cast<float *>(psi2->ptr), psi2->ld, psi2->nst, dt2_re, dt2_im, order, nullptr,
+                          st);
+    if (!s)
+      s = taylor_dev<float>(h, static_cast<float *>(psi->ptr), psi->ld, psi->nst, dt_re, dt_im, order, nullptr, st);
+  }
+  return s;
+}

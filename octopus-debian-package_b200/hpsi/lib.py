@@ -81,6 +81,8 @@ SIGNATURES = {
                                            C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_lanczos_step": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_double, C.c_int32, C.c_double,
                                       C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_taylor_step_dual": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_double, C.c_double,
+                                          C.c_double, C.c_double, C.c_int32, C.c_void_p]),
     "hpsi_ghost_pack": (C.c_int32, [C.POINTER(Batch), C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "hpsi_ghost_unpack": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(Batch), C.c_void_p]),
     "hpsi_group_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
@@ -349,6 +351,14 @@ class Hamiltonian:
     def boundaries_set(self, psi, nst=None, stream=None):
         b = as_batch(psi, nst=nst)
         check(load().hpsi_boundaries_set(self.handle, C.byref(b), _stream_ptr(stream)))
+
+    def taylor_step_dual(self, psi, psi2, dt, dt2, order=4, nst=None, stream=None):
+        """psi2 <- exp(-i dt2 H) psi and psi <- exp(-i dt H) psi (Taylor, the
+        psib2 output of exponential_apply_batch)."""
+        b, b2 = as_batch(psi, nst=nst), as_batch(psi2, nst=nst)
+        dt, dt2 = complex(dt), complex(dt2)
+        check(load().hpsi_taylor_step_dual(self.handle, C.byref(b), C.byref(b2), dt.real, dt.imag, dt2.real,
+                                           dt2.imag, int(order), _stream_ptr(stream)))
 
     # Lanczos branch of exponential_apply_batch
     def lanczos_step(self, psi, dt, max_order=30, tol=1e-5, nst=None, stream=None):

@@ -76,3 +76,24 @@ def test_td_etrs_matches_oracle(cuda, graph):
     assert np.max(np.abs(E - Er) / np.abs(Er)) <= 1e-11
     assert np.max(np.abs(N - Nr) / Nr) <= 1e-12
     assert np.max(np.abs(D - Dr)) <= 1e-11 * np.max(np.abs(Nr))
+
+
+def test_taylor_step_dual_outputs(cuda):
+    """psib2 output of exponential_apply_batch: psi2 = exp(-i dt2 H) psi and
+    psi = exp(-i dt H) psi from one call, against the oracle's Taylor step."""
+    import torch
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    from oracle import oracle as O
+    from helpers import rel_maxnorm_per_state, small_sphere_system
+    m, v, proj, psi = small_sphere_system(seed=29, nst=8)
+    w = laplacian_weights(m.spacing)
+    ham = lib.Hamiltonian(lib.DeviceMesh(m), w, star_points(), v=v, projectors=proj)
+    H = O.Hamiltonian(m, w, star_points(), v=v, projectors=O.Projectors(proj.maps, proj.mats, proj.scals))
+    x = torch.from_numpy(psi.copy()).to(cuda)
+    x2 = torch.zeros((m.np, 16), dtype=torch.complex128, device=cuda)
+    ham.taylor_step_dual(x, x2, 0.005, 0.01, order=4, nst=8)  # psi2 rows strided (ld 16)
+    assert rel_maxnorm_per_state(x.cpu().numpy()[: m.np], H.taylor(psi, 0.005, 4)) <= 1e-12
+    assert rel_maxnorm_per_state(x2.cpu().numpy()[:, :8], H.taylor(psi, 0.01, 4)) <= 1e-12
+    with pytest.raises(lib.HpsiError):
+        ham.taylor_step_dual(x, x, 0.005, 0.01)  # same storage
