@@ -14,7 +14,7 @@ from helpers import small_sphere_system
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-@pytest.mark.parametrize("nparts", [2, 3, 5])
+@pytest.mark.parametrize("nparts", [1, 2, 3, 5])
 def test_partition_layout_and_partitioned_hpsi(nparts):
     from hpsi.domain import partition_z
     from hpsi.stencil import laplacian_weights, star_points
@@ -44,6 +44,8 @@ def test_partition_layout_and_partitioned_hpsi(nparts):
         assert d.ghost_rcounts[p] == 0 and d.ghost_scounts[p] == 0
         if nparts > 1:
             assert d.np_ghost > 0
+        else:
+            assert d.np_ghost == 0 and d.ghost_sendmap.size == 0 and d.mesh.np == m.np
 
 
 def test_partition_rejects_periodic_and_too_many_parts():
