@@ -329,13 +329,18 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   E *out = static_cast<E *>(p.out);
   const long long out_lde = 2 * p.out_ld / LY::LW;  // elements per output row
   const int ocol = col / LY::LW + l;
-  Kahan ke = {0, 0}, kn = {0, 0}, kd = {0, 0};
-  double n2c[RX][RY];  // observables: per-cell sums of |psi|^2 over the z march
-#pragma unroll
-  for (int cx = 0; cx < RX; ++cx)
-#pragma unroll
-    for (int r = 0; r < RY; ++r) n2c[cx][r] = 0.0;
-  (void)n2c;
+  // observables: plain per-thread sums over the thread's z march (a few
+  // hundred terms); the sums over threads and CTAs are compensated.  The x/y
+  // part of the dipole weight of the thread's first cell, dxy00, is the only
+  // per-cell constant kept live: fewer registers than per-cell norm sums
+  double se = 0.0, sn = 0.0, sd = 0.0;
+  const double dxy00 = OBS ? p.obs_pol[0] * B.h[0] * double(cx0 + bx + B.lo[0]) +
+                                 p.obs_pol[1] * B.h[1] * double(cy0 + by + B.lo[1])
+                           : 0.0;
+  (void)se;
+  (void)sn;
+  (void)sd;
+  (void)dxy00;
   (void)lane;
 
   // z range of the inner points under this thread's cells: planes more than
@@ -448,9 +453,10 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
           for (int cx = 0; cx < RX; ++cx) rowv[cx][r] = rows[(by + r) * TX + bx + cx];
         }
       }
-      double pe = 0.0, pn = 0.0;
+      double pe = 0.0, pn = 0.0, pd = 0.0;
       (void)pe;
       (void)pn;
+      (void)pd;
 #pragma unroll
       for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
@@ -483,16 +489,16 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
             }
             pe += eh;
             pn += n2;
-            n2c[cx][r] += n2;
+            if (cx || r) pd += n2 * (double(cx) * (p.obs_pol[0] * B.h[0]) + double(r) * (p.obs_pol[1] * B.h[1]));
           }
           out[row * out_lde + ocol] = val;
         }
       if constexpr (OBS) {
-        // energy: one compensated add per plane (the plane's few cells summed
-        // plainly first); norm: per-cell sums of positive terms, folded at
-        // the end; dipole: z part per plane, x/y parts from the cell sums
-        kadd(ke, pe);
-        kadd(kd, pn * (p.obs_pol[2] * B.h[2] * double(zo + B.lo[2])));
+        // the plane's cells summed first, then one add per plane and sum;
+        // dipole weight of a cell = dxy00 + its x/y offset terms (in pd) + z term
+        se += pe;
+        sn += pn;
+        sd += pn * (dxy00 + p.obs_pol[2] * B.h[2] * double(zo + B.lo[2])) + pd;
       }
     } else {
 #pragma unroll
@@ -539,26 +545,18 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   cp_async_wait<0>();
 
   if constexpr (OBS) {
-#pragma unroll
-    for (int cx = 0; cx < RX; ++cx)
-#pragma unroll
-      for (int r = 0; r < RY; ++r) {
-        kadd(kn, n2c[cx][r]);
-        kadd(kd, n2c[cx][r] * (p.obs_pol[0] * B.h[0] * double(cx0 + bx + cx + B.lo[0]) +
-                               p.obs_pol[1] * B.h[1] * double(cy0 + by + r + B.lo[1])));
-      }
     // per-state sums over the threads of this chunk; the two lanes of a state
     // fold into one entry
     __syncthreads();
     double *red = reinterpret_cast<double *>(smem);  // threads x 6
     {
       double *o = red + tid * 6;
-      o[0] = ke.s;
-      o[1] = ke.c;
-      o[2] = kn.s;
-      o[3] = kn.c;
-      o[4] = kd.s;
-      o[5] = kd.c;
+      o[0] = se;
+      o[1] = 0.0;
+      o[2] = sn;
+      o[3] = 0.0;
+      o[4] = sd;
+      o[5] = 0.0;
     }
     __syncthreads();
     if (tid < SL / 2) {
