@@ -1174,7 +1174,9 @@ hpsi_status apply_h_host_pipelined(hpsi_hamiltonian *h, const hpsi_batch *psi, h
 // HPSI_HOST_SLABS) whose width is a multiple of the blocked pass's chunk; 0
 // when the batch does not split.  Measured on 904,089 x 128 complex128 (two
 // 1.85 GB copies at 53-56 GB/s each way): 2 slabs 55.0 ms, 4 slabs 46.7 ms,
-// 8 slabs 53.5 ms (the strided copies of narrow slabs lose bandwidth).
+// 8 slabs 53.5 ms (the strided copies of narrow slabs lose bandwidth); four
+// slabs with the last split in two halves (a shorter copy-back tail) measured
+// within the run-to-run spread of four.
 long long pipeline_slab(const hpsi_batch *psi, const hpsi_batch *hpsi) {
   const long long chunk = psi->dtype == HPSI_C128 ? blk_chunk_states<double>() : blk_chunk_states<float>();
   if (psi->ld != hpsi->ld || psi->nst != psi->ld) return 0;

@@ -157,7 +157,8 @@ def test_paths_agree_fp32(cuda, monkeypatch):
         assert rel_maxnorm_per_state(o, outs[0]) <= 2e-6
 
 
-@pytest.mark.parametrize("dtype,ld", [(np.complex128, 32), (np.complex64, 64), (np.complex128, 12)])
+@pytest.mark.parametrize("dtype,ld", [(np.complex128, 32), (np.complex64, 64), (np.complex128, 12),
+                                      (np.complex128, 64), (np.complex64, 128)])
 @pytest.mark.parametrize("set_bc", [True, False])
 def test_host_batches_pipelined(cuda, dtype, ld, set_bc):
     """Host (pinned) batches go through the slab pipeline (copy-in, passes,
