@@ -82,3 +82,14 @@ def test_ghost_pack_rejects_host_buffers(cuda):
     out = torch.zeros((3, 4), dtype=torch.complex128)
     with pytest.raises(lib.HpsiError):
         lib.ghost_pack(x, smap, out)
+
+
+def test_ghost_pack_empty_map_is_a_no_op(cuda):
+    import torch
+    from hpsi import lib
+    x = torch.ones((10, 4), dtype=torch.complex64, device=cuda)
+    lib.ghost_pack(x, torch.zeros(0, dtype=torch.int32, device=cuda),
+                   torch.zeros((0, 4), dtype=torch.complex64, device=cuda))
+    lib.ghost_unpack(torch.zeros((0, 4), dtype=torch.complex64, device=cuda),
+                     torch.zeros(0, dtype=torch.int32, device=cuda), x)
+    assert x.abs().min().item() == 1.0

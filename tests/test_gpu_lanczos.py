@@ -53,3 +53,17 @@ def test_lanczos_stable_beyond_taylor_limit(cuda):
     n1 = np.sum(np.abs(x.cpu().numpy()[: m.np]) ** 2, axis=0)
     assert res < 1e-6
     assert np.max(np.abs(n1 - n0) / n0) <= 1e-6
+
+
+def test_lanczos_null_states_and_fp32_rejected(cuda):
+    """All-zero states: nothing to expand (the reference returns early too);
+    complex64 batches are refused (the Lanczos step is FP64 only)."""
+    import torch
+    from hpsi import lib
+    m, psi, ham, H = _setup(87, 4)
+    z = torch.zeros((m.np_part, 4), dtype=torch.complex128, device=cuda)
+    assert ham.lanczos_step(z, 0.05) == (0, 0.0)
+    assert not z.abs().max().item()
+    x32 = torch.from_numpy(psi.copy()).to(cuda).to(torch.complex64)
+    with pytest.raises(lib.HpsiError):
+        ham.lanczos_step(x32, 0.05)
