@@ -219,67 +219,92 @@ hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStrea
 namespace {
 template <typename T, typename C2>
 __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
-  const int s = blockIdx.x * 32 + threadIdx.x;
-  const bool active = s < k.nst;
+  // each thread serves two states (sb, sb + 32) of its rows: the row's
+  // metadata and projector weights are loaded once for both
+  constexpr int SPT = 2;
+  const int sb = blockIdx.x * 32 * SPT + threadIdx.x;
+  bool act[SPT];
+#pragma unroll
+  for (int u = 0; u < SPT; ++u) act[u] = sb + 32 * u < k.nst;
   const T *pt = static_cast<const T *>(k.pt);
   const C2 *proj = static_cast<const C2 *>(k.proj);
   C2 *out = static_cast<C2 *>(k.out);
   const C2 *psi0 = static_cast<const C2 *>(k.psi0);
-  Kahan ke = {0, 0};
+  Kahan ke[SPT];
+#pragma unroll
+  for (int u = 0; u < SPT; ++u) ke[u] = {0, 0};
   // each CTA row takes a contiguous range of covered rows: neighbouring rows
   // lie in the same few spheres, so their projections stay in L1
   const int per = (k.nk + gridDim.y - 1) / gridDim.y;
   const int r0 = blockIdx.y * per, r1 = min(k.nk, r0 + per);
   for (int i = r0 + threadIdx.y; i < r1; i += 8) {
-    if (!active) continue;
+    if (!act[0]) continue;
     const int row = k.krows[i];
-    // the output element is loaded before the sums, so its latency overlaps
-    // theirs (19 % faster on the R = 12 sphere; prefetching the next row's
-    // metadata as well measured slower again)
-    C2 *o = out + (long long)row * k.out_ld + s;
-    C2 y = *o;
-    C2 h;
-    h.x = 0;
-    h.y = 0;
+    // the output elements are loaded before the sums, so their latency
+    // overlaps theirs (prefetching the next row's metadata as well, or four
+    // rows per warp, measured slower)
+    C2 *o = out + (long long)row * k.out_ld + sb;
+    C2 y[SPT], h[SPT];
+#pragma unroll
+    for (int u = 0; u < SPT; ++u) {
+      if (act[u]) y[u] = o[32 * u];
+      h[u].x = 0;
+      h[u].y = 0;
+    }
     for (int e = k.kptr[i]; e < k.kptr[i + 1]; ++e) {
       const int4 E = __ldg(k.ent + e);
       const T *pp = pt + E.x;
-      const C2 *pr = proj + (long long)E.y * k.proj_ld + s;
+      const C2 *pr = proj + (long long)E.y * k.proj_ld + sb;
       for (int j = 0; j < E.z; ++j) {
         const T w = pp[j];
-        const C2 v = pr[(long long)j * k.proj_ld];
-        h.x += w * v.x;
-        h.y += w * v.y;
+#pragma unroll
+        for (int u = 0; u < SPT; ++u) {
+          if (!act[u]) continue;
+          const C2 v = pr[(long long)j * k.proj_ld + 32 * u];
+          h[u].x += w * v.x;
+          h[u].y += w * v.y;
+        }
       }
     }
-    if (k.mode == 1) {
-      const T ar = T(k.a_re), ai = T(k.a_im);
-      y.x += ar * h.x - ai * h.y;
-      y.y += ar * h.y + ai * h.x;
-    } else {
-      y.x += h.x;
-      y.y += h.y;
-    }
-    *o = y;
-    if (k.obs) {
-      const C2 x = psi0[(long long)row * k.psi0_ld + s];
-      kadd(ke, double(x.x) * double(h.x) + double(x.y) * double(h.y));
+#pragma unroll
+    for (int u = 0; u < SPT; ++u) {
+      if (!act[u]) continue;
+      if (k.mode == 1) {
+        const T ar = T(k.a_re), ai = T(k.a_im);
+        y[u].x += ar * h[u].x - ai * h[u].y;
+        y[u].y += ar * h[u].y + ai * h[u].x;
+      } else {
+        y[u].x += h[u].x;
+        y[u].y += h[u].y;
+      }
+      o[32 * u] = y[u];
+      if (k.obs) {
+        const C2 x = psi0[(long long)row * k.psi0_ld + sb + 32 * u];
+        kadd(ke[u], double(x.x) * double(h[u].x) + double(x.y) * double(h[u].y));
+      }
     }
   }
   if (k.obs) {
-    __shared__ double red[8][32][2];
-    red[threadIdx.y][threadIdx.x][0] = ke.s;
-    red[threadIdx.y][threadIdx.x][1] = ke.c;
+    __shared__ double red[8][32 * SPT][2];
+#pragma unroll
+    for (int u = 0; u < SPT; ++u) {
+      red[threadIdx.y][threadIdx.x + 32 * u][0] = ke[u].s;
+      red[threadIdx.y][threadIdx.x + 32 * u][1] = ke[u].c;
+    }
     __syncthreads();
-    if (threadIdx.y == 0 && active) {
-      Kahan a = {0, 0};
-      for (int y = 0; y < 8; ++y) {
-        kadd(a, red[y][threadIdx.x][0]);
-        a.c += red[y][threadIdx.x][1];
+    if (threadIdx.y == 0) {
+#pragma unroll
+      for (int u = 0; u < SPT; ++u) {
+        if (!act[u]) continue;
+        Kahan a = {0, 0};
+        for (int y = 0; y < 8; ++y) {
+          kadd(a, red[y][threadIdx.x + 32 * u][0]);
+          a.c += red[y][threadIdx.x + 32 * u][1];
+        }
+        double *o = k.obs + ((long long)blockIdx.y * k.obs_ld + sb + 32 * u) * 2;
+        o[0] = a.s;
+        o[1] = a.c;
       }
-      double *o = k.obs + ((long long)blockIdx.y * k.obs_ld + s) * 2;
-      o[0] = a.s;
-      o[1] = a.c;
     }
   }
 }
@@ -300,7 +325,7 @@ template <typename T>
 hpsi_status launch_ket(const KetArgs &k, cudaStream_t st) {
   if (k.nk == 0) return HPSI_OK;
   using C2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
-  dim3 grid((k.nst + 31) / 32, ket_row_blocks(k.nk));
+  dim3 grid((k.nst + 63) / 64, ket_row_blocks(k.nk));  // two states per thread
   ket_kernel<T, C2><<<grid, dim3(32, 8), 0, st>>>(k);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
