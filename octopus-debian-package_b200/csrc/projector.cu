@@ -220,7 +220,9 @@ namespace {
 template <typename T, typename C2>
 __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
   // each thread serves two states (sb, sb + 32) of its rows: the row's
-  // metadata and projector weights are loaded once for both
+  // metadata and projector weights are loaded once for both (12 % faster than
+  // one state per thread on the R = 12 sphere, 128 states; four states per
+  // thread measured 30 % slower, the grid no longer filling the GPU)
   constexpr int SPT = 2;
   const int sb = blockIdx.x * 32 * SPT + threadIdx.x;
   bool act[SPT];
