@@ -340,6 +340,29 @@ hpsi_status hpsi_ghost_pack(const hpsi_batch *psi, const int32_t *sendmap,
 hpsi_status hpsi_ghost_unpack(const void *recvbuf, const int32_t *pos,
                               int32_t count, hpsi_batch *psi, void *stream);
 
+/* The KB term split at its reduction, for meshes whose projector spheres
+ * cross partitions: X(hamiltonian_elec_base_nlocal_start) computes the
+ * projections of the local points, mesh%allreduce sums them over the
+ * partitions, X(hamiltonian_elec_base_nlocal_finish) adds the ket
+ * (src/hamiltonian/hamiltonian_elec_base_inc.F90:444-790, :836, :794-1200).
+ * hpsi_projector_bra:
+ *   proj[r][s] = scal[r] * sum_k P[k][r] * psi[map[k]][s]
+ * for every projection row r (matrices in order, their projectors in order)
+ * and s < psi->ld; proj is device memory of nprojections x psi->ld complex
+ * numbers of psi's dtype (row stride psi->ld).  A matrix with no points here
+ * gives zero rows, so every partition's rows line up for the sum.
+ * hpsi_projector_ket: hpsi[map[k]][s] += sum_r P[k][r] * proj[r][s] for
+ * s < hpsi->nst, proj laid out as the bra writes it with row stride
+ * hpsi->ld.  hpsi_apply_h without HPSI_TERM_NON_LOCAL_POTENTIAL followed by
+ * the bra, the sum and the ket equals hpsi_apply_h with every term.
+ * Batches and proj on the device; stream ordered, no synchronisation. */
+hpsi_status hpsi_projector_count(const hpsi_hamiltonian *ham,
+                                 int32_t *nprojections);
+hpsi_status hpsi_projector_bra(hpsi_hamiltonian *ham, const hpsi_batch *psi,
+                               void *proj, void *stream);
+hpsi_status hpsi_projector_ket(hpsi_hamiltonian *ham, const void *proj,
+                               hpsi_batch *hpsi, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Library-wide controls and diagnostics. */
 const char *hpsi_last_error_string(void);

@@ -1454,4 +1454,56 @@ hpsi_status hpsi_orthonormalize_cholesky(hpsi_mesh *m, hpsi_batch *psi, void *st
   return s;
 }
 
+hpsi_status hpsi_projector_count(const hpsi_hamiltonian *h, int32_t *nprojections) {
+  if (!h || !nprojections) return HPSI_ERR_ARG;
+  *nprojections = h->nmat > 0 ? h->nprojections : 0;
+  return HPSI_OK;
+}
+
+// proj must be device memory on a 16-byte boundary (the bra and ket read and
+// write whole complex numbers of each row)
+static hpsi_status check_proj(const void *proj, const char *what) {
+  if (!proj || !is_device_ptr(proj) || reinterpret_cast<uintptr_t>(proj) % 16 != 0) {
+    set_error(std::string(what) + ": proj must be device memory on a 16-byte boundary");
+    return HPSI_ERR_ARG;
+  }
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_projector_bra(hpsi_hamiltonian *h, const hpsi_batch *psi, void *proj, void *stream) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_status s = check_batch(h->mesh, psi, h->mesh->np, "hpsi_projector_bra(psi)");
+  if (s) return s;
+  if (h->nmat == 0) return HPSI_OK;
+  if (!is_device_ptr(psi->ptr)) {
+    set_error("hpsi_projector_bra: psi must be device memory");
+    return HPSI_ERR_ARG;
+  }
+  s = check_proj(proj, "hpsi_projector_bra");
+  if (s) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (psi->dtype == HPSI_C128)
+    return run_bra<double>(h, static_cast<const double *>(psi->ptr), psi->ld, static_cast<double *>(proj), st);
+  return run_bra<float>(h, static_cast<const float *>(psi->ptr), psi->ld, static_cast<float *>(proj), st);
+}
+
+hpsi_status hpsi_projector_ket(hpsi_hamiltonian *h, const void *proj, hpsi_batch *hpsi, void *stream) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_status s = check_batch(h->mesh, hpsi, h->mesh->np, "hpsi_projector_ket(hpsi)");
+  if (s) return s;
+  if (h->nmat == 0) return HPSI_OK;
+  if (!is_device_ptr(hpsi->ptr)) {
+    set_error("hpsi_projector_ket: hpsi must be device memory");
+    return HPSI_ERR_ARG;
+  }
+  s = check_proj(proj, "hpsi_projector_ket");
+  if (s) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (hpsi->dtype == HPSI_C128)
+    return run_ket<double>(h, static_cast<const double *>(proj), hpsi->ld, hpsi->nst,
+                           static_cast<double *>(hpsi->ptr), hpsi->ld, 0, 0.0, 0.0, nullptr, 0, nullptr, st);
+  return run_ket<float>(h, static_cast<const float *>(proj), hpsi->ld, hpsi->nst, static_cast<float *>(hpsi->ptr),
+                        hpsi->ld, 0, 0.0, 0.0, nullptr, 0, nullptr, st);
+}
+
 }  // extern "C"

@@ -21,10 +21,14 @@ par_vec_init) and of X(ghost_update_batch_start/finish)
 
 After the update, H psi of the partition's inner points is ``hpsi_apply_h``
 with ``set_bc = 0`` on the local mesh: ghost rows hold the neighbours' values
-and boundary rows zeros.  Kinetic and local terms only: KB spheres that cross
-partitions need a sum of the projections over the partitions
-(mesh%allreduce of hamiltonian_elec_base_inc.F90:836), which this module does
-not do; ``DomainHamiltonian`` refuses projectors.
+and boundary rows zeros.  KB spheres may cross partitions: each partition
+holds every projector matrix restricted to its own inner points
+(``local_projectors``), computes its share of the projections
+(``hpsi_projector_bra``), the shares are summed over the partitions (the
+mesh%allreduce of X(hamiltonian_elec_base_nlocal_finish),
+src/hamiltonian/hamiltonian_elec_base_inc.F90:836) while the stencil pass
+runs, and the sum is added back on the partition's covered rows
+(``hpsi_projector_ket``): ``apply_partitioned``.
 """
 from __future__ import annotations
 
@@ -218,20 +222,94 @@ def ghost_update(dom: Domain, psi, nst=None, group=None, pack=None, unpack=None,
         unpack(recvbuf, ghost_pos, psi, nst=nst)
 
 
+def local_projectors(dom: Domain, projectors):
+    """Every projector matrix restricted to the partition's inner points:
+    the sphere points this partition owns, as local rows, with their rows of
+    the matrix; a matrix with no point here keeps its projectors (and zero
+    points), so the projection rows of all partitions line up for the sum
+    (the reference builds the projector maps from the local points of each
+    domain, src/hamiltonian/hamiltonian_elec_base.F90:715-718)."""
+    from .fixtures import ProjectorSet
+    nglob = int(dom.global_rows.max()) + 1 if dom.global_rows.size else 0
+    nglob = max(nglob, max((int(np.max(m)) + 1 for m in projectors.maps if len(m)), default=0))
+    loc = -np.ones(nglob, dtype=np.int64)
+    loc[dom.inner_rows] = np.arange(dom.np_local)
+    maps, mats = [], []
+    for mp, mt in zip(projectors.maps, projectors.mats):
+        mp = np.asarray(mp, dtype=np.int64)
+        li = loc[mp]
+        sel = li >= 0
+        maps.append(li[sel].astype(np.int32))
+        mats.append(np.ascontiguousarray(np.asarray(mt, dtype=np.float64)[sel]))
+    return ProjectorSet(maps, mats, [np.asarray(c, dtype=np.float64) for c in projectors.scals],
+                        getattr(projectors, "positions", None))
+
+
+def apply_partitioned(dom: Domain, psi, hpsi, local_apply, bra=None, ket=None, proj=None, nst=None, group=None,
+                      pack=None, unpack=None):
+    """H psi of one partition; every rank of ``group`` calls it together.
+
+    1. ghost update of ``psi`` (``ghost_update``);
+    2. if ``bra`` is given: ``bra(psi, proj)`` writes this partition's share of
+       the KB projections into ``proj`` (nprojections, ld) and an
+       asynchronous all-reduce sums the shares over the ranks
+       (X(hamiltonian_elec_base_nlocal_start) and the mesh%allreduce of
+       hamiltonian_elec_base_inc.F90:836);
+    3. ``local_apply(psi, hpsi)``: kinetic and local terms on the local mesh,
+       overlapping the all-reduce;
+    4. wait for the sum, then ``ket(proj, hpsi)`` adds the KB term on the
+       covered rows (X(hamiltonian_elec_base_nlocal_finish)).
+    With NCCL the all-reduce runs on its own stream after the bra and the
+    ket's stream waits for it; nothing synchronises the host."""
+    import torch
+    import torch.distributed as dist
+    ghost_update(dom, psi, nst=nst, group=group, pack=pack, unpack=unpack)
+    work = None
+    if bra is not None:
+        bra(psi, proj)
+        if dom.nparts > 1:
+            work = dist.all_reduce(torch.view_as_real(proj), group=group, async_op=True)
+    local_apply(psi, hpsi)
+    if bra is not None:
+        if work is not None:
+            work.wait()
+        ket(proj, hpsi)
+
+
 class DomainHamiltonian:
-    """Kinetic + local H psi of one partition on its local mesh."""
+    """H psi of one partition on its local mesh: kinetic, local and KB terms
+    (KB spheres may cross partitions)."""
 
     def __init__(self, dom: Domain, weights, points, v_global=None, projectors=None):
         from . import lib
-        if projectors is not None:
-            raise ValueError("DomainHamiltonian: KB projectors across partitions are not supported")
         self.dom = dom
         self.dmesh = lib.DeviceMesh(dom.mesh)
         v = None if v_global is None else np.asarray(v_global)[dom.inner_rows]
-        self.ham = lib.Hamiltonian(self.dmesh, weights, points, v=v)
+        self.local_proj = None if projectors is None else local_projectors(dom, projectors)
+        self.ham = lib.Hamiltonian(self.dmesh, weights, points, v=v, projectors=self.local_proj)
+        self.nprojections = self.ham.nprojections()
+        self._proj = {}
+
+    def projection_buffer(self, psi):
+        """The (nprojections, ld) device buffer of the summed projections for
+        batches like ``psi`` (kept between calls)."""
+        import torch
+        key = (psi.dtype, psi.shape[1], str(psi.device))
+        if key not in self._proj:
+            self._proj[key] = torch.zeros((self.nprojections, psi.shape[1]), dtype=psi.dtype, device=psi.device)
+        return self._proj[key]
 
     def apply(self, psi, hpsi, nst=None, group=None):
         """Ghost update of ``psi`` (boundary rows must be zero), then H psi of
-        the inner rows into ``hpsi`` (hpsi_apply_h, set_bc = 0)."""
-        ghost_update(self.dom, psi, nst=nst, group=group)
-        self.ham.apply(psi, hpsi, nst=nst, set_bc=False)
+        the inner rows into ``hpsi``: hpsi_apply_h (set_bc = 0) for the
+        kinetic and local terms, the projections summed over the ranks of
+        ``group`` and the KB ket (``apply_partitioned``)."""
+        from . import lib
+        kb = self.nprojections > 0
+        terms = lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL
+        apply_partitioned(
+            self.dom, psi, hpsi,
+            lambda x, y: self.ham.apply(x, y, nst=nst, terms=terms, set_bc=False),
+            bra=self.ham.projector_bra if kb else None,
+            ket=(lambda p, y: self.ham.projector_ket(p, y, nst=nst)) if kb else None,
+            proj=self.projection_buffer(psi) if kb else None, nst=nst, group=group)

@@ -85,6 +85,9 @@ SIGNATURES = {
                                           C.c_double, C.c_double, C.c_int32, C.c_void_p]),
     "hpsi_ghost_pack": (C.c_int32, [C.POINTER(Batch), C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "hpsi_ghost_unpack": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(Batch), C.c_void_p]),
+    "hpsi_projector_count": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "hpsi_projector_bra": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),
+    "hpsi_projector_ket": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Batch), C.c_void_p]),
     "hpsi_group_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "hpsi_group_destroy": (C.c_int32, [C.c_void_p]),
     "hpsi_group_taylor_steps": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
@@ -347,6 +350,26 @@ class Hamiltonian:
         bo = as_batch(hpsi, nst=nst)
         check(load().hpsi_apply_h(self.handle, C.byref(bi), C.byref(bo), terms, 1 if set_bc else 0,
                                   _stream_ptr(stream)))
+
+    def nprojections(self) -> int:
+        n = C.c_int32()
+        check(load().hpsi_projector_count(self.handle, C.byref(n)))
+        return int(n.value)
+
+    # X(hamiltonian_elec_base_nlocal_start), without the reduction
+    def projector_bra(self, psi, proj, stream=None):
+        """proj (nprojections, ld) <- the KB projections of the device batch
+        psi (hpsi_projector_bra)."""
+        b = as_batch(psi)
+        check(load().hpsi_projector_bra(self.handle, C.byref(b), C.c_void_p(proj.data_ptr()),
+                                        _stream_ptr(stream)))
+
+    # X(hamiltonian_elec_base_nlocal_finish), after the reduction
+    def projector_ket(self, proj, hpsi, nst=None, stream=None):
+        """hpsi += P proj on the covered rows (hpsi_projector_ket)."""
+        b = as_batch(hpsi, nst=nst)
+        check(load().hpsi_projector_ket(self.handle, C.c_void_p(proj.data_ptr()), C.byref(b),
+                                        _stream_ptr(stream)))
 
     def boundaries_set(self, psi, nst=None, stream=None):
         b = as_batch(psi, nst=nst)

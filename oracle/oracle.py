@@ -12,6 +12,9 @@ adds the numpy restatements of the small dense pieces:
 * ``cholesky_orthonormalize`` -- states_elec_orthogonalization_full,
   ``cholesky_serial`` branch, src/states/states_elec_calc_inc.F90:66-98
   (S = U^H U, psi <- psi U^-1);
+* ``kb_bra`` / ``kb_ket`` -- the KB projections of a batch and their
+  scatter-add back, src/hamiltonian/hamiltonian_elec_base_inc.F90:650-780,
+  909-1027 (split at the reduction over domains, :836);
 * ``derivatives_test_error`` -- src/grid/derivatives_inc.F90:378-492, the
   Laplacian error that testsuite/components/03-derivatives_3d.test pins.
 
@@ -332,6 +335,31 @@ def ghost_exchange(domains, batches):
             ro = dp.np_local + int(dp.ghost_rdispls[q])
             batches[p][ro: ro + n] = batches[q][rows]
     return batches
+
+
+def kb_bra(maps, mats, scals, psi):
+    """KB projections of a batch, proj[r, s] = scal[r] * sum_k P[k, r] *
+    psi[map[k], s], matrices in order: the gather and GEMM of
+    X(hamiltonian_elec_base_nlocal_start)
+    (src/hamiltonian/hamiltonian_elec_base_inc.F90:650-780), before the
+    reduction over domains (:836)."""
+    x = np.asarray(psi)
+    rows = [np.asarray(sc, dtype=np.float64)[:, None] * (np.asarray(mt, dtype=np.float64).T @ x[np.asarray(mp)])
+            for mp, mt, sc in zip(maps, mats, scals)]
+    return np.concatenate(rows) if rows else np.zeros((0,) + x.shape[1:], dtype=x.dtype)
+
+
+def kb_ket(maps, mats, proj, h):
+    """h[map[k], s] += sum_r P[k, r] * proj[r, s], in place: the GEMM and
+    scatter-add of X(hamiltonian_elec_base_nlocal_finish)
+    (src/hamiltonian/hamiltonian_elec_base_inc.F90:909-1027)."""
+    r = 0
+    for mp, mt in zip(maps, mats):
+        mt = np.asarray(mt, dtype=np.float64)
+        n = mt.shape[1]
+        np.add.at(h, np.asarray(mp), mt @ proj[r: r + n])
+        r += n
+    return h
 
 
 def mesh_batch_nrm2(mesh, psi):

@@ -93,3 +93,84 @@ def test_ghost_pack_empty_map_is_a_no_op(cuda):
     lib.ghost_unpack(torch.zeros((0, 4), dtype=torch.complex64, device=cuda),
                      torch.zeros(0, dtype=torch.int32, device=cuda), x)
     assert x.abs().min().item() == 1.0
+
+
+@pytest.mark.parametrize("dtype,ld,nst", [("c128", 16, 13), ("c64", 32, 32)])
+def test_split_kb_term_equals_full_apply(cuda, dtype, ld, nst):
+    """hpsi_apply_h without the KB term, then hpsi_projector_bra and
+    hpsi_projector_ket, equals hpsi_apply_h with every term."""
+    import torch
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    m, v, proj, psi = small_sphere_system(seed=23, nst=nst, radius=4.5, natoms=4)
+    g = np.zeros((m.np_part, ld), dtype=np.complex128)
+    g[:, :nst] = psi
+    H = lib.Hamiltonian(lib.DeviceMesh(m), laplacian_weights(m.spacing), star_points(), v=v, projectors=proj)
+    x = torch.from_numpy(g).to(cuda).to(tdt)
+    full = torch.zeros((m.np, ld), dtype=tdt, device=cuda)
+    H.apply(x, full, nst=nst)
+    part = torch.zeros((m.np, ld), dtype=tdt, device=cuda)
+    H.apply(x, part, nst=nst, terms=lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL)
+    pr = torch.zeros((H.nprojections(), ld), dtype=tdt, device=cuda)
+    assert pr.shape[0] == sum(mt.shape[1] for mt in proj.mats)
+    H.projector_bra(x, pr)
+    H.projector_ket(pr, part, nst=nst)
+    a, b = full.cpu().numpy()[:, :nst], part.cpu().numpy()[:, :nst]
+    tol = 1e-13 if dtype == "c128" else 2e-6
+    assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(a))
+
+
+@pytest.mark.parametrize("nparts,ld,dtype", [(2, 16, "c128"), (3, 16, "c128"), (3, 32, "c64")])
+def test_partitioned_hpsi_with_kb_equals_global(cuda, nparts, ld, dtype):
+    """KB spheres across partitions: each partition's projection share
+    (hpsi_projector_bra on its own sphere points), summed on the device (the
+    all-reduce NCCL does between GPUs), added back by hpsi_projector_ket after
+    the kinetic and local pass; equals the global H psi with every term."""
+    import torch
+    from hpsi import lib
+    from hpsi.domain import DomainHamiltonian, partition_z
+    from hpsi.stencil import laplacian_weights, star_points
+    nst = 16
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    m, v, proj, psi = small_sphere_system(seed=29, nst=nst, radius=4.5, natoms=4)
+    g = np.zeros((m.np_part, ld), dtype=np.complex128)
+    g[:, :nst] = psi
+    w = laplacian_weights(m.spacing)
+    H = lib.Hamiltonian(lib.DeviceMesh(m), w, star_points(), v=v, projectors=proj)
+    x = torch.from_numpy(g).to(cuda).to(tdt)
+    y = torch.zeros((m.np, ld), dtype=tdt, device=cuda)
+    H.apply(x, y, nst=nst)
+    ref = y.cpu().numpy()[:, :nst]
+    doms = partition_z(m, nparts)
+    hams = [DomainHamiltonian(d, w, star_points(), v_global=v, projectors=proj) for d in doms]
+    locs = []
+    for d in doms:
+        b = d.local_batch(g)
+        b[d.np_local: d.np_local + d.np_ghost] = 0.0
+        locs.append(torch.from_numpy(b).to(cuda).to(tdt))
+    _exchange_on_one_gpu(doms, locs, nst)
+    shares = []
+    for hm, b in zip(hams, locs):
+        pr = torch.zeros((hm.nprojections, ld), dtype=tdt, device=cuda)
+        hm.ham.projector_bra(b, pr)
+        shares.append(pr)
+    total = torch.stack(shares).sum(0)
+    tol = 1e-13 if dtype == "c128" else 2e-6
+    for d, hm, b in zip(doms, hams, locs):
+        out = torch.zeros((d.np_local, ld), dtype=tdt, device=cuda)
+        hm.ham.apply(b, out, nst=nst, terms=lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL, set_bc=False)
+        hm.ham.projector_ket(total, out, nst=nst)
+        got = out.cpu().numpy()[:, :nst]
+        assert np.max(np.abs(got - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+
+
+def test_projector_bra_rejects_host_buffers(cuda):
+    import torch
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    m, v, proj, psi = small_sphere_system(seed=31, nst=4)
+    H = lib.Hamiltonian(lib.DeviceMesh(m), laplacian_weights(m.spacing), star_points(), v=v, projectors=proj)
+    x = torch.zeros((m.np_part, 4), dtype=torch.complex128, device=cuda)
+    with pytest.raises(lib.HpsiError):
+        H.projector_bra(x, torch.zeros((H.nprojections(), 4), dtype=torch.complex128))
