@@ -351,8 +351,8 @@ hpsi_status hpsi_ghost_unpack(const void *recvbuf, const int32_t *pos,
  * and s < psi->ld; proj is device memory of nprojections x psi->ld complex
  * numbers of psi's dtype (row stride psi->ld).  A matrix with no points here
  * gives zero rows, so every partition's rows line up for the sum.
- * hpsi_projector_ket: hpsi[map[k]][s] += sum_r P[k][r] * proj[r][s] for
- * s < hpsi->nst, proj laid out as the bra writes it with row stride
+ * hpsi_projector_ket: hpsi[map[k]][s] += a * sum_r P[k][r] * proj[r][s]
+ * (a = a_re + i a_im; 1 for H psi) for s < hpsi->nst, proj laid out as the bra writes it with row stride
  * hpsi->ld.  hpsi_apply_h without HPSI_TERM_NON_LOCAL_POTENTIAL followed by
  * the bra, the sum and the ket equals hpsi_apply_h with every term.
  * Batches and proj on the device; stream ordered, no synchronisation. */
@@ -361,7 +361,23 @@ hpsi_status hpsi_projector_count(const hpsi_hamiltonian *ham,
 hpsi_status hpsi_projector_bra(hpsi_hamiltonian *ham, const hpsi_batch *psi,
                                void *proj, void *stream);
 hpsi_status hpsi_projector_ket(hpsi_hamiltonian *ham, const void *proj,
-                               hpsi_batch *hpsi, void *stream);
+                               double a_re, double a_im, hpsi_batch *hpsi,
+                               void *stream);
+
+/* One level of the Horner form of the Taylor series
+ * (src/electrons/exponential.F90:701-748 sums the same polynomial term by
+ * term): out = psi0 + a * H psi on the np inner points, a = a_re + i a_im,
+ * for the terms selected.  psi holds np_part points (its boundary rows, or
+ * the ghost rows of a domain-parallel mesh, are read as stored with
+ * set_bc = 0); psi0 and out hold >= np points and may be the same batch, out
+ * may not be psi.  With the KB term split off (domain-parallel meshes), the
+ * ket of the summed projections follows with hpsi_projector_ket(.., a, ..).
+ * Order-K Taylor step: for k = K..1, in <- psi + (-i dt / k) H in.  Device
+ * batches with equal dtype, ld and nst; stream ordered. */
+hpsi_status hpsi_apply_h_horner(hpsi_hamiltonian *ham, const hpsi_batch *psi,
+                                const hpsi_batch *psi0, hpsi_batch *out,
+                                double a_re, double a_im, int32_t terms,
+                                int32_t set_bc, void *stream);
 
 /* ------------------------------------------------------------------ */
 /* Library-wide controls and diagnostics. */

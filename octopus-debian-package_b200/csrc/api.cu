@@ -1487,7 +1487,8 @@ hpsi_status hpsi_projector_bra(hpsi_hamiltonian *h, const hpsi_batch *psi, void 
   return run_bra<float>(h, static_cast<const float *>(psi->ptr), psi->ld, static_cast<float *>(proj), st);
 }
 
-hpsi_status hpsi_projector_ket(hpsi_hamiltonian *h, const void *proj, hpsi_batch *hpsi, void *stream) {
+hpsi_status hpsi_projector_ket(hpsi_hamiltonian *h, const void *proj, double a_re, double a_im, hpsi_batch *hpsi,
+                               void *stream) {
   if (!h) return HPSI_ERR_ARG;
   hpsi_status s = check_batch(h->mesh, hpsi, h->mesh->np, "hpsi_projector_ket(hpsi)");
   if (s) return s;
@@ -1499,11 +1500,49 @@ hpsi_status hpsi_projector_ket(hpsi_hamiltonian *h, const void *proj, hpsi_batch
   s = check_proj(proj, "hpsi_projector_ket");
   if (s) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int mode = (a_re == 1.0 && a_im == 0.0) ? PASS_APPLY : PASS_HORNER;
   if (hpsi->dtype == HPSI_C128)
     return run_ket<double>(h, static_cast<const double *>(proj), hpsi->ld, hpsi->nst,
-                           static_cast<double *>(hpsi->ptr), hpsi->ld, 0, 0.0, 0.0, nullptr, 0, nullptr, st);
+                           static_cast<double *>(hpsi->ptr), hpsi->ld, mode, a_re, a_im, nullptr, 0, nullptr, st);
   return run_ket<float>(h, static_cast<const float *>(proj), hpsi->ld, hpsi->nst, static_cast<float *>(hpsi->ptr),
-                        hpsi->ld, 0, 0.0, 0.0, nullptr, 0, nullptr, st);
+                        hpsi->ld, mode, a_re, a_im, nullptr, 0, nullptr, st);
+}
+
+hpsi_status hpsi_apply_h_horner(hpsi_hamiltonian *h, const hpsi_batch *psi, const hpsi_batch *psi0,
+                                hpsi_batch *out, double a_re, double a_im, int32_t terms, int32_t set_bc,
+                                void *stream) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_mesh *m = h->mesh;
+  hpsi_status s = check_batch(m, psi, m->np_part, "hpsi_apply_h_horner(psi)");
+  if (!s) s = check_batch(m, psi0, m->np, "hpsi_apply_h_horner(psi0)");
+  if (!s) s = check_batch(m, out, m->np, "hpsi_apply_h_horner(out)");
+  if (s) return s;
+  if (psi->dtype != out->dtype || psi0->dtype != out->dtype || psi->ld != out->ld || psi0->ld != out->ld ||
+      psi->nst != out->nst || psi0->nst != out->nst) {
+    set_error("hpsi_apply_h_horner: psi, psi0 and out differ in dtype, ld or nst");
+    return HPSI_ERR_ARG;
+  }
+  if (!is_device_ptr(psi->ptr) || !is_device_ptr(psi0->ptr) || !is_device_ptr(out->ptr)) {
+    set_error("hpsi_apply_h_horner: batches must be device memory");
+    return HPSI_ERR_ARG;
+  }
+  if (psi->ptr == out->ptr) {
+    set_error("hpsi_apply_h_horner: out must not be psi (the stencil reads neighbours of each row)");
+    return HPSI_ERR_ARG;
+  }
+  if ((terms & HPSI_TERM_KINETIC) && !h->have_kinetic) {
+    set_error("hpsi_apply_h_horner: kinetic weights not set");
+    return HPSI_ERR_STATE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long long ld = out->ld;
+  if (out->dtype == HPSI_C128)
+    return run_pass<double>(h, terms, load_map(h, set_bc), static_cast<const double *>(psi->ptr), ld,
+                            static_cast<double *>(out->ptr), ld, ld, PASS_HORNER,
+                            static_cast<const double *>(psi0->ptr), ld, a_re, a_im, nullptr, nullptr, st);
+  return run_pass<float>(h, terms, load_map(h, set_bc), static_cast<const float *>(psi->ptr), ld,
+                         static_cast<float *>(out->ptr), ld, ld, PASS_HORNER, static_cast<const float *>(psi0->ptr),
+                         ld, a_re, a_im, nullptr, nullptr, st);
 }
 
 }  // extern "C"

@@ -276,6 +276,45 @@ def apply_partitioned(dom: Domain, psi, hpsi, local_apply, bra=None, ket=None, p
         ket(proj, hpsi)
 
 
+def taylor_partitioned(dom: Domain, psi, work, horner, bra=None, ket=None, proj=None, dt=0.0, order=4, nst=None,
+                       group=None, pack=None, unpack=None):
+    """psi <- sum_{k=0..order} (-i dt H)^k / k! psi on this partition's inner
+    rows, every rank of ``group`` calling it together: the Taylor series of
+    exponential_taylor_series_batch (src/electrons/exponential.F90:677-757)
+    in Horner form, in <- psi + (-i dt / k) H in for k = order..1, each level
+    after a ghost update of its input (X(ghost_update_batch_start/finish)
+    inside every H psi of the reference's domain-parallel run).
+
+    ``work`` holds two (npts, ld) batches like ``psi`` whose boundary rows are
+    zero; ``horner(x, psi0, out, a)`` writes out = psi0 + a (T + V) x
+    (hpsi_apply_h_horner, set_bc = 0); with KB projectors ``bra(x, proj)``
+    writes this partition's projection share, summed over the ranks while the
+    pass runs, and ``ket(proj, out, a)`` adds a P proj."""
+    import torch
+    import torch.distributed as dist
+    if order < 1:
+        raise ValueError("taylor_partitioned: order must be >= 1")
+    dt = complex(dt)
+    x = psi
+    for k in range(order, 0, -1):
+        a = -1j * dt / k
+        out = work[(order - k) % 2] if (k > 1 or order == 1) else psi
+        ghost_update(dom, x, nst=nst, group=group, pack=pack, unpack=unpack)
+        work_ar = None
+        if bra is not None:
+            bra(x, proj)
+            if dom.nparts > 1:
+                work_ar = dist.all_reduce(torch.view_as_real(proj), group=group, async_op=True)
+        horner(x, psi, out, a)
+        if bra is not None:
+            if work_ar is not None:
+                work_ar.wait()
+            ket(proj, out, a)
+        x = out
+    if order == 1:
+        psi[: dom.np_local].copy_(x[: dom.np_local])
+
+
 class DomainHamiltonian:
     """H psi of one partition on its local mesh: kinetic, local and KB terms
     (KB spheres may cross partitions)."""
@@ -313,3 +352,21 @@ class DomainHamiltonian:
             bra=self.ham.projector_bra if kb else None,
             ket=(lambda p, y: self.ham.projector_ket(p, y, nst=nst)) if kb else None,
             proj=self.projection_buffer(psi) if kb else None, nst=nst, group=group)
+
+    def taylor_step(self, psi, dt, order=4, nst=None, group=None):
+        """psi <- exp(-i dt H) psi (order-``order`` Taylor) on the partition's
+        inner rows; ``psi`` is the local (np_part, ld) device batch with zero
+        boundary rows (``taylor_partitioned``)."""
+        import torch
+        from . import lib
+        key = ("work", psi.dtype, psi.shape, str(psi.device))
+        if key not in self._proj:
+            self._proj[key] = [torch.zeros_like(psi), torch.zeros_like(psi)]
+        kb = self.nprojections > 0
+        terms = lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL
+        taylor_partitioned(
+            self.dom, psi, self._proj[key],
+            lambda x, p0, y, a: self.ham.apply_horner(x, p0, y, a, nst=nst, terms=terms, set_bc=False),
+            bra=self.ham.projector_bra if kb else None,
+            ket=(lambda p, y, a: self.ham.projector_ket(p, y, nst=nst, a=a)) if kb else None,
+            proj=self.projection_buffer(psi) if kb else None, dt=dt, order=order, nst=nst, group=group)

@@ -87,7 +87,10 @@ SIGNATURES = {
     "hpsi_ghost_unpack": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(Batch), C.c_void_p]),
     "hpsi_projector_count": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32)]),
     "hpsi_projector_bra": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),
-    "hpsi_projector_ket": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(Batch), C.c_void_p]),
+    "hpsi_projector_ket": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.POINTER(Batch),
+                                       C.c_void_p]),
+    "hpsi_apply_h_horner": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(Batch),
+                                        C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_void_p]),
     "hpsi_group_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "hpsi_group_destroy": (C.c_int32, [C.c_void_p]),
     "hpsi_group_taylor_steps": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
@@ -365,11 +368,19 @@ class Hamiltonian:
                                         _stream_ptr(stream)))
 
     # X(hamiltonian_elec_base_nlocal_finish), after the reduction
-    def projector_ket(self, proj, hpsi, nst=None, stream=None):
-        """hpsi += P proj on the covered rows (hpsi_projector_ket)."""
+    def projector_ket(self, proj, hpsi, nst=None, a=1.0, stream=None):
+        """hpsi += a P proj on the covered rows (hpsi_projector_ket)."""
         b = as_batch(hpsi, nst=nst)
-        check(load().hpsi_projector_ket(self.handle, C.c_void_p(proj.data_ptr()), C.byref(b),
+        a = complex(a)
+        check(load().hpsi_projector_ket(self.handle, C.c_void_p(proj.data_ptr()), a.real, a.imag, C.byref(b),
                                         _stream_ptr(stream)))
+
+    def apply_horner(self, psi, psi0, out, a, nst=None, terms=TERM_ALL, set_bc=True, stream=None):
+        """out = psi0 + a H psi on the inner rows (hpsi_apply_h_horner)."""
+        bi, b0, bo = as_batch(psi, nst=nst), as_batch(psi0, nst=nst), as_batch(out, nst=nst)
+        a = complex(a)
+        check(load().hpsi_apply_h_horner(self.handle, C.byref(bi), C.byref(b0), C.byref(bo), a.real, a.imag,
+                                         terms, 1 if set_bc else 0, _stream_ptr(stream)))
 
     def boundaries_set(self, psi, nst=None, stream=None):
         b = as_batch(psi, nst=nst)

@@ -196,9 +196,28 @@ def _rank_kb_main(rank, world, port, out):
     apply_partitioned(d, x, y, lambda a, h: h.copy_(torch.from_numpy(Hl.apply(a.numpy()))),
                       bra=bra, ket=ket, proj=pr, pack=pack, unpack=unpack)
     err = float(np.max(np.abs(y.numpy() - ref[d.inner_rows])) / np.max(np.abs(ref)))
+
+    # Taylor step level by level (ghost update and projection sum per level)
+    from hpsi.domain import taylor_partitioned
+    dt = 0.02
+    ref_t = O.Hamiltonian(m, w, star_points(), v=v,
+                          projectors=O.Projectors(proj.maps, proj.mats, proj.scals)).taylor(psi, dt)
+
+    def horner(a_in, p0, o, a):
+        o[: d.np_local] = p0[: d.np_local] + a * torch.from_numpy(Hl.apply(a_in.numpy()))
+
+    def ket_a(p, h, a):
+        hn = h.numpy()
+        hn[: d.np_local] += a * O.kb_ket(lp.maps, lp.mats, p.numpy(), np.zeros((d.np_local, 3), complex))
+
+    x = torch.from_numpy(b.copy())
+    x[d.np_local: d.np_local + d.np_ghost] = 0.0
+    work = [torch.zeros_like(x), torch.zeros_like(x)]
+    taylor_partitioned(d, x, work, horner, bra=bra, ket=ket_a, proj=pr, dt=dt, order=4, pack=pack, unpack=unpack)
+    err_t = float(np.max(np.abs(x.numpy()[: d.np_local] - ref_t[d.inner_rows])) / np.max(np.abs(ref_t)))
     dist.barrier()
     dist.destroy_process_group()
-    out.put((rank, err))
+    out.put((rank, (err, err_t)))
 
 
 def test_partitioned_kb_gloo_two_ranks():
@@ -214,4 +233,5 @@ def test_partitioned_kb_gloo_two_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert set(res) == {0, 1}
-    assert max(res.values()) <= 1e-13
+    assert max(e for e, _ in res.values()) <= 1e-13
+    assert max(t for _, t in res.values()) <= 1e-12

@@ -174,3 +174,76 @@ def test_projector_bra_rejects_host_buffers(cuda):
     x = torch.zeros((m.np_part, 4), dtype=torch.complex128, device=cuda)
     with pytest.raises(lib.HpsiError):
         H.projector_bra(x, torch.zeros((H.nprojections(), 4), dtype=torch.complex128))
+
+
+@pytest.mark.parametrize("nparts,ld,dtype", [(2, 16, "c128"), (3, 16, "c128"), (3, 32, "c64")])
+def test_partitioned_taylor_step_equals_global(cuda, nparts, ld, dtype):
+    """Order-4 Taylor step on partitions, level by level in Horner form
+    (hpsi_apply_h_horner without the KB term, the projection shares of every
+    partition summed on the device, hpsi_projector_ket with a = -i dt / k),
+    each level after a ghost exchange: equals the global hpsi_taylor_step."""
+    import torch
+    from hpsi import lib
+    from hpsi.domain import DomainHamiltonian, partition_z
+    from hpsi.stencil import laplacian_weights, star_points
+    nst, dt, order = 16, 0.02, 4
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    m, v, proj, psi = small_sphere_system(seed=37, nst=nst, radius=4.5, natoms=4)
+    g = np.zeros((m.np_part, ld), dtype=np.complex128)
+    g[:, :nst] = psi
+    w = laplacian_weights(m.spacing)
+    H = lib.Hamiltonian(lib.DeviceMesh(m), w, star_points(), v=v, projectors=proj)
+    xg = torch.from_numpy(g).to(cuda).to(tdt)
+    H.taylor_step(xg, dt, order=order, nst=nst)
+    ref = xg.cpu().numpy()[: m.np, :nst]
+    doms = partition_z(m, nparts)
+    hams = [DomainHamiltonian(d, w, star_points(), v_global=v, projectors=proj) for d in doms]
+    psis = []
+    for d in doms:
+        b = d.local_batch(g)
+        b[d.np_local: d.np_local + d.np_ghost] = 0.0
+        psis.append(torch.from_numpy(b).to(cuda).to(tdt))
+    work = [[torch.zeros_like(p), torch.zeros_like(p)] for p in psis]
+    terms = lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL
+    xs = list(psis)
+    for k in range(order, 0, -1):
+        a = -1j * dt / k
+        _exchange_on_one_gpu(doms, xs, nst)
+        shares = []
+        for hm, x in zip(hams, xs):
+            pr = torch.zeros((hm.nprojections, ld), dtype=tdt, device=cuda)
+            hm.ham.projector_bra(x, pr)
+            shares.append(pr)
+        total = torch.stack(shares).sum(0)
+        outs = []
+        for p, (hm, x) in enumerate(zip(hams, xs)):
+            out = work[p][(order - k) % 2] if k > 1 else psis[p]
+            hm.ham.apply_horner(x, psis[p], out, a, nst=nst, terms=terms, set_bc=False)
+            hm.ham.projector_ket(total, out, nst=nst, a=a)
+            outs.append(out)
+        xs = outs
+    tol = 1e-12 if dtype == "c128" else 1e-5
+    for d, p in zip(doms, psis):
+        got = p.cpu().numpy()[: d.np_local, :nst]
+        assert np.max(np.abs(got - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+
+
+def test_apply_h_horner_matches_apply(cuda):
+    """hpsi_apply_h_horner: out = psi0 + a H psi (every term), and it refuses
+    out aliasing psi."""
+    import torch
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    m, v, proj, psi = small_sphere_system(seed=41, nst=8, radius=4.0, natoms=3)
+    H = lib.Hamiltonian(lib.DeviceMesh(m), laplacian_weights(m.spacing), star_points(), v=v, projectors=proj)
+    x = torch.from_numpy(psi).to(cuda)
+    p0 = torch.from_numpy(np.roll(psi, 1, axis=1)).to(cuda)
+    hx = torch.zeros((m.np, 8), dtype=torch.complex128, device=cuda)
+    H.apply(x, hx)
+    a = 0.3 - 0.7j
+    out = torch.zeros((m.np, 8), dtype=torch.complex128, device=cuda)
+    H.apply_horner(x, p0, out, a)
+    want = p0[: m.np] + a * hx
+    assert (out - want).abs().max().item() <= 1e-13 * want.abs().max().item()
+    with pytest.raises(lib.HpsiError):
+        H.apply_horner(x, p0, x, a)
