@@ -29,6 +29,11 @@ mesh%allreduce of X(hamiltonian_elec_base_nlocal_finish),
 src/hamiltonian/hamiltonian_elec_base_inc.F90:836) while the stencil pass
 runs, and the sum is added back on the partition's covered rows
 (``hpsi_projector_ket``): ``apply_partitioned``.
+
+The Taylor exponential on partitions (``taylor_partitioned``) runs its
+Horner levels one at a time, each after a ghost update of its input:
+``hpsi_apply_h_horner`` for the kinetic and local terms and, with KB spheres,
+the summed projections added with the level's factor -i dt / k.
 """
 from __future__ import annotations
 
