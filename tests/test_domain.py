@@ -235,3 +235,54 @@ def test_partitioned_kb_gloo_two_ranks():
     assert set(res) == {0, 1}
     assert max(e for e, _ in res.values()) <= 1e-13
     assert max(t for _, t in res.values()) <= 1e-12
+
+
+@pytest.mark.parametrize("order", [1, 2, 4])
+def test_taylor_partitioned_single_partition_orders(order):
+    """One partition (no exchange, no all-reduce): the level-by-level Taylor
+    step with oracle stand-ins equals the oracle's Taylor step of each order,
+    order 1 included (its result lands in a work batch and is copied back)."""
+    import torch
+    from hpsi.domain import local_projectors, partition_z, taylor_partitioned
+    from hpsi.stencil import laplacian_weights, star_points
+    from oracle import oracle as O
+    m, v, proj, psi = small_sphere_system(seed=43, nst=2, natoms=2)
+    w = laplacian_weights(m.spacing)
+    dt = 0.03
+    ref = O.Hamiltonian(m, w, star_points(), v=v,
+                        projectors=O.Projectors(proj.maps, proj.mats, proj.scals)).taylor(psi, dt, order=order)
+    d = partition_z(m, 1)[0]
+    lp = local_projectors(d, proj)
+    Hl = O.Hamiltonian(d.mesh, w, star_points(), v=v[d.inner_rows], bc="none")
+    x = torch.from_numpy(d.local_batch(psi))
+    work = [torch.zeros_like(x), torch.zeros_like(x)]
+    pr = torch.zeros((sum(mt.shape[1] for mt in lp.mats), 2), dtype=torch.complex128)
+
+    def horner(a_in, p0, o, a):
+        o[: d.np_local] = p0[: d.np_local] + a * torch.from_numpy(Hl.apply(a_in.numpy()))
+
+    def bra(a_in, p):
+        p.copy_(torch.from_numpy(O.kb_bra(lp.maps, lp.mats, lp.scals, a_in.numpy()[: d.np_local])))
+
+    def ket(p, h, a):
+        h.numpy()[: d.np_local] += a * O.kb_ket(lp.maps, lp.mats, p.numpy(), np.zeros((d.np_local, 2), complex))
+
+    taylor_partitioned(d, x, work, horner, bra=bra, ket=ket, proj=pr, dt=dt, order=order)
+    got = x.numpy()[: d.np_local]
+    assert np.max(np.abs(got - ref[d.inner_rows])) <= 1e-12 * np.max(np.abs(ref))
+
+
+def test_local_projectors_partition_without_spheres():
+    """A partition that no sphere reaches keeps every matrix with zero
+    points: its projection share is zero and its rows still line up."""
+    from hpsi.domain import local_projectors, partition_z
+    from oracle import oracle as O
+    m, v, proj, psi = small_sphere_system(seed=47, nst=2, natoms=1)
+    doms = partition_z(m, 5)
+    lps = [local_projectors(d, proj) for d in doms]
+    empty = [i for i, lp in enumerate(lps) if all(len(a) == 0 for a in lp.maps)]
+    assert empty, "expected a partition outside the one sphere"
+    lp, d = lps[empty[0]], doms[empty[0]]
+    assert [mt.shape[1] for mt in lp.mats] == [mt.shape[1] for mt in proj.mats]
+    share = O.kb_bra(lp.maps, lp.mats, lp.scals, d.local_batch(psi)[: d.np_local])
+    assert share.shape == (sum(mt.shape[1] for mt in proj.mats), 2) and not share.any()
