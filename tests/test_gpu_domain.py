@@ -247,3 +247,37 @@ def test_apply_h_horner_matches_apply(cuda):
     assert (out - want).abs().max().item() <= 1e-13 * want.abs().max().item()
     with pytest.raises(lib.HpsiError):
         H.apply_horner(x, p0, x, a)
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_domain_hamiltonian_methods_single_partition(cuda, dtype):
+    """DomainHamiltonian.apply and .taylor_step (the classes' own paths:
+    apply_partitioned, taylor_partitioned, the projection buffer) on one
+    partition, where no exchange or all-reduce runs: equal the global
+    hpsi_apply_h and hpsi_taylor_step."""
+    import torch
+    from hpsi import lib
+    from hpsi.domain import DomainHamiltonian, partition_z
+    from hpsi.stencil import laplacian_weights, star_points
+    nst, ld, dt = 16, 16, 0.02
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    m, v, proj, psi = small_sphere_system(seed=53, nst=nst, radius=4.5, natoms=4)
+    w = laplacian_weights(m.spacing)
+    H = lib.Hamiltonian(lib.DeviceMesh(m), w, star_points(), v=v, projectors=proj)
+    x = torch.from_numpy(psi).to(cuda).to(tdt)
+    y = torch.zeros((m.np, ld), dtype=tdt, device=cuda)
+    H.apply(x, y)
+    d = partition_z(m, 1)[0]
+    hm = DomainHamiltonian(d, w, star_points(), v_global=v, projectors=proj)
+    xl = torch.from_numpy(d.local_batch(psi)).to(cuda).to(tdt)
+    yl = torch.zeros((d.np_local, ld), dtype=tdt, device=cuda)
+    hm.apply(xl, yl)
+    tol = 1e-13 if dtype == "c128" else 2e-6
+    ref = y.cpu().numpy()
+    assert np.max(np.abs(yl.cpu().numpy() - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+    H.taylor_step(x, dt)
+    hm.taylor_step(xl, dt)
+    ref_t = x.cpu().numpy()[: m.np]
+    tol_t = 1e-12 if dtype == "c128" else 1e-5
+    got_t = xl.cpu().numpy()[: d.np_local]
+    assert np.max(np.abs(got_t - ref_t[d.inner_rows])) <= tol_t * np.max(np.abs(ref_t))
