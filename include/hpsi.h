@@ -18,6 +18,11 @@
  *    returns only when the result is back in host memory).
  *  - Every call that takes a `stream` is ordered on that CUDA stream
  *    (cudaStream_t passed as void*; NULL is the legacy default stream).
+ *  - Handles own device scratch that their calls reuse: a hamiltonian its
+ *    Taylor work batches, projection and split-K buffers; a mesh its
+ *    reduction scratch and the staging buffers of host batches.  Calls that
+ *    share a handle (a mesh included) must be ordered on the GPU: one stream,
+ *    or events between streams.
  *  - Errors are returned as hpsi_status; the library never exits the process.
  *    hpsi_last_error_string() gives a one-line message for the calling thread.
  */
