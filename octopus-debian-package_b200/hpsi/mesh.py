@@ -203,3 +203,108 @@ def permuted(mesh: Mesh, seed: int = 0) -> tuple[Mesh, np.ndarray, np.ndarray]:
         old_b = perm[mesh.np:] - mesh.np
         m2.per_inner = np.ascontiguousarray(inv[mesh.per_inner[old_b]].astype(np.int32))
     return m2, perm, inv
+
+
+# ---------------------------------------------------------------------------
+# Mesh order on disk: the restart file indices.obf
+
+IO_TYPE_INT_32 = 4   # TYPE_INT_32 of src/basic/io_binary.h:39
+IO_TYPE_INT_64 = 5   # TYPE_INT_64 of src/basic/io_binary.h:40
+_OBF_HEADER = np.dtype([("text", "S7"), ("version", "u1"), ("one_32", "<u4"), ("one_f", "<f4"),
+                        ("one_64", "<u8"), ("one_d", "<f8"), ("np", "<u8"), ("type", "<u4"),
+                        ("extra", "<u4", (5,))])
+assert _OBF_HEADER.itemsize == 64
+
+
+def cubic_extent(mesh: Mesh) -> np.ndarray:
+    """Half-width of the enlarged index range per axis, nr(2, :) (the range
+    is symmetric, -nr..nr).  For meshes built here it is the largest |coordinate|
+    over inner and boundary points, which is the reference's enlarged range
+    (src/grid/mesh_init.F90:216-218) for sphere and parallelepiped boxes."""
+    return np.max(np.abs(np.asarray(mesh.lxyz, dtype=np.int64)), axis=0)
+
+
+def cubic_index(lxyz, extent) -> np.ndarray:
+    """Spatial index of IDX_CUBIC (the default MeshIndexType,
+    src/grid/mesh_init.F90:232): sum_d (x_d + offset_d) * stride_d with
+    offset = grid size // 2 (:234-235) and strides 1, G1, G1*G2 over the
+    enlarged grid sizes G = 2 * extent + 1 (:172-175;
+    index_point_to_cubic, src/grid/index.F90:313-329)."""
+    L = np.asarray(lxyz, dtype=np.int64)
+    G = 2 * np.asarray(extent, dtype=np.int64) + 1
+    off = G // 2
+    if np.any(np.abs(L) > np.asarray(extent)[None, :]):
+        raise ValueError("cubic_index: a point lies outside the index range")
+    stride = np.array([1, G[0], G[0] * G[1]], dtype=np.int64)
+    return ((L + off[None, :]) * stride[None, :]).sum(axis=1)
+
+
+def cubic_point(index, extent) -> np.ndarray:
+    """Inverse of ``cubic_index`` (index_cubic_to_point,
+    src/grid/index.F90:295-311): (n, 3) int32 coordinates."""
+    t = np.asarray(index, dtype=np.int64).copy()
+    G = 2 * np.asarray(extent, dtype=np.int64) + 1
+    off = G // 2
+    stride = np.array([1, G[0], G[0] * G[1]], dtype=np.int64)
+    out = np.empty((t.shape[0], 3), dtype=np.int64)
+    for d in (2, 1):
+        out[:, d] = t // stride[d] - off[d]
+        t = t % stride[d]
+    out[:, 0] = t - off[0]
+    return out.astype(np.int32)
+
+
+def write_indices_obf(path, mesh: Mesh, extent=None) -> None:
+    """Write the mesh order as the reference's restart file indices.obf
+    (index_dump, src/grid/index.F90:176-200): the io_binary header
+    (src/basic/io_binary.c:112-150: "pulpo", version 0, the value one in four
+    formats for the endianness check, np, type) and the np_part spatial
+    indices as int64, in mesh order."""
+    idx = cubic_index(mesh.lxyz, cubic_extent(mesh) if extent is None else extent)
+    h = np.zeros((), dtype=_OBF_HEADER)
+    h["text"] = b"pulpo"
+    h["one_32"], h["one_f"], h["one_64"], h["one_d"] = 1, 1.0, 1, 1.0
+    h["np"] = idx.shape[0]
+    h["type"] = IO_TYPE_INT_64
+    with open(path, "wb") as f:
+        f.write(h.tobytes())
+        f.write(idx.astype("<i8").tobytes())
+
+
+def read_indices_obf(path) -> np.ndarray:
+    """Spatial indices of an indices.obf file (index_load,
+    src/grid/index.F90:204-257, through io_binary_read): checks the header
+    as check_header does (src/basic/io_binary.c:152-192: text, version,
+    endianness from the stored one) and converts byte-swapped files; int32
+    and int64 payloads are accepted."""
+    raw = open(path, "rb").read()
+    if len(raw) < 64:
+        raise ValueError("indices.obf: file shorter than its header")
+    h = np.frombuffer(raw[:64], dtype=_OBF_HEADER)[0]
+    if bytes(h["text"]).rstrip(b"\0") != b"pulpo" or int(h["version"]) != 0:
+        raise ValueError("indices.obf: not an io_binary file (text or version)")
+    if int(h["one_32"]) == 1:
+        end = "<"
+    elif int(h["one_32"]) == 1 << 24:
+        end = ">"
+        h = np.frombuffer(raw[:64], dtype=_OBF_HEADER.newbyteorder(">"))[0]
+    else:
+        raise ValueError("indices.obf: unknown byte order")
+    n, typ = int(h["np"]), int(h["type"])
+    size = {IO_TYPE_INT_32: 4, IO_TYPE_INT_64: 8}.get(typ)
+    if size is None:
+        raise ValueError(f"indices.obf: payload type {typ} is not an integer type")
+    if len(raw) < 64 + n * size:
+        raise ValueError("indices.obf: file shorter than its np entries")
+    return np.frombuffer(raw[64: 64 + n * size], dtype=f"{end}i{size}").astype(np.int64)
+
+
+def mesh_from_indices_obf(path, np_inner: int, spacing, extent) -> Mesh:
+    """Mesh point list in the order a reference run stored: the first
+    ``np_inner`` entries are the inner points, the rest the boundary points
+    (mesh%np_global of the same run)."""
+    idx = read_indices_obf(path)
+    if not 0 < np_inner <= idx.shape[0]:
+        raise ValueError("mesh_from_indices_obf: np_inner outside 1..np_part")
+    return Mesh(lxyz=cubic_point(idx, extent), np=int(np_inner),
+                spacing=np.asarray(spacing, dtype=np.float64) * np.ones(3), label=str(path))

@@ -1,0 +1,48 @@
+"""Generate the indices.obf golden file with the reference's own binary I/O.
+
+Run in a container where the reference sources are present:
+
+    make -C oracle ref && python tests/golden/make_indices_obf.py
+
+It loads oracle/_ref/libref_io_binary.so (the reference's
+src/basic/io_binary.c built from source) and writes, through its
+``write_binary`` (header + payload, as index_dump does,
+src/grid/index.F90:176-200), the cubic spatial indices of the points of a
+small sphere mesh (R = 1.5, h = 0.3, order 4) in mesh order.  The tests
+compare this library's writer and reader against the file on machines
+without the reference.
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "octopus-debian-package_b200"))
+
+from hpsi.mesh import IO_TYPE_INT_64, cubic_extent, cubic_index, sphere_mesh  # noqa: E402
+
+OUT = os.path.join(HERE, "indices_sphere_r1.5_h0.3.obf")
+
+
+def reference_write(path, values):
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_io_binary.so"))
+    v = np.ascontiguousarray(values, dtype=np.int64)
+    n = C.c_int64(v.shape[0])
+    typ, ierr, iio, nhd, flpe = C.c_int(IO_TYPE_INT_64), C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+    lib.write_binary(C.byref(n), v.ctypes.data_as(C.c_void_p), C.byref(typ), C.byref(ierr), C.byref(iio),
+                     C.byref(nhd), C.byref(flpe), C.c_char_p(os.fsencode(path)))
+    if ierr.value != 0:
+        raise RuntimeError(f"write_binary failed: {ierr.value}")
+
+
+def main():
+    m = sphere_mesh(1.5, 0.3)
+    reference_write(OUT, cubic_index(m.lxyz, cubic_extent(m)))
+    print(OUT, m.np, m.np_part, cubic_extent(m))
+
+
+if __name__ == "__main__":
+    main()

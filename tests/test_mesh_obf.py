@@ -1,0 +1,93 @@
+"""The mesh order on disk (the reference's restart file indices.obf): cubic
+spatial indices, the io_binary header, and parity with the reference's own
+binary I/O (a golden file it wrote, and, where oracle/_ref holds the
+reference's io_binary.c built from source, its reader on our file)."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden", "indices_sphere_r1.5_h0.3.obf")
+REF_IO = os.path.join(ROOT, "oracle", "_ref", "libref_io_binary.so")
+
+
+def _meshes():
+    from hpsi.mesh import index_box_mesh, parallelepiped_mesh, sphere_mesh
+    return [sphere_mesh(1.5, 0.3), sphere_mesh(3.0, 0.25), parallelepiped_mesh([1.0, 1.5, 0.75], 0.25),
+            index_box_mesh((6, 5, 4), 0.3)]
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_cubic_index_round_trip(k):
+    from hpsi.mesh import cubic_extent, cubic_index, cubic_point
+    m = _meshes()[k]
+    e = cubic_extent(m)
+    idx = cubic_index(m.lxyz, e)
+    assert np.unique(idx).shape[0] == m.np_part
+    assert idx.min() >= 0 and idx.max() < np.prod(2 * e + 1)
+    assert np.array_equal(cubic_point(idx, e), m.lxyz)
+    with pytest.raises(ValueError):
+        cubic_index(m.lxyz, e - 1)
+
+
+def test_writer_is_byte_identical_to_the_reference_file(tmp_path):
+    from hpsi.mesh import sphere_mesh, write_indices_obf
+    p = tmp_path / "indices.obf"
+    write_indices_obf(p, sphere_mesh(1.5, 0.3))
+    assert p.read_bytes() == open(GOLDEN, "rb").read()
+
+
+def test_reader_recovers_the_mesh_from_the_reference_file():
+    from hpsi.mesh import mesh_from_indices_obf, read_indices_obf, sphere_mesh
+    m = sphere_mesh(1.5, 0.3)
+    assert read_indices_obf(GOLDEN).shape == (m.np_part,)
+    m2 = mesh_from_indices_obf(GOLDEN, m.np, m.spacing, [9, 9, 9])
+    assert m2.np == m.np and np.array_equal(m2.lxyz, m.lxyz)
+
+
+def test_reader_converts_big_endian_files(tmp_path):
+    from hpsi.mesh import _OBF_HEADER, read_indices_obf
+    raw = open(GOLDEN, "rb").read()
+    h = np.frombuffer(raw[:64], dtype=_OBF_HEADER).astype(_OBF_HEADER.newbyteorder(">"))
+    n = int(h["np"][0])
+    vals = np.frombuffer(raw[64:], dtype="<i8").astype(">i8")
+    p = tmp_path / "be.obf"
+    p.write_bytes(h.tobytes() + vals.tobytes())
+    assert np.array_equal(read_indices_obf(p), read_indices_obf(GOLDEN))
+    assert read_indices_obf(p).shape == (n,)
+
+
+def test_reader_rejects_bad_files(tmp_path):
+    from hpsi.mesh import read_indices_obf
+    raw = bytearray(open(GOLDEN, "rb").read())
+    cases = {"short": bytes(raw[:40]), "text": b"pulpX" + bytes(raw[5:]),
+             "truncated": bytes(raw[:64 + 8 * 10])}
+    bad_type = bytearray(raw)
+    bad_type[40:44] = (3).to_bytes(4, "little")   # TYPE_DOUBLE_COMPLEX payload
+    cases["type"] = bytes(bad_type)
+    for name, data in cases.items():
+        p = tmp_path / f"{name}.obf"
+        p.write_bytes(data)
+        with pytest.raises(ValueError):
+            read_indices_obf(p)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_IO), reason="reference io_binary.c not built (make -C oracle ref)")
+def test_reference_reader_reads_our_file(tmp_path):
+    from hpsi.mesh import IO_TYPE_INT_64, cubic_extent, cubic_index, sphere_mesh, write_indices_obf
+    lib = C.CDLL(REF_IO)
+    m = sphere_mesh(3.0, 0.25)
+    p = tmp_path / "indices.obf"
+    write_indices_obf(p, m)
+    fname = C.c_char_p(os.fsencode(str(p)))
+    n, typ, size, ierr, iio = C.c_int64(0), C.c_int(0), C.c_int64(0), C.c_int(0), C.c_int(0)
+    lib.get_info_binary(C.byref(n), C.byref(typ), C.byref(size), C.byref(ierr), C.byref(iio), fname)
+    assert ierr.value == 0 and n.value == m.np_part and typ.value == IO_TYPE_INT_64
+    out = np.zeros(m.np_part, dtype=np.int64)
+    off, otyp = C.c_int64(0), C.c_int(IO_TYPE_INT_64)
+    lib.read_binary(C.byref(n), C.byref(off), out.ctypes.data_as(C.c_void_p), C.byref(otyp), C.byref(ierr),
+                    C.byref(iio), fname)
+    assert ierr.value == 0
+    assert np.array_equal(out, cubic_index(m.lxyz, cubic_extent(m)))
