@@ -254,13 +254,117 @@ def cubic_point(index, extent) -> np.ndarray:
     return out.astype(np.int32)
 
 
-def write_indices_obf(path, mesh: Mesh, extent=None) -> None:
+def hilbert_bits(extent) -> int:
+    """Bits per axis of the Hilbert index, idx%bits = max over axes of
+    ceil(log2(grid size)) (src/grid/mesh_init.F90:242-243), in integer
+    arithmetic (grid sizes 2 * extent + 1 are odd, never a power of two)."""
+    G = 2 * np.asarray(extent, dtype=np.int64) + 1
+    return int(max(int(g - 1).bit_length() for g in G))
+
+
+def _hilbert_pack(X, bits):
+    # bit b of axis d goes to bit b * 3 + (2 - d) of the index (the bit order of
+    # TransposetoInt, src/grid/hilbert.c:94-108)
+    h = np.zeros(X.shape[0], dtype=np.int64)
+    for b in range(bits):
+        for d in range(3):
+            h |= ((X[:, d] >> b) & 1) << (b * 3 + 2 - d)
+    return h
+
+
+def _hilbert_unpack(h, bits):
+    X = np.zeros((h.shape[0], 3), dtype=np.int64)
+    for b in range(bits):
+        for d in range(3):
+            X[:, d] |= ((h >> (b * 3 + 2 - d)) & 1) << b
+    return X
+
+
+def hilbert_index(lxyz, extent) -> np.ndarray:
+    """Spatial index of IDX_HILBERT (MeshIndexType = idx_hilbert,
+    index_point_to_hilbert, src/grid/index.F90:343-354): the point shifted by
+    the offset, then J. Skilling's axes -> transposed Hilbert index
+    ("Programming the Hilbert curve", AIP Conf. Proc. 707, 381 (2004)), the
+    algorithm src/grid/hilbert.c uses, vectorised over points."""
+    L = np.asarray(lxyz, dtype=np.int64)
+    e = np.asarray(extent, dtype=np.int64)
+    if np.any(np.abs(L) > e[None, :]):
+        raise ValueError("hilbert_index: a point lies outside the index range")
+    bits = hilbert_bits(e)
+    X = L + ((2 * e + 1) // 2)[None, :]
+    # undo the rotations and reflections, from the top bit down
+    q = 1 << (bits - 1)
+    while q > 1:
+        p = q - 1
+        for d in range(3):
+            hit = (X[:, d] & q) != 0
+            X[hit, 0] ^= p
+            t = np.where(hit, 0, (X[:, 0] ^ X[:, d]) & p)
+            X[:, 0] ^= t
+            X[:, d] ^= t
+        q >>= 1
+    # Gray encode
+    for d in (1, 2):
+        X[:, d] ^= X[:, d - 1]
+    t = np.zeros(X.shape[0], dtype=np.int64)
+    q = 1 << (bits - 1)
+    while q > 1:
+        t ^= np.where((X[:, 2] & q) != 0, q - 1, 0)
+        q >>= 1
+    X ^= t[:, None]
+    return _hilbert_pack(X, bits)
+
+
+def hilbert_point(index, extent) -> np.ndarray:
+    """Inverse of ``hilbert_index`` (index_hilbert_to_point,
+    src/grid/index.F90:332-341): (n, 3) int32 coordinates."""
+    e = np.asarray(extent, dtype=np.int64)
+    bits = hilbert_bits(e)
+    X = _hilbert_unpack(np.asarray(index, dtype=np.int64), bits)
+    # Gray decode
+    t = X[:, 2] >> 1
+    for d in (2, 1):
+        X[:, d] ^= X[:, d - 1]
+    X[:, 0] ^= t
+    # redo the rotations and reflections, from the bottom bit up
+    q = 2
+    while q != (2 << (bits - 1)):
+        p = q - 1
+        for d in (2, 1, 0):
+            hit = (X[:, d] & q) != 0
+            X[hit, 0] ^= p
+            t = np.where(hit, 0, (X[:, 0] ^ X[:, d]) & p)
+            X[:, 0] ^= t
+            X[:, d] ^= t
+        q <<= 1
+    return (X - ((2 * e + 1) // 2)[None, :]).astype(np.int32)
+
+
+def spatial_index(lxyz, extent, index_type: str = "cubic") -> np.ndarray:
+    """Spatial index of the points for MeshIndexType idx_cubic (the default)
+    or idx_hilbert."""
+    if index_type == "cubic":
+        return cubic_index(lxyz, extent)
+    if index_type == "hilbert":
+        return hilbert_index(lxyz, extent)
+    raise ValueError(f"unknown index type {index_type!r}")
+
+
+def spatial_point(index, extent, index_type: str = "cubic") -> np.ndarray:
+    if index_type == "cubic":
+        return cubic_point(index, extent)
+    if index_type == "hilbert":
+        return hilbert_point(index, extent)
+    raise ValueError(f"unknown index type {index_type!r}")
+
+
+def write_indices_obf(path, mesh: Mesh, extent=None, index_type: str = "cubic") -> None:
     """Write the mesh order as the reference's restart file indices.obf
     (index_dump, src/grid/index.F90:176-200): the io_binary header
     (src/basic/io_binary.c:112-150: "pulpo", version 0, the value one in four
     formats for the endianness check, np, type) and the np_part spatial
     indices as int64, in mesh order."""
-    idx = cubic_index(mesh.lxyz, cubic_extent(mesh) if extent is None else extent)
+    idx = spatial_index(mesh.lxyz, cubic_extent(mesh) if extent is None else extent, index_type)
     h = np.zeros((), dtype=_OBF_HEADER)
     h["text"] = b"pulpo"
     h["one_32"], h["one_f"], h["one_64"], h["one_d"] = 1, 1.0, 1, 1.0
@@ -299,12 +403,12 @@ def read_indices_obf(path) -> np.ndarray:
     return np.frombuffer(raw[64: 64 + n * size], dtype=f"{end}i{size}").astype(np.int64)
 
 
-def mesh_from_indices_obf(path, np_inner: int, spacing, extent) -> Mesh:
+def mesh_from_indices_obf(path, np_inner: int, spacing, extent, index_type: str = "cubic") -> Mesh:
     """Mesh point list in the order a reference run stored: the first
     ``np_inner`` entries are the inner points, the rest the boundary points
     (mesh%np_global of the same run)."""
     idx = read_indices_obf(path)
     if not 0 < np_inner <= idx.shape[0]:
         raise ValueError("mesh_from_indices_obf: np_inner outside 1..np_part")
-    return Mesh(lxyz=cubic_point(idx, extent), np=int(np_inner),
+    return Mesh(lxyz=spatial_point(idx, extent, index_type), np=int(np_inner),
                 spacing=np.asarray(spacing, dtype=np.float64) * np.ones(3), label=str(path))

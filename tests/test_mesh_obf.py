@@ -91,3 +91,57 @@ def test_reference_reader_reads_our_file(tmp_path):
                     C.byref(iio), fname)
     assert ierr.value == 0
     assert np.array_equal(out, cubic_index(m.lxyz, cubic_extent(m)))
+
+
+GOLDEN_HILBERT = os.path.join(ROOT, "tests", "golden", "indices_hilbert_sphere_r1.5_h0.3.obf")
+REF_HILBERT = os.path.join(ROOT, "oracle", "_ref", "libref_hilbert.so")
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_hilbert_index_round_trip(k):
+    from hpsi.mesh import cubic_extent, hilbert_bits, hilbert_index, hilbert_point
+    m = _meshes()[k]
+    e = cubic_extent(m)
+    idx = hilbert_index(m.lxyz, e)
+    assert np.unique(idx).shape[0] == m.np_part
+    assert idx.min() >= 0 and idx.max() < 1 << (3 * hilbert_bits(e))
+    assert np.array_equal(hilbert_point(idx, e), m.lxyz)
+
+
+def test_hilbert_curve_is_continuous():
+    """Consecutive Hilbert indices are neighbouring grid points."""
+    from hpsi.mesh import hilbert_point
+    e = np.array([3, 3, 3])  # grid 7^3 inside the 8^3 curve
+    pts = hilbert_point(np.arange(8 ** 3), e).astype(np.int64)
+    assert np.all(np.abs(np.diff(pts, axis=0)).sum(axis=1) == 1)
+
+
+def test_hilbert_file_matches_the_reference_golden(tmp_path):
+    from hpsi.mesh import mesh_from_indices_obf, sphere_mesh, write_indices_obf
+    m = sphere_mesh(1.5, 0.3)
+    p = tmp_path / "h.obf"
+    write_indices_obf(p, m, index_type="hilbert")
+    assert p.read_bytes() == open(GOLDEN_HILBERT, "rb").read()
+    m2 = mesh_from_indices_obf(GOLDEN_HILBERT, m.np, m.spacing, [9, 9, 9], index_type="hilbert")
+    assert np.array_equal(m2.lxyz, m.lxyz)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_HILBERT), reason="reference hilbert.c not built (make -C oracle ref)")
+def test_hilbert_matches_the_reference_kernel():
+    from hpsi.mesh import hilbert_bits, hilbert_index, hilbert_point
+    lib = C.CDLL(REF_HILBERT)
+    rng = np.random.default_rng(5)
+    for e in ([9, 9, 9], [12, 7, 20], [30, 30, 30]):
+        e = np.asarray(e)
+        pts = rng.integers(-e, e + 1, size=(400, 3))
+        ours = hilbert_index(pts, e)
+        dim, nb, idx = C.c_int(3), C.c_int(hilbert_bits(e)), C.c_longlong(0)
+        off = (2 * e + 1) // 2
+        for p, h in zip(pts + off, ours):
+            pt = (C.c_int * 3)(*[int(v) for v in p])
+            lib.hilbert_point_to_index_(C.byref(dim), C.byref(nb), C.byref(idx), pt)
+            assert idx.value == h
+            back = (C.c_int * 3)()
+            lib.hilbert_index_to_point_(C.byref(dim), C.byref(nb), C.byref(C.c_longlong(int(h))), back)
+            assert list(back) == [int(v) for v in p]
+        assert np.array_equal(hilbert_point(ours, e), pts)
