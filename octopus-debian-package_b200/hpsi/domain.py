@@ -198,7 +198,9 @@ def ghost_update(dom: Domain, psi, nst=None, group=None, pack=None, unpack=None,
         sendbuf = torch.empty((nsend, nst), dtype=psi.dtype, device=dev)
     if nsend:
         pack(psi, sendmap, sendbuf, nst=nst)
-        if dev.type == "cuda":
+        # NCCL orders its sends after the work already queued on the current
+        # stream (the pack); other backends read the buffer from the host side
+        if dev.type == "cuda" and dist.get_backend(group) != "nccl":
             torch.cuda.current_stream(dev).synchronize()
     direct = ld == nst
     if not direct and recvbuf is None:
