@@ -357,8 +357,8 @@ hpsi_status hpsi_ghost_unpack(const void *recvbuf, const int32_t *pos,
  * numbers of psi's dtype (row stride psi->ld).  A matrix with no points here
  * gives zero rows, so every partition's rows line up for the sum.
  * hpsi_projector_ket: hpsi[map[k]][s] += a * sum_r P[k][r] * proj[r][s]
- * (a = a_re + i a_im; 1 for H psi) for s < hpsi->nst, proj laid out as the bra writes it with row stride
- * hpsi->ld.  hpsi_apply_h without HPSI_TERM_NON_LOCAL_POTENTIAL followed by
+ * (a = a_re + i a_im; 1 for H psi) for s < hpsi->nst, proj laid out as
+ * the bra writes it, with row stride hpsi->ld.  hpsi_apply_h without HPSI_TERM_NON_LOCAL_POTENTIAL followed by
  * the bra, the sum and the ket equals hpsi_apply_h with every term.
  * Batches and proj on the device; stream ordered, no synchronisation. */
 hpsi_status hpsi_projector_count(const hpsi_hamiltonian *ham,
