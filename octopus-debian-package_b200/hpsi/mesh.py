@@ -208,12 +208,9 @@ def permuted(mesh: Mesh, seed: int = 0) -> tuple[Mesh, np.ndarray, np.ndarray]:
 # ---------------------------------------------------------------------------
 # Mesh order on disk: the restart file indices.obf
 
-IO_TYPE_INT_32 = 4   # TYPE_INT_32 of src/basic/io_binary.h:39
-IO_TYPE_INT_64 = 5   # TYPE_INT_64 of src/basic/io_binary.h:40
-_OBF_HEADER = np.dtype([("text", "S7"), ("version", "u1"), ("one_32", "<u4"), ("one_f", "<f4"),
-                        ("one_64", "<u8"), ("one_d", "<f8"), ("np", "<u8"), ("type", "<u4"),
-                        ("extra", "<u4", (5,))])
-assert _OBF_HEADER.itemsize == 64
+from .obf import TYPE_INT_32 as IO_TYPE_INT_32  # noqa: E402,F401
+from .obf import TYPE_INT_64 as IO_TYPE_INT_64  # noqa: E402,F401
+from .obf import write_obf  # noqa: E402
 
 
 def cubic_extent(mesh: Mesh) -> np.ndarray:
@@ -365,42 +362,19 @@ def write_indices_obf(path, mesh: Mesh, extent=None, index_type: str = "cubic") 
     formats for the endianness check, np, type) and the np_part spatial
     indices as int64, in mesh order."""
     idx = spatial_index(mesh.lxyz, cubic_extent(mesh) if extent is None else extent, index_type)
-    h = np.zeros((), dtype=_OBF_HEADER)
-    h["text"] = b"pulpo"
-    h["one_32"], h["one_f"], h["one_64"], h["one_d"] = 1, 1.0, 1, 1.0
-    h["np"] = idx.shape[0]
-    h["type"] = IO_TYPE_INT_64
-    with open(path, "wb") as f:
-        f.write(h.tobytes())
-        f.write(idx.astype("<i8").tobytes())
+    write_obf(path, idx.astype(np.int64))
 
 
 def read_indices_obf(path) -> np.ndarray:
     """Spatial indices of an indices.obf file (index_load,
-    src/grid/index.F90:204-257, through io_binary_read): checks the header
-    as check_header does (src/basic/io_binary.c:152-192: text, version,
-    endianness from the stored one) and converts byte-swapped files; int32
-    and int64 payloads are accepted."""
-    raw = open(path, "rb").read()
-    if len(raw) < 64:
-        raise ValueError("indices.obf: file shorter than its header")
-    h = np.frombuffer(raw[:64], dtype=_OBF_HEADER)[0]
-    if bytes(h["text"]).rstrip(b"\0") != b"pulpo" or int(h["version"]) != 0:
-        raise ValueError("indices.obf: not an io_binary file (text or version)")
-    if int(h["one_32"]) == 1:
-        end = "<"
-    elif int(h["one_32"]) == 1 << 24:
-        end = ">"
-        h = np.frombuffer(raw[:64], dtype=_OBF_HEADER.newbyteorder(">"))[0]
-    else:
-        raise ValueError("indices.obf: unknown byte order")
-    n, typ = int(h["np"]), int(h["type"])
-    size = {IO_TYPE_INT_32: 4, IO_TYPE_INT_64: 8}.get(typ)
-    if size is None:
-        raise ValueError(f"indices.obf: payload type {typ} is not an integer type")
-    if len(raw) < 64 + n * size:
-        raise ValueError("indices.obf: file shorter than its np entries")
-    return np.frombuffer(raw[64: 64 + n * size], dtype=f"{end}i{size}").astype(np.int64)
+    src/grid/index.F90:204-257, through io_binary_read; header checks and
+    byte order in ``hpsi.obf.read_obf``); int32 and int64 payloads are
+    accepted."""
+    from .obf import read_obf
+    v = read_obf(path)
+    if v.dtype.kind != "i":
+        raise ValueError(f"indices.obf: payload type {v.dtype} is not an integer type")
+    return v.astype(np.int64)
 
 
 def mesh_from_indices_obf(path, np_inner: int, spacing, extent, index_type: str = "cubic") -> Mesh:

@@ -48,7 +48,8 @@ def test_reader_recovers_the_mesh_from_the_reference_file():
 
 
 def test_reader_converts_big_endian_files(tmp_path):
-    from hpsi.mesh import _OBF_HEADER, read_indices_obf
+    from hpsi.mesh import read_indices_obf
+    from hpsi.obf import HEADER as _OBF_HEADER
     raw = open(GOLDEN, "rb").read()
     h = np.frombuffer(raw[:64], dtype=_OBF_HEADER).astype(_OBF_HEADER.newbyteorder(">"))
     n = int(h["np"][0])
@@ -145,3 +146,70 @@ def test_hilbert_matches_the_reference_kernel():
             lib.hilbert_index_to_point_(C.byref(dim), C.byref(nb), C.byref(C.c_longlong(int(h))), back)
             assert list(back) == [int(v) for v in p]
         assert np.array_equal(hilbert_point(ours, e), pts)
+
+
+@pytest.mark.parametrize("dt", ["f4", "f8", "c8", "c16", "i4", "i8"])
+def test_obf_round_trip_every_type(tmp_path, dt):
+    from hpsi.obf import read_obf, write_obf
+    rng = np.random.default_rng(3)
+    v = (rng.standard_normal(37) * 100).astype(dt) if dt[0] in "fi" else \
+        (rng.standard_normal(37) + 1j * rng.standard_normal(37)).astype(dt)
+    p = tmp_path / "v.obf"
+    write_obf(p, v)
+    got = read_obf(p)
+    assert got.dtype == np.dtype(dt) and np.array_equal(got, v)
+    with pytest.raises(ValueError):
+        write_obf(tmp_path / "e.obf", v[:0])
+
+
+@pytest.mark.skipif(not os.path.exists(REF_IO), reason="reference io_binary.c not built (make -C oracle ref)")
+def test_state_files_both_ways_with_the_reference(tmp_path):
+    """Complex and real mesh functions: files the reference's write_binary
+    makes load into a batch (real ones widened as its read_binary converts
+    them), and the reference's read_binary reads write_obf's files."""
+    from hpsi.mesh import sphere_mesh
+    from hpsi.obf import TYPE_DOUBLE, TYPE_DOUBLE_COMPLEX, load_states_obf, write_obf
+    lib = C.CDLL(REF_IO)
+    m = sphere_mesh(1.5, 0.3)
+    rng = np.random.default_rng(7)
+    states = [rng.standard_normal(m.np) + 1j * rng.standard_normal(m.np) for _ in range(2)]
+    states.append(rng.standard_normal(m.np))          # a real state (gs restart of a real run)
+    paths = []
+    for i, s in enumerate(states):
+        p = tmp_path / f"{i + 1:010d}.obf"
+        v = np.ascontiguousarray(s)
+        n = C.c_int64(m.np)
+        typ = C.c_int(TYPE_DOUBLE_COMPLEX if np.iscomplexobj(v) else TYPE_DOUBLE)
+        ierr, iio, nhd, flpe = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        lib.write_binary(C.byref(n), v.ctypes.data_as(C.c_void_p), C.byref(typ), C.byref(ierr), C.byref(iio),
+                         C.byref(nhd), C.byref(flpe), C.c_char_p(os.fsencode(str(p))))
+        assert ierr.value == 0
+        paths.append(p)
+    b = load_states_obf(paths, m, ld=4)
+    assert b.shape == (m.np_part, 4) and not b[m.np:].any() and not b[:, 3].any()
+    for i, s in enumerate(states):
+        assert np.array_equal(b[: m.np, i], s.astype(np.complex128))
+    # the reference's reader, asked for complex output, on the real file and on write_obf's file
+    for src in (paths[2], tmp_path / "ours.obf"):
+        if src == tmp_path / "ours.obf":
+            write_obf(src, states[0])
+        out = np.zeros(m.np, dtype=np.complex128)
+        n, off, otyp = C.c_int64(m.np), C.c_int64(0), C.c_int(TYPE_DOUBLE_COMPLEX)
+        ierr, iio = C.c_int(0), C.c_int(0)
+        lib.read_binary(C.byref(n), C.byref(off), out.ctypes.data_as(C.c_void_p), C.byref(otyp), C.byref(ierr),
+                        C.byref(iio), C.c_char_p(os.fsencode(str(src))))
+        want = states[2].astype(np.complex128) if src == paths[2] else states[0]
+        assert np.array_equal(out, want), ierr.value
+
+
+def test_load_states_rejects_wrong_sizes(tmp_path):
+    from hpsi.mesh import sphere_mesh
+    from hpsi.obf import load_states_obf, write_obf
+    m = sphere_mesh(1.5, 0.3)
+    write_obf(tmp_path / "a.obf", np.zeros(m.np + 1, dtype=np.complex128))
+    write_obf(tmp_path / "i.obf", np.zeros(m.np, dtype=np.int64))
+    for name in ("a.obf", "i.obf"):
+        with pytest.raises(ValueError):
+            load_states_obf([tmp_path / name], m)
+    with pytest.raises(ValueError):
+        load_states_obf([tmp_path / "a.obf"] * 2, m, ld=1)
