@@ -95,3 +95,23 @@ def load_states_obf(paths, mesh, ld=None, dtype=np.complex128) -> np.ndarray:
             raise ValueError(f"{p}: holds {v.shape[0]} points, the mesh has {mesh.np} inner points")
         out[: mesh.np, i] = v
     return out
+
+
+def save_states_obf(batch, mesh, paths) -> None:
+    """One .obf file per state from a packed (npts, ld) batch (numpy or a
+    torch tensor, device tensors copied to the host): column i, inner rows
+    only, as the reference writes a state for a restart
+    (X(restart_write_mesh_function), src/grid/restart_inc.F90:21-97), so a
+    reference run can continue from states this library propagated."""
+    paths = list(paths)
+    try:
+        import torch
+        if isinstance(batch, torch.Tensor):
+            batch = batch.detach().cpu().numpy()
+    except ImportError:  # pragma: no cover
+        pass
+    b = np.asarray(batch)
+    if b.ndim != 2 or b.shape[0] < mesh.np or b.shape[1] < len(paths):
+        raise ValueError("save_states_obf: batch must be (>= np, >= number of files)")
+    for i, p in enumerate(paths):
+        write_obf(p, np.ascontiguousarray(b[: mesh.np, i]))

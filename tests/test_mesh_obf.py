@@ -213,3 +213,20 @@ def test_load_states_rejects_wrong_sizes(tmp_path):
             load_states_obf([tmp_path / name], m)
     with pytest.raises(ValueError):
         load_states_obf([tmp_path / "a.obf"] * 2, m, ld=1)
+
+
+def test_save_and_load_states_round_trip(tmp_path):
+    import torch
+    from hpsi.mesh import sphere_mesh
+    from hpsi.obf import load_states_obf, read_obf, save_states_obf
+    m = sphere_mesh(1.5, 0.3)
+    rng = np.random.default_rng(11)
+    b = np.zeros((m.np_part, 4), dtype=np.complex64)
+    b[: m.np, :3] = rng.standard_normal((m.np, 3)) + 1j * rng.standard_normal((m.np, 3))
+    paths = [tmp_path / f"{i + 1:010d}.obf" for i in range(3)]
+    save_states_obf(torch.from_numpy(b), m, paths)
+    assert read_obf(paths[0]).dtype == np.complex64
+    got = load_states_obf(paths, m, ld=4, dtype=np.complex64)
+    assert np.array_equal(got, b)
+    with pytest.raises(ValueError):
+        save_states_obf(b[:, :2], m, paths)
