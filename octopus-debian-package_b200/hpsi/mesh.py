@@ -386,3 +386,78 @@ def mesh_from_indices_obf(path, np_inner: int, spacing, extent, index_type: str 
         raise ValueError("mesh_from_indices_obf: np_inner outside 1..np_part")
     return Mesh(lxyz=spatial_point(idx, extent, index_type), np=int(np_inner),
                 spacing=np.asarray(spacing, dtype=np.float64) * np.ones(3), label=str(path))
+
+
+def index_checksum(indices) -> int:
+    """mesh%idx%checksum: sum over points of (position, 1-based) x spatial
+    index in wrapping 64-bit arithmetic (checksum_calculate,
+    src/math/checksum.c:30-41, called at src/grid/mesh_init.F90:446)."""
+    v = np.asarray(indices, dtype=np.int64).astype(np.uint64)
+    k = np.arange(1, v.shape[0] + 1, dtype=np.uint64)
+    s = int(np.sum(k * v, dtype=np.uint64))
+    return s - (1 << 64) if s >= 1 << 63 else s
+
+
+_INDEX_TYPES = {"cubic": 1, "hilbert": 2}   # IDX_CUBIC, IDX_HILBERT (src/grid/index.F90:66-67)
+
+
+def write_grid_fingerprint(path, mesh: Mesh, index_type: str = "cubic", extent=None) -> None:
+    """The restart file "grid" (mesh_write_fingerprint,
+    src/grid/mesh.F90:315-352): np_part_global, np_global, algorithm,
+    checksum, bits, dim, type, then offset(i) and nn(i) per axis, each a
+    20-character label and a 21-wide integer."""
+    e = np.asarray(cubic_extent(mesh) if extent is None else extent, dtype=np.int64)
+    G = 2 * e + 1
+    idx = spatial_index(mesh.lxyz, e, index_type)
+    lines = [("np_part_global=", mesh.np_part), ("np_global=", mesh.np), ("algorithm=", 1),
+             ("checksum=", index_checksum(idx)), ("bits=", hilbert_bits(e)), ("dim=", 3),
+             ("type=", _INDEX_TYPES[index_type])]
+    out = [f"{a:<20s}{b:21d}" for a, b in lines]
+    # '(a7,i2,a11,i21)': a label shorter than its A field is right-justified
+    # ("    nn("), a longer one cut to the field (")=" and 9 blanks)
+    out += [f"{'offset(':>7s}{d + 1:2d}{')=':<11s}{int(G[d] // 2):21d}" for d in range(3)]
+    out += [f"{'nn(':>7s}{d + 1:2d}{')=':<11s}{int(G[d]):21d}" for d in range(3)]
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+
+
+def read_grid_fingerprint(path) -> dict:
+    """Fields of a restart "grid" file (mesh_read_fingerprint,
+    src/grid/mesh.F90:361-446): each line read as a 20-character label and
+    an integer."""
+    with open(path) as f:
+        rows = [ln.rstrip("\n") for ln in f if ln.strip()]
+    if len(rows) < 7:
+        raise ValueError(f"{path}: fewer than 7 lines")
+    val = [int(r[20:41]) for r in rows]
+    dim = val[5]
+    if len(rows) < 7 + 2 * dim:
+        raise ValueError(f"{path}: missing offset or nn lines")
+    return {"np_part": val[0], "np": val[1], "algorithm": val[2], "checksum": val[3], "bits": val[4],
+            "dim": dim, "type": val[6], "offset": val[7: 7 + dim], "nn": val[7 + dim: 7 + 2 * dim]}
+
+
+def mesh_from_restart(directory, spacing) -> Mesh:
+    """The mesh of a reference restart directory from its "grid" fingerprint
+    and indices.obf (what mesh_check_dump_compatibility reads,
+    src/grid/mesh.F90:449-533): point order, inner/boundary split and index
+    type from the files, the checksum verified; the spacing is an input of
+    the run, not stored there."""
+    import os
+    fp = read_grid_fingerprint(os.path.join(directory, "grid"))
+    if fp["dim"] != 3:
+        raise ValueError("mesh_from_restart: only 3D meshes")
+    types = {v: k for k, v in _INDEX_TYPES.items()}
+    if fp["type"] not in types:
+        raise ValueError(f"mesh_from_restart: unknown index type {fp['type']}")
+    nn = np.asarray(fp["nn"], dtype=np.int64)
+    if np.any(nn % 2 == 0) or np.any(np.asarray(fp["offset"]) != nn // 2):
+        raise ValueError("mesh_from_restart: only symmetric index ranges (odd nn, offset = nn / 2)")
+    idx = read_indices_obf(os.path.join(directory, "indices.obf"))
+    if idx.shape[0] != fp["np_part"]:
+        raise ValueError("mesh_from_restart: indices.obf and grid disagree on np_part")
+    if index_checksum(idx) != fp["checksum"]:
+        raise ValueError("mesh_from_restart: index checksum mismatch")
+    m = Mesh(lxyz=spatial_point(idx, nn // 2, types[fp["type"]]), np=int(fp["np"]),
+             spacing=np.asarray(spacing, dtype=np.float64) * np.ones(3), label=str(directory))
+    return m

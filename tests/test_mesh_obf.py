@@ -230,3 +230,42 @@ def test_save_and_load_states_round_trip(tmp_path):
     assert np.array_equal(got, b)
     with pytest.raises(ValueError):
         save_states_obf(b[:, :2], m, paths)
+
+
+REF_CK = os.path.join(ROOT, "oracle", "_ref", "libref_checksum.so")
+
+
+@pytest.mark.parametrize("index_type", ["cubic", "hilbert"])
+def test_mesh_from_restart_directory(tmp_path, index_type):
+    """A restart directory as the reference leaves it (the "grid"
+    fingerprint and indices.obf) gives back the mesh; a wrong checksum is
+    refused."""
+    from hpsi.mesh import (mesh_from_restart, read_grid_fingerprint, sphere_mesh, write_grid_fingerprint,
+                           write_indices_obf)
+    m = sphere_mesh(2.0, 0.25)
+    write_indices_obf(tmp_path / "indices.obf", m, index_type=index_type)
+    write_grid_fingerprint(tmp_path / "grid", m, index_type=index_type)
+    lines = (tmp_path / "grid").read_text().splitlines()
+    assert len(lines) == 13 and all(len(ln) == 41 for ln in lines)
+    assert lines[7].startswith("offset( 1)=") and lines[10].startswith("    nn( 1)=")
+    fp = read_grid_fingerprint(tmp_path / "grid")
+    assert fp["np"] == m.np and fp["np_part"] == m.np_part and fp["type"] == (1 if index_type == "cubic" else 2)
+    m2 = mesh_from_restart(tmp_path, m.spacing)
+    assert m2.np == m.np and np.array_equal(m2.lxyz, m.lxyz)
+    bad = lines[:3] + [f"{'checksum=':<20s}{fp['checksum'] + 1:21d}"] + lines[4:]
+    (tmp_path / "grid").write_text("\n".join(bad) + "\n")
+    with pytest.raises(ValueError):
+        mesh_from_restart(tmp_path, m.spacing)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CK), reason="reference checksum.c not built (make -C oracle ref)")
+def test_index_checksum_matches_the_reference():
+    from hpsi.mesh import index_checksum
+    lib = C.CDLL(REF_CK)
+    rng = np.random.default_rng(13)
+    for n in (1, 10, 5000):
+        for hi in (100, 1 << 40, (1 << 62)):   # the last case wraps around 2^64
+            v = rng.integers(0, hi, size=n, dtype=np.int64)
+            alg, nn, s = C.c_int(1), C.c_int64(n), C.c_int64(0)
+            lib.checksum_calculate_(C.byref(alg), C.byref(nn), v.ctypes.data_as(C.c_void_p), C.byref(s))
+            assert index_checksum(v) == s.value
