@@ -2,6 +2,9 @@
 
 ``hpsi.lib`` binds the C ABI of ``libhpsi.so``; ``hpsi.mesh``, ``hpsi.stencil``
 and ``hpsi.fixtures`` are the host-side set-up a caller performs (mesh point
-lists, finite-difference weights, synthetic systems).
+lists, finite-difference weights, synthetic systems); ``hpsi.obf`` reads and
+writes the reference's binary restart files; ``hpsi.domain`` and
+``hpsi.states_parallel`` are the multi-rank layers (domain partitions with
+ghost rows, state blocks).
 """
 from . import mesh, stencil  # noqa: F401
