@@ -136,6 +136,17 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *ham, int32_t nmat,
                                             const double *matrices,
                                             const double *scal);
 
+/* Projector phases for k != 0 (projector_phases, built by
+ * projector_init_phases, src/hamiltonian/projector.F90:171-247, and applied
+ * in src/hamiltonian/hamiltonian_elec_base_inc.F90:680-701 and :934-1025):
+ * one complex number per sphere point, 2*sum(npoints) doubles in the order of
+ * the map passed to hpsi_hamiltonian_set_projectors.  The bra gathers
+ * psi(map) * phase, the ket adds its contribution times conj(phase).  NULL
+ * removes them; setting new projectors removes them too.  With phases the
+ * bra runs on the SIMT kernel (at most 32 projectors per matrix). */
+hpsi_status hpsi_hamiltonian_set_projector_phases(hpsi_hamiltonian *ham,
+                                                  const double *phases);
+
 /* ------------------------------------------------------------------ */
 /* A borrowed state batch (batch_t / wfs_elec_t in packed status). */
 typedef struct {

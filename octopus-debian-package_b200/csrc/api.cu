@@ -513,6 +513,11 @@ void hpsi_hamiltonian::proj_free() {
   dev_free(d_krows);
   dev_free(d_kptr);
   dev_free(d_kb_ent);
+  dev_free(d_kb_phase);
+  dev_free(d_kb_phase_f);
+  d_kb_phase = nullptr;
+  d_kb_phase_f = nullptr;
+  kb_npts = 0;
   d_mat = nullptr;
   d_proj_row = d_map = d_krows = d_kptr = nullptr;
   nk = 0;
@@ -685,7 +690,7 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, c
   for (int i = 0; i < nmat; ++i)
     for (int k = 0; k < npoints[i]; ++k) {
       const int row = map[mat[i].z + k];
-      ent[fill[row]++] = make_int4(mat[i].w + k * nprojs[i], prow[i], nprojs[i], 0);
+      ent[fill[row]++] = make_int4(mat[i].w + k * nprojs[i], prow[i], nprojs[i], mat[i].z + k);
     }
   // compress to the covered rows (entries stay in matrix order per row)
   std::vector<int> krows, kptr(1, 0);
@@ -727,6 +732,35 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, c
   h->max_nproj = maxp;
   h->nk = int(krows.size());
   h->min_npoints = minp;
+  h->kb_npts = npts_tot;
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_hamiltonian_set_projector_phases(hpsi_hamiltonian *h, const double *phases) {
+  if (!h) return HPSI_ERR_ARG;
+  dev_free(h->d_kb_phase);
+  dev_free(h->d_kb_phase_f);
+  h->d_kb_phase = nullptr;
+  h->d_kb_phase_f = nullptr;
+  if (!phases) return HPSI_OK;
+  if (h->nmat == 0) {
+    set_error("hpsi_hamiltonian_set_projector_phases: no projectors set");
+    return HPSI_ERR_STATE;
+  }
+  const size_t n = 2 * size_t(h->kb_npts);
+  std::vector<float> pf(n);
+  for (size_t i = 0; i < n; ++i) {
+    if (!std::isfinite(phases[i])) {
+      set_error("hpsi_hamiltonian_set_projector_phases: non-finite phase");
+      return HPSI_ERR_NONFINITE;
+    }
+    pf[i] = float(phases[i]);
+  }
+  hpsi_status s = dev_alloc(reinterpret_cast<void **>(&h->d_kb_phase), n * sizeof(double));
+  if (!s) s = dev_alloc(reinterpret_cast<void **>(&h->d_kb_phase_f), n * sizeof(float));
+  if (s) return s;
+  HPSI_TRY_CUDA(cudaMemcpy(h->d_kb_phase, phases, n * sizeof(double), cudaMemcpyHostToDevice));
+  HPSI_TRY_CUDA(cudaMemcpy(h->d_kb_phase_f, pf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   return HPSI_OK;
 }
 
@@ -839,6 +873,9 @@ hpsi_status run_bra(hpsi_hamiltonian *h, const T *psi, long long ld, T *proj, cu
   p.proj_ld = ld;
   p.nprojections = h->nprojections;
   p.min_npoints = h->min_npoints;
+  p.phase = h->d_kb_phase ? (sizeof(T) == 8 ? static_cast<const void *>(h->d_kb_phase)
+                                            : static_cast<const void *>(h->d_kb_phase_f))
+                          : nullptr;
   const int ksplit = bra_ksplit(p, h->mesh->num_sms);
   hpsi_status s = h->bra_partial.ensure(size_t(ksplit) * h->nprojections * ld * 2 * sizeof(double));
   if (s) return s;
@@ -868,6 +905,9 @@ hpsi_status run_ket(hpsi_hamiltonian *h, const T *proj, long long ld, int nst, T
   k.psi0_ld = psi0_ld;
   k.obs = obs;
   k.obs_ld = int(ld);
+  k.phase = h->d_kb_phase ? (sizeof(T) == 8 ? static_cast<const void *>(h->d_kb_phase)
+                                            : static_cast<const void *>(h->d_kb_phase_f))
+                          : nullptr;
   ProfScope prof(sizeof(T) == 8 ? "ket_fp64" : "ket_fp32", st);
   return launch_ket<T>(k, st);
 }

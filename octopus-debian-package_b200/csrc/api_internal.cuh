@@ -78,6 +78,10 @@ struct hpsi_hamiltonian {
   int nk = 0, min_npoints = 0;
   int *d_krows = nullptr, *d_kptr = nullptr;
   int4 *d_kb_ent = nullptr;
+  // projector phases (k != 0): one complex number per sphere point, or null
+  long long kb_npts = 0;
+  double *d_kb_phase = nullptr;
+  float *d_kb_phase_f = nullptr;
   bool use_tensor_bra = true;
   // autotuned pass shape per storage type (valid for batches of width ld)
   struct Tuned {

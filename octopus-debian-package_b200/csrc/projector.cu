@@ -133,8 +133,11 @@ __global__ void bra_reduce_kernel(const ProjArgs p, int ksplit) {
   static_cast<T *>(p.proj)[i] = T(acc * p.scal64[j]);
 }
 
-// SIMT bra: grid (nmat, ceil(ld2/32)); block 128 = 32 lanes x 4 point groups
-template <typename T>
+// SIMT bra: grid (nmat, ceil(ld2/32)); block 128 = 32 lanes x 4 point groups.
+// PHASE: each gathered point is first multiplied by its projector phase
+// (lpsi = psi(map) * projector_phases, hamiltonian_elec_base_inc.F90:680-701);
+// lane pairs (2s, 2s + 1) hold one complex number, exchanged by a shuffle.
+template <typename T, bool PHASE>
 __global__ void __launch_bounds__(128) bra_simt_kernel(const ProjArgs p) {
   constexpr int MAXP = 32;
   __shared__ T red[4][MAXP][32];
@@ -150,9 +153,24 @@ __global__ void __launch_bounds__(128) bra_simt_kernel(const ProjArgs p) {
   T acc[MAXP];
 #pragma unroll
   for (int j = 0; j < MAXP; ++j) acc[j] = T(0);
-  if (lane < ld2) {
+  if constexpr (!PHASE) {
+    if (lane < ld2) {
+      for (int k = grp; k < npts; k += 4) {
+        const T x = psi[__ldg(map + k) * ld2 + lane];
+        const T *pk = pt + (long long)k * npr;
+#pragma unroll
+        for (int j = 0; j < MAXP; ++j)
+          if (j < npr) acc[j] += pk[j] * x;
+      }
+    }
+  } else {
+    // every lane of the warp runs the loop (the shuffle needs all 32)
+    const T *ph = static_cast<const T *>(p.phase) + 2 * (long long)md.z;
     for (int k = grp; k < npts; k += 4) {
-      const T x = psi[__ldg(map + k) * ld2 + lane];
+      T x = lane < ld2 ? psi[__ldg(map + k) * ld2 + lane] : T(0);
+      const T other = __shfl_xor_sync(0xffffffffu, x, 1);
+      const T c = ph[2 * k], sn = ph[2 * k + 1];
+      x = (ln & 1) ? other * sn + x * c : x * c - other * sn;
       const T *pk = pt + (long long)k * npr;
 #pragma unroll
       for (int j = 0; j < MAXP; ++j)
@@ -191,6 +209,16 @@ hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStrea
   if (p.nmat == 0) return HPSI_OK;
   const long long ld2 = 2 * p.psi_ld;
   // the staged rows are copied in 16-byte pieces: FP32 needs an even width
+  if (p.phase) {  // projector phases: the SIMT kernel rotates each gathered point
+    if (p.max_nproj > 32) {
+      set_error("projector matrices with more than 32 projectors are not supported");
+      return HPSI_ERR_UNSUPPORTED;
+    }
+    dim3 grid(p.nmat, unsigned((ld2 + 31) / 32));
+    bra_simt_kernel<T, true><<<grid, 128, 0, st>>>(p);
+    HPSI_CHECK_LAUNCH();
+    return HPSI_OK;
+  }
   if (use_tensor && p.max_nproj <= NMAX && ld2 % (16 / sizeof(T)) == 0) {
     dim3 grid(p.nmat, unsigned((ld2 + LANES - 1) / LANES), ksplit);
     bra_dmma_kernel<T><<<grid, 128, 0, st>>>(p);
@@ -205,7 +233,7 @@ hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStrea
     return HPSI_ERR_UNSUPPORTED;
   }
   dim3 grid(p.nmat, unsigned((ld2 + 31) / 32));
-  bra_simt_kernel<T><<<grid, 128, 0, st>>>(p);
+  bra_simt_kernel<T, false><<<grid, 128, 0, st>>>(p);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
 }
@@ -217,7 +245,7 @@ hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStrea
 // energy partial Re(conj(psi0[row]) h) per state.  Each output element is
 // written by exactly one thread, in a fixed order: no atomics, deterministic.
 namespace {
-template <typename T, typename C2>
+template <typename T, typename C2, bool PHASE>
 __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
   // each thread serves two states (sb, sb + 32) of its rows: the row's
   // metadata and projector weights are loaded once for both (12 % faster than
@@ -257,14 +285,39 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
       const int4 E = __ldg(k.ent + e);
       const T *pp = pt + E.x;
       const C2 *pr = proj + (long long)E.y * k.proj_ld + sb;
-      for (int j = 0; j < E.z; ++j) {
-        const T w = pp[j];
+      if constexpr (!PHASE) {
+        for (int j = 0; j < E.z; ++j) {
+          const T w = pp[j];
+#pragma unroll
+          for (int u = 0; u < SPT; ++u) {
+            if (!act[u]) continue;
+            const C2 v = pr[(long long)j * k.proj_ld + 32 * u];
+            h[u].x += w * v.x;
+            h[u].y += w * v.y;
+          }
+        }
+      } else {
+        // this point's contribution times conj(phase) (the ket of
+        // hamiltonian_elec_base_inc.F90:934-1025 with projector phases)
+        C2 g[SPT];
+#pragma unroll
+        for (int u = 0; u < SPT; ++u) g[u].x = g[u].y = 0;
+        for (int j = 0; j < E.z; ++j) {
+          const T w = pp[j];
+#pragma unroll
+          for (int u = 0; u < SPT; ++u) {
+            if (!act[u]) continue;
+            const C2 v = pr[(long long)j * k.proj_ld + 32 * u];
+            g[u].x += w * v.x;
+            g[u].y += w * v.y;
+          }
+        }
+        const T *ph = static_cast<const T *>(k.phase) + 2 * (long long)E.w;
+        const T c = ph[0], sn = ph[1];
 #pragma unroll
         for (int u = 0; u < SPT; ++u) {
-          if (!act[u]) continue;
-          const C2 v = pr[(long long)j * k.proj_ld + 32 * u];
-          h[u].x += w * v.x;
-          h[u].y += w * v.y;
+          h[u].x += g[u].x * c + g[u].y * sn;
+          h[u].y += g[u].y * c - g[u].x * sn;
         }
       }
     }
@@ -328,7 +381,10 @@ hpsi_status launch_ket(const KetArgs &k, cudaStream_t st) {
   if (k.nk == 0) return HPSI_OK;
   using C2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   dim3 grid((k.nst + 63) / 64, ket_row_blocks(k.nk));  // two states per thread
-  ket_kernel<T, C2><<<grid, dim3(32, 8), 0, st>>>(k);
+  if (k.phase)
+    ket_kernel<T, C2, true><<<grid, dim3(32, 8), 0, st>>>(k);
+  else
+    ket_kernel<T, C2, false><<<grid, dim3(32, 8), 0, st>>>(k);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
 }

@@ -22,6 +22,7 @@ struct ProjArgs {
   int nprojections;
   int min_npoints;       // smallest sphere (bounds the K split)
   double *partial;       // split-K partials [ksplit][nprojections][proj_ld] complex, FP64
+  const void *phase = nullptr;  // per sphere point complex phase (storage type), or null
 };
 
 struct KetArgs {
@@ -41,6 +42,7 @@ struct KetArgs {
   long long psi0_ld;
   double *obs;           // [ket_row_blocks][obs_ld][2] or null
   int obs_ld;
+  const void *phase = nullptr;  // per sphere point complex phase (storage type), or null
 };
 
 int bra_ksplit(const ProjArgs &p, int num_sms);

@@ -67,6 +67,7 @@ SIGNATURES = {
     "hpsi_hamiltonian_set_projectors": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
                                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                                     C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "hpsi_hamiltonian_set_projector_phases": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
     "hpsi_apply_h": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_int32, C.c_int32,
                                  C.c_void_p]),
     "hpsi_boundaries_set": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_void_p]),
@@ -297,6 +298,17 @@ class Hamiltonian:
         sc = np.ascontiguousarray(np.concatenate(scals).astype(np.float64))
         check(load().hpsi_hamiltonian_set_projectors(self.handle, len(maps), _ip(npts), _ip(nproj), _ip(mp),
                                                      _dp(mt), _dp(sc)))
+
+    def set_projector_phases(self, phases):
+        """Per sphere point complex phases (a list with one array per matrix,
+        or one concatenated array), or None to remove them."""
+        if phases is None:
+            check(load().hpsi_hamiltonian_set_projector_phases(self.handle, None))
+            return
+        if isinstance(phases, (list, tuple)):
+            phases = np.concatenate([np.asarray(a, dtype=np.complex128) for a in phases])
+        ph = np.ascontiguousarray(np.asarray(phases, dtype=np.complex128))
+        check(load().hpsi_hamiltonian_set_projector_phases(self.handle, _dp(ph.view(np.float64))))
 
     def autotune(self, dtype=HPSI_C128, ld=32, stream=None):
         """Pick the fastest pass shape for batches of width ld; returns
