@@ -14,7 +14,8 @@ adds the numpy restatements of the small dense pieces:
   (S = U^H U, psi <- psi U^-1);
 * ``kb_bra`` / ``kb_ket`` -- the KB projections of a batch and their
   scatter-add back, src/hamiltonian/hamiltonian_elec_base_inc.F90:650-780,
-  909-1027 (split at the reduction over domains, :836);
+  909-1027 (split at the reduction over domains, :836), with optional projector
+  phases for k != 0 (:680-701, 934-1025);
 * ``derivatives_test_error`` -- src/grid/derivatives_inc.F90:378-492, the
   Laplacian error that testsuite/components/03-derivatives_3d.test pins.
 
@@ -337,27 +338,36 @@ def ghost_exchange(domains, batches):
     return batches
 
 
-def kb_bra(maps, mats, scals, psi):
+def kb_bra(maps, mats, scals, psi, phases=None):
     """KB projections of a batch, proj[r, s] = scal[r] * sum_k P[k, r] *
     psi[map[k], s], matrices in order: the gather and GEMM of
     X(hamiltonian_elec_base_nlocal_start)
     (src/hamiltonian/hamiltonian_elec_base_inc.F90:650-780), before the
     reduction over domains (:836)."""
     x = np.asarray(psi)
-    rows = [np.asarray(sc, dtype=np.float64)[:, None] * (np.asarray(mt, dtype=np.float64).T @ x[np.asarray(mp)])
-            for mp, mt, sc in zip(maps, mats, scals)]
+    phases = [None] * len(maps) if phases is None else phases
+    # with projector phases (k != 0) the gathered points are psi(map) * phase
+    # (hamiltonian_elec_base_inc.F90:680-701)
+    rows = [np.asarray(sc, dtype=np.float64)[:, None] *
+            (np.asarray(mt, dtype=np.float64).T @ (x[np.asarray(mp)] if ph is None else
+                                                   x[np.asarray(mp)] * np.asarray(ph)[:, None]))
+            for mp, mt, sc, ph in zip(maps, mats, scals, phases)]
     return np.concatenate(rows) if rows else np.zeros((0,) + x.shape[1:], dtype=x.dtype)
 
 
-def kb_ket(maps, mats, proj, h):
+def kb_ket(maps, mats, proj, h, phases=None):
     """h[map[k], s] += sum_r P[k, r] * proj[r, s], in place: the GEMM and
     scatter-add of X(hamiltonian_elec_base_nlocal_finish)
     (src/hamiltonian/hamiltonian_elec_base_inc.F90:909-1027)."""
     r = 0
-    for mp, mt in zip(maps, mats):
+    phases = [None] * len(maps) if phases is None else phases
+    for mp, mt, ph in zip(maps, mats, phases):
         mt = np.asarray(mt, dtype=np.float64)
         n = mt.shape[1]
-        np.add.at(h, np.asarray(mp), mt @ proj[r: r + n])
+        c = mt @ proj[r: r + n]
+        if ph is not None:  # conjugate phase on the way back (:934-1025)
+            c = c * np.conj(np.asarray(ph))[:, None]
+        np.add.at(h, np.asarray(mp), c)
         r += n
     return h
 

@@ -203,3 +203,26 @@ def test_lanczos_restatement_matches_dense_exponential():
         got, mdim, res = O.lanczos(H, psi, dt, max_order=60, tol=1e-11)
         assert res < 1e-11 and mdim > 3
         assert rel_maxnorm_per_state(got, ref) <= 1e-9
+
+
+def test_kb_with_projector_phases_is_hermitian():
+    """The oracle's KB term with projector phases (k != 0) is a Hermitian
+    operator, <a|K b> = <K a|b>, and unit phases give the plain term."""
+    from helpers import small_sphere_system
+    from oracle import oracle as O
+    m, v, proj, psi = small_sphere_system(seed=67, nst=2, natoms=3)
+    rng = np.random.default_rng(68)
+    ph = [np.exp(1j * rng.uniform(0, 2 * np.pi, len(mp))) for mp in proj.maps]
+
+    def K(x, phases):
+        p = O.kb_bra(proj.maps, proj.mats, proj.scals, x, phases)
+        return O.kb_ket(proj.maps, proj.mats, p, np.zeros((m.np, x.shape[1]), complex), phases)
+
+    a, b = psi[: m.np, :1], psi[: m.np, 1:2]
+    lhs = np.vdot(a, K(b, ph))
+    rhs = np.vdot(K(a, ph), b)
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+    ones = [np.ones(len(mp)) for mp in proj.maps]
+    x = psi[: m.np]
+    assert np.allclose(K(x, ones), K(x, None), rtol=0, atol=1e-13 * np.abs(K(x, None)).max())
+    assert np.abs(K(x, ph) - K(x, None)).max() > 1e-3 * np.abs(K(x, None)).max()
