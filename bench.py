@@ -169,15 +169,26 @@ def build_system(small=False):
     return fixtures.config1()
 
 
-def cpu_reference_rate(sysm, nst_sample, min_seconds=10.0, max_reps=200):
-    """Reference CPU H.psi rate (Gpoint-states/s) on a sample of the states."""
+SAMPLE_STATES = [0, 17, 38, 63, 64, 90, 111, 127]  # spread over the 16 state chunks
+
+
+def rel_maxnorm_per_state(got, ref):
+    """max over states of max_ip |got - ref| / max_ip |ref| (the parity metric)."""
+    num = np.max(np.abs(np.asarray(got) - np.asarray(ref)), axis=0)
+    den = np.max(np.abs(np.asarray(ref)), axis=0)
+    return float(np.max(num / np.where(den == 0, 1.0, den)))
+
+
+def cpu_reference_rate(sysm, sample, min_seconds=10.0, max_reps=200):
+    """Reference CPU H.psi rate (Gpoint-states/s) on a sample of the states,
+    and the CPU H psi of that sample (the parity check of the timed run)."""
     from oracle import oracle as O
     from hpsi.stencil import laplacian_weights, star_points
     m = sysm.mesh
     P = O.Projectors(sysm.proj.maps, sysm.proj.mats, sysm.proj.scals) if sysm.proj else None
     H = O.Hamiltonian(m, laplacian_weights(m.spacing), star_points(), v=sysm.v, projectors=P)
-    psi = np.ascontiguousarray(sysm.psi[:, :nst_sample])
-    H.apply(psi)  # warm
+    psi = np.ascontiguousarray(sysm.psi[:, sample])
+    ref = H.apply(psi)  # warm, and the check values
     t0 = time.perf_counter()
     reps = 0
     while True:
@@ -186,16 +197,18 @@ def cpu_reference_rate(sysm, nst_sample, min_seconds=10.0, max_reps=200):
         el = time.perf_counter() - t0
         if el >= min_seconds or reps >= max_reps:
             break
-    rate = m.np * nst_sample * reps / el / 1e9
+    n = len(sample)
+    rate = m.np * n * reps / el / 1e9
     kind = "reference" if H.used_reference_kernel else "port"
-    sample = (f"{reps} H.psi applications on {nst_sample} of the 128 states "
-              f"({el:.1f} s; stencil = reference operate.c compiled from source)" if kind == "reference"
-              else f"{reps} H.psi applications on {nst_sample} states ({el:.1f} s)")
-    return rate, H.nthreads, kind, sample
+    sample_txt = (f"{reps} H.psi applications on {n} of the {sysm.psi.shape[1]} states "
+                  f"({el:.1f} s; stencil = reference operate.c compiled from source)" if kind == "reference"
+                  else f"{reps} H.psi applications on {n} states ({el:.1f} s)")
+    return rate, H.nthreads, kind, sample_txt, ref
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference CPU path on the box's host cores."""
+    """--impl reference: the reference CPU path on the box's host cores, each
+    step one H.psi over the whole 128-state batch of the workload."""
     if rank != 0:
         return
     sysm = build_system(args.small)
@@ -204,23 +217,25 @@ def run_reference(args, rank, world):
     m = sysm.mesh
     P = O.Projectors(sysm.proj.maps, sysm.proj.mats, sysm.proj.scals)
     H = O.Hamiltonian(m, laplacian_weights(m.spacing), star_points(), v=sysm.v, projectors=P)
-    nst_sample = 8
-    psi = np.ascontiguousarray(sysm.psi[:, :nst_sample])
+    psi = np.ascontiguousarray(sysm.psi)
+    nst = psi.shape[1]
     for _ in range(args.warmup):
         H.apply(psi)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         H.apply(psi)
     el = time.perf_counter() - t0
-    rate = m.np * nst_sample * args.steps / el / 1e9
+    rate = m.np * nst * args.steps / el / 1e9
     kind = "reference" if H.used_reference_kernel else "port"
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "sample_states": nst_sample},
+        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD + (" [small]" if args.small else ""),
+                                                 "step": "one H.psi (kinetic + local + KB) over the whole batch"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": H.nthreads, "kind": kind,
-                         "sample": f"each step = one H.psi on {nst_sample} of the 128 states"},
+                         "sample": f"each step = one H.psi on all {nst} states (stencil = the reference's "
+                                   "operate.c compiled from source; vpsi and KB restated)"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -364,30 +379,19 @@ def run_configs(args):
     del ham, dm
 
     # ---- 64 grouped systems of uneven size, 100 Taylor steps -----------------------
-    rng = np.random.default_rng(2024)
-    nsys = 16 if args.small else 64
-    sides = np.exp(rng.uniform(np.log(32), np.log(96), nsys)).astype(int)
-    nsts = np.exp(rng.uniform(np.log(4), np.log(64), nsys)).astype(int)
-    atoms = rng.integers(2, 17, nsys)
+    systems = fixtures.config3(nsys=16 if args.small else 64)
+    nsys = len(systems)
     hams, dms, xs64 = [], [], []
     pts = 0
-    for i in range(nsys):
-        n = int(sides[i])
-        mm = index_box_mesh((n, n, n), 0.25)
-        v = fixtures.soft_coulomb(mm, rng)
-        proj = fixtures.kb_projectors(mm, int(atoms[i]), rng, radius=2.0, min_dist=2.0,
-                                      place_radius=0.45 * n * 0.25)
-        d_ = lib.DeviceMesh(mm)
-        h_ = lib.Hamiltonian(d_, laplacian_weights(mm.spacing), star_points(), v=v, projectors=proj)
-        nst = int(nsts[i])
-        ld = 8 * ((nst + 7) // 8)
-        xx = torch.zeros((mm.np_part, ld), dtype=torch.complex128, device=dev)
-        f = rng.standard_normal((mm.np, nst)) + 1j * rng.standard_normal((mm.np, nst))
-        xx[: mm.np, :nst] = torch.from_numpy(f / np.sqrt(mm.np * mm.vol_pp))
+    for sy in systems:
+        d_ = lib.DeviceMesh(sy.mesh)
+        h_ = lib.Hamiltonian(d_, laplacian_weights(sy.mesh.spacing), star_points(), v=sy.v, projectors=sy.proj)
         dms.append(d_)
         hams.append(h_)
-        xs64.append(xx)
-        pts += mm.np * nst
+        xs64.append(torch.from_numpy(sy.psi).to(dev))
+        pts += sy.mesh.np * sy.nst
+    sides = np.array([round(sy.mesh.np ** (1 / 3)) for sy in systems])
+    nsts = np.array([sy.nst for sy in systems])
     grp = lib.Group(hams)
     out = {}
     steps = 100
@@ -425,6 +429,64 @@ def run_configs(args):
     emit({"config": f"adjoint gradient, box 64^3 h=0.25, 16 states, {nsteps} steps dt=0.01, checkpoint 25",
           "unit": "s per gradient", "seconds": el, "forward_equiv_steps_per_s": nsteps / el, "J": J,
           "grad_eps_norm": float(np.linalg.norm(ge)), "grad_v_norm": float(np.linalg.norm(gv))})
+
+
+def _group_extra(dev, small, timed):
+    """Config 3: uneven independent systems advanced together (one persistent
+    stencil launch per Horner level, CUDA graph), FP64 and FP32 storage.
+    Roofline: algorithmic bytes of a Taylor step, 14 S per point-state of the
+    useful states (read psi once per level, write the level, update psi)."""
+    import torch
+    from hpsi import fixtures, lib
+    from hpsi.stencil import laplacian_weights, star_points
+    systems = fixtures.config3(nsys=16 if small else 64)
+    hams, dms, xs = [], [], []
+    pts = 0
+    for sy in systems:
+        d_ = lib.DeviceMesh(sy.mesh)
+        h_ = lib.Hamiltonian(d_, laplacian_weights(sy.mesh.spacing), star_points(), v=sy.v, projectors=sy.proj)
+        dms.append(d_)
+        hams.append(h_)
+        xs.append(torch.from_numpy(sy.psi).to(dev))
+        pts += sy.mesh.np * sy.nst
+    grp = lib.Group(hams)
+    out = {"systems": len(systems), "point_states": int(pts), "steps": 10, "dt": 0.01}
+    peak, _ = peaks()
+    for name, dtype, S in (("fp64", torch.complex128, 16), ("fp32", torch.complex64, 8)):
+        ys = [x.to(dtype) for x in xs]
+        ms = timed(lambda: grp.taylor_steps(ys, 10, 0.01), 1, 1)
+        alg = pts * 14 * S * 10
+        out[name] = {"ms_per_taylor_step": ms / 10, "taylor_steps_per_s": 10 / (ms / 1e3),
+                     "hpsi_Gpoint_states_per_s": 4 * pts * 10 / (ms / 1e3) / 1e9,
+                     "roofline": {"achieved_GBs": alg / (ms / 1e3) / 1e9, "frac": alg / (ms / 1e3) / 1e9 / peak,
+                                  "alg_bytes_per_step": alg / 10}}
+        del ys
+    grp.close()
+    return out
+
+
+def _box_extra(dev, timed, steps):
+    """Config 0: 64^3 box, 32 states, kinetic + local H.psi, FP64 and FP32
+    storage; roofline of the whole apply (2 S + 8/nst bytes per point-state)."""
+    import torch
+    from hpsi import fixtures, lib
+    from hpsi.stencil import laplacian_weights, star_points
+    s0 = fixtures.config0()
+    m = s0.mesh
+    dm = lib.DeviceMesh(m)
+    ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=s0.v)
+    x = torch.from_numpy(s0.psi).to(dev)
+    peak, _ = peaks()
+    out = {"workload": "box 64^3 h=0.25 (np=262144), 32 states, kinetic + local"}
+    for name, dtype, S in (("fp64", torch.complex128, 16), ("fp32", torch.complex64, 8)):
+        xx = x.to(dtype)
+        y = torch.zeros((m.np, 32), dtype=dtype, device=dev)
+        ms = timed(lambda: ham.apply(xx, y), steps, 3)
+        alg = m.np * 32 * 2 * S + m.np * 8
+        out[name] = {"value": m.np * 32 * steps / (ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms / steps,
+                     "roofline": {"achieved_GBs": alg / (ms / steps / 1e3) / 1e9,
+                                  "frac": alg / (ms / steps / 1e3) / 1e9 / peak}}
+    return out
 
 
 def main():
@@ -495,6 +557,8 @@ def main():
     lib.profile_enable(False)
     ms_step = ms / args.steps
     value = world * m.np * nst * args.steps / (ms / 1e3) / 1e9
+    sample = [i for i in SAMPLE_STATES if i < nst]
+    y_sample = y[:, sample].cpu().numpy()
 
     # roofline of the dominant kernel (fused stencil pass)
     S = 16
@@ -519,30 +583,41 @@ def main():
     # ---- TD steps (exp_mid + laser): FP64 plain launches vs FP32 graph replay --
     # dt = 0.005: at h = 0.2 the order-4 star Laplacian reaches E_max ~ 244 Ha, and
     # the 4th-order Taylor series is stable only for dt * E_max <= 2 sqrt(2); dt = 0.02
-    # (dt * E_max = 4.9) diverges within a few steps in any implementation.
+    # (dt * E_max = 4.9) diverges within a few steps in any implementation.  The
+    # FP32-vs-FP64 observables are compared over the whole 200-step run.
     dt_td = 0.005
-    laser = dict(E0=0.01, omega=0.057, T=2000 * dt_td)
+    ntd = 200
+    laser = dict(E0=0.01, omega=0.057, T=ntd * dt_td)
     td = {}
     for name, xs, graph in (("td_fp64_plain", x.clone(), False), ("td_fp32_graph", x32.clone(), True)):
-        ham.td_propagate(xs, 1, dt_td, graph=graph, **laser)  # warm-up (workspaces, graph path)
+        xw = xs.clone()
+        ham.td_propagate(xw, 1, dt_td, graph=graph, **laser)  # warm-up (workspaces, graph path)
+        del xw
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
-        E, D, N = ham.td_propagate(xs, tk, dt_td, graph=graph, **laser)
+        E, D, N = ham.td_propagate(xs, ntd, dt_td, graph=graph, **laser)
         el = max_over_ranks(time.perf_counter() - t0)
-        td[name] = {"steps_per_s": tk / el, "ms_per_step": el / tk * 1e3, "energy": E, "dipole": D}
+        td[name] = {"steps_per_s": ntd / el, "ms_per_step": el / ntd * 1e3, "energy": E, "dipole": D, "norm": N}
         del xs
     e64, e32 = td["td_fp64_plain"].pop("energy"), td["td_fp32_graph"].pop("energy")
     d64, d32 = td["td_fp64_plain"].pop("dipole"), td["td_fp32_graph"].pop("dipole")
+    nn64, nn32 = td["td_fp64_plain"].pop("norm"), td["td_fp32_graph"].pop("norm")
     td["fp32_vs_fp64"] = {"energy_rel_err_max": float(np.max(np.abs(e32 - e64) / np.abs(e64))),
-                          "dipole_abs_err_max": float(np.max(np.abs(d32 - d64))), "steps": tk, "dt": dt_td}
+                          "dipole_abs_err_max": float(np.max(np.abs(d32 - d64))),
+                          "dipole_rel_err_max": float(np.max(np.abs(d32 - d64)) / max(np.max(np.abs(d64)), 1e-300)),
+                          "norm_rel_err_max": float(np.max(np.abs(nn32 - nn64) / nn64)),
+                          "steps": ntd, "dt": dt_td, "laser": "E0=0.01 w=0.057 sin^2 envelope over the run"}
+
+    # ---- other configurations, measured in the same run --------------------------
+    box = _box_extra(dev, timed, args.steps)
+    group = _group_extra(dev, args.small, timed)
 
     # ---- e2e through the C ABI with pinned host buffers -----------------------
     xh = torch.from_numpy(sysm.psi).pin_memory()
     yh = torch.zeros((m.np, nst), dtype=torch.complex128).pin_memory()
-    ke = max(2, min(args.steps, 5))
-    for _ in range(1):
-        ham.apply(xh, yh)
+    ke = args.steps
+    ham.apply(xh, yh)
     barrier()
     t0 = time.perf_counter()
     for _ in range(ke):
@@ -551,11 +626,14 @@ def main():
     el = max_over_ranks(time.perf_counter() - t0)
     e2e = world * m.np * nst * ke / el / 1e9
 
-    # ---- CPU baseline (rank 0, N=1 only) -------------------------------------
+    # ---- CPU baseline and the oracle check of the timed run (rank 0, N=1) -----
     cpu = None
+    err = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, kind, sample = cpu_reference_rate(sysm, 8)
-        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        rate, cores, kind, sample_txt, ref = cpu_reference_rate(sysm, sample)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample_txt}
+        err = {"rel_maxnorm_per_state_max": rel_maxnorm_per_state(y_sample, ref), "states": sample,
+               "tolerance": 1e-12, "of": "the FP64 H psi of the timed run vs the FP64 CPU oracle"}
 
     if rank == 0:
         line = {
@@ -567,9 +645,11 @@ def main():
                        "l2": "inputs (2.2 GB) larger than L2; no flush",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(m.np * nst * S),
-                    "d2h_bytes_per_step": int(m.np * nst * S)},
+                    "d2h_bytes_per_step": int(m.np * nst * S), "calls": ke},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "traffic_kind": "ncu DRAM bytes of a smaller case of the same kernel, scaled by "
+                                         "point-states (committed profile summary)",
                          "kernel": "pass_blk_kernel FP64 (fused stencil + local potential)",
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": pass_avg_ms},
             "kernels": {"pass_fp64": {"launches": npass, "ms": pass_ms},
@@ -582,8 +662,12 @@ def main():
                 "taylor4_fp64": {"steps_per_s": tk / (ms_t64 / 1e3), "ms_per_step": ms_t64 / tk},
                 "taylor4_fp32": {"steps_per_s": tk / (ms_t32 / 1e3), "ms_per_step": ms_t32 / tk},
                 **td,
+                "config0_box64": box,
+                "config3_group": group,
             },
         }
+        if err is not None:
+            line["err_vs_oracle"] = err
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)

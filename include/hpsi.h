@@ -104,8 +104,21 @@ hpsi_status hpsi_hamiltonian_set_kinetic(hpsi_hamiltonian *ham, int32_t W,
 
 /* Local potential v(np) for the spin channel of the batch
  * (hm_base%potential, used by X(hamiltonian_elec_base_local_sub),
- * src/hamiltonian/hamiltonian_elec_base_inc.F90:233-242).  Host pointer. */
+ * src/hamiltonian/hamiltonian_elec_base_inc.F90:233-242).  Set-up call: host
+ * or device pointer, returns with the potential in place (it synchronises the
+ * legacy default stream); NULL removes the term. */
 hpsi_status hpsi_hamiltonian_set_vloc(hpsi_hamiltonian *ham, const double *v);
+
+/* The same potential update ordered on `stream`, for hosts that rebuild
+ * hm%potential every time step (hamiltonian_elec_update,
+ * src/hamiltonian/hamiltonian_elec.F90:985-1304): no device synchronisation,
+ * and no allocation after the first call on the handle (which allocates the
+ * device copy and, for host input, a staging buffer of np doubles).  A device
+ * `v` is read when the stream reaches the update, a pinned host `v` likewise
+ * (keep it unchanged until then); a pageable host `v` is copied before the
+ * call returns.  Host input is checked for NaN/Inf; device input is not. */
+hpsi_status hpsi_hamiltonian_update_vloc(hpsi_hamiltonian *ham, const double *v,
+                                         void *stream);
 
 /* Length-gauge laser term folded into the local potential,
  * v(r) += amplitude * pol . r (laser_potential, src/hamiltonian/lasers.F90:823-853). */
@@ -139,13 +152,26 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *ham, int32_t nmat,
 /* Projector phases for k != 0 (projector_phases, built by
  * projector_init_phases, src/hamiltonian/projector.F90:171-247, and applied
  * in src/hamiltonian/hamiltonian_elec_base_inc.F90:680-701 and :934-1025):
- * one complex number per sphere point, 2*sum(npoints) doubles in the order of
- * the map passed to hpsi_hamiltonian_set_projectors.  The bra gathers
- * psi(map) * phase, the ket adds its contribution times conj(phase).  NULL
- * removes them; setting new projectors removes them too.  With phases the
- * bra runs on the SIMT kernel (at most 32 projectors per matrix). */
+ * one complex number per sphere point of each matrix, in the order of the
+ * map passed to hpsi_hamiltonian_set_projectors.  The bra gathers
+ * psi(map) * phase, the ket adds its contribution times conj(phase).
+ * Layout of `phases` (complex numbers as pairs of doubles):
+ *   ld_points == 0: packed, the matrices' points concatenated in matrix
+ *                   order (2*sum(npoints) doubles);
+ *   ld_points >= max(npoints): padded, point k of matrix m at complex index
+ *                   k + m*ld_points (2*nmat*ld_points doubles).  This is the
+ *                   reference's hm_base%projector_phases(1:max_npoints, 1,
+ *                   1:nmat, ik) slice (hamiltonian_elec_base.F90:1267, 1877:
+ *                   projector_phases(max_npoints, nphase, nmat, kpt)), which a
+ *                   Fortran caller passes as projector_phases(:, 1, :, ik) with
+ *                   ld_points = max_npoints (the compiler copies the section
+ *                   into a contiguous temporary).
+ * ld_points below the largest sphere gives HPSI_ERR_ARG.  NULL removes the
+ * phases; setting new projectors removes them too.  With phases the bra runs
+ * on the SIMT kernel (at most 32 projectors per matrix). */
 hpsi_status hpsi_hamiltonian_set_projector_phases(hpsi_hamiltonian *ham,
-                                                  const double *phases);
+                                                  const double *phases,
+                                                  int32_t ld_points);
 
 /* ------------------------------------------------------------------ */
 /* A borrowed state batch (batch_t / wfs_elec_t in packed status). */
@@ -328,8 +354,10 @@ hpsi_status hpsi_density_accumulate(hpsi_mesh *mesh, const hpsi_batch *psi,
  * nor cudaFree.  Its partial sums live in one fixed device array of the
  * library (about 1 MiB, held by every GPU that loads the library until the
  * process exits), so at most HPSI_NOALLOC_MAX_STATES states are accepted;
- * larger batches get HPSI_ERR_ARG.  The first call on a device looks up that
- * array's device address and should come before any stream capture.  All
+ * larger batches get HPSI_ERR_ARG.  The first call in a CUDA context (the
+ * device's primary context, or a context the application created and made
+ * current) looks up that array's address in the context and should come
+ * before any stream capture.  All
  * calls on a device share the array and it keeps the last call's contents:
  * calls that overlap on the GPU (for example on two streams) race and must be
  * ordered by the caller.  `out` (nst doubles) may be host or device memory;

@@ -488,6 +488,7 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   h->tdbuf.release();
   h->adjbuf.release();
   h->lzbuf.release();
+  h->vstage.release();
   h->lzsmall.release();
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   if (h->capture_event) cudaEventDestroy(h->capture_event);
@@ -518,6 +519,7 @@ void hpsi_hamiltonian::proj_free() {
   d_kb_phase = nullptr;
   d_kb_phase_f = nullptr;
   kb_npts = 0;
+  kb_npoints_h.clear();
   d_mat = nullptr;
   d_proj_row = d_map = d_krows = d_kptr = nullptr;
   nk = 0;
@@ -562,38 +564,62 @@ hpsi_status hpsi_hamiltonian_set_kinetic(hpsi_hamiltonian *h, int32_t W, const i
   return HPSI_OK;
 }
 
-hpsi_status hpsi_hamiltonian_set_vloc(hpsi_hamiltonian *h, const double *v) {
-  if (!h) return HPSI_ERR_ARG;
+// Writes v (np doubles, host or device) into the cell array of the potential
+// on `st`.  The cell array and, for host input, the staging buffer are
+// allocated on the first call and reused afterwards.
+static hpsi_status vloc_write(hpsi_hamiltonian *h, const double *v, cudaStream_t st, const char *who) {
   hpsi_mesh *m = h->mesh;
   const long long ncell = (long long)m->box.NX * m->box.NY * m->box.NZ;
+  const bool dev_in = is_device_ptr(v);
+  if (!dev_in)
+    for (int i = 0; i < m->np; ++i)
+      if (!std::isfinite(v[i])) {
+        set_error(std::string(who) + ": non-finite potential at point " + std::to_string(i));
+        return HPSI_ERR_NONFINITE;
+      }
+  if (!h->d_vcell) {
+    hpsi_status s = dev_alloc(reinterpret_cast<void **>(&h->d_vcell), ncell * sizeof(double));
+    if (s) return s;
+    // cells that hold no inner point stay zero from here on
+    HPSI_TRY_CUDA(cudaMemsetAsync(h->d_vcell, 0, ncell * sizeof(double), st));
+  }
+  const double *src = v;
+  if (!dev_in) {
+    hpsi_status s = h->vstage.ensure(size_t(m->np) * sizeof(double));
+    if (s) return s;
+    HPSI_TRY_CUDA(cudaMemcpyAsync(h->vstage.ptr, v, size_t(m->np) * sizeof(double), cudaMemcpyHostToDevice, st));
+    src = static_cast<const double *>(h->vstage.ptr);
+  }
+  scatter_cells_kernel<<<(m->np + 255) / 256, 256, 0, st>>>(src, m->d_cell_of_row, m->np, h->d_vcell);
+  g_launches++;
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_hamiltonian_set_vloc(hpsi_hamiltonian *h, const double *v) {
+  if (!h) return HPSI_ERR_ARG;
   if (!v) {
     dev_free(h->d_vcell);
     h->d_vcell = nullptr;
     return HPSI_OK;
   }
-  for (int i = 0; i < m->np; ++i)
-    if (!std::isfinite(v[i])) {
-      set_error("hpsi_hamiltonian_set_vloc: non-finite potential at point " + std::to_string(i));
-      return HPSI_ERR_NONFINITE;
-    }
-  if (!h->d_vcell) {
-    hpsi_status s = dev_alloc(reinterpret_cast<void **>(&h->d_vcell), ncell * sizeof(double));
-    if (s) return s;
-  }
-  HPSI_TRY_CUDA(cudaMemset(h->d_vcell, 0, ncell * sizeof(double)));
-  double *dv = nullptr;
-  hpsi_status s = dev_alloc(reinterpret_cast<void **>(&dv), size_t(m->np) * sizeof(double));
+  hpsi_status s = vloc_write(h, v, nullptr, "hpsi_hamiltonian_set_vloc");
   if (s) return s;
-  cudaMemcpy(dv, v, size_t(m->np) * sizeof(double), cudaMemcpyHostToDevice);
-  scatter_cells_kernel<<<(m->np + 255) / 256, 256>>>(dv, m->d_cell_of_row, m->np, h->d_vcell);
-  g_launches++;
-  cudaError_t e = cudaDeviceSynchronize();
-  dev_free(dv);
+  // the set-up call returns with the potential in place (legacy stream only)
+  cudaError_t e = cudaStreamSynchronize(nullptr);
   if (e != cudaSuccess) {
     set_error(std::string("hpsi_hamiltonian_set_vloc: ") + cudaGetErrorString(e));
     return HPSI_ERR_CUDA;
   }
   return HPSI_OK;
+}
+
+hpsi_status hpsi_hamiltonian_update_vloc(hpsi_hamiltonian *h, const double *v, void *stream) {
+  if (!h || !v) {
+    set_error("hpsi_hamiltonian_update_vloc: null argument");
+    return HPSI_ERR_ARG;
+  }
+  return vloc_write(h, v, static_cast<cudaStream_t>(stream), "hpsi_hamiltonian_update_vloc");
 }
 
 hpsi_status hpsi_hamiltonian_set_field(hpsi_hamiltonian *h, const double pol[3], double amplitude) {
@@ -733,10 +759,11 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, c
   h->nk = int(krows.size());
   h->min_npoints = minp;
   h->kb_npts = npts_tot;
+  h->kb_npoints_h.assign(npoints, npoints + nmat);
   return HPSI_OK;
 }
 
-hpsi_status hpsi_hamiltonian_set_projector_phases(hpsi_hamiltonian *h, const double *phases) {
+hpsi_status hpsi_hamiltonian_set_projector_phases(hpsi_hamiltonian *h, const double *phases, int32_t ld_points) {
   if (!h) return HPSI_ERR_ARG;
   dev_free(h->d_kb_phase);
   dev_free(h->d_kb_phase_f);
@@ -747,19 +774,38 @@ hpsi_status hpsi_hamiltonian_set_projector_phases(hpsi_hamiltonian *h, const dou
     set_error("hpsi_hamiltonian_set_projector_phases: no projectors set");
     return HPSI_ERR_STATE;
   }
+  int maxn = 0;
+  for (int n : h->kb_npoints_h) maxn = std::max(maxn, n);
+  if (ld_points != 0 && ld_points < maxn) {
+    set_error("hpsi_hamiltonian_set_projector_phases: ld_points " + std::to_string(ld_points) +
+              " is below the largest sphere (" + std::to_string(maxn) + " points)");
+    return HPSI_ERR_ARG;
+  }
+  // packed copy in the order of the map: matrix m's points start at
+  // sum(npoints[0..m-1]) in the packed form, at m * ld_points in the padded one
   const size_t n = 2 * size_t(h->kb_npts);
+  std::vector<double> pd(n);
   std::vector<float> pf(n);
-  for (size_t i = 0; i < n; ++i) {
-    if (!std::isfinite(phases[i])) {
-      set_error("hpsi_hamiltonian_set_projector_phases: non-finite phase");
-      return HPSI_ERR_NONFINITE;
-    }
-    pf[i] = float(phases[i]);
+  size_t o = 0;
+  for (size_t m = 0; m < h->kb_npoints_h.size(); ++m) {
+    const size_t src0 = ld_points ? 2 * m * size_t(ld_points) : o;
+    for (int k = 0; k < h->kb_npoints_h[m]; ++k)
+      for (int c = 0; c < 2; ++c) {
+        const double x = phases[src0 + 2 * size_t(k) + c];
+        if (!std::isfinite(x)) {
+          set_error("hpsi_hamiltonian_set_projector_phases: non-finite phase of matrix " + std::to_string(m) +
+                    ", point " + std::to_string(k));
+          return HPSI_ERR_NONFINITE;
+        }
+        pd[o + 2 * size_t(k) + c] = x;
+        pf[o + 2 * size_t(k) + c] = float(x);
+      }
+    o += 2 * size_t(h->kb_npoints_h[m]);
   }
   hpsi_status s = dev_alloc(reinterpret_cast<void **>(&h->d_kb_phase), n * sizeof(double));
   if (!s) s = dev_alloc(reinterpret_cast<void **>(&h->d_kb_phase_f), n * sizeof(float));
   if (s) return s;
-  HPSI_TRY_CUDA(cudaMemcpy(h->d_kb_phase, phases, n * sizeof(double), cudaMemcpyHostToDevice));
+  HPSI_TRY_CUDA(cudaMemcpy(h->d_kb_phase, pd.data(), n * sizeof(double), cudaMemcpyHostToDevice));
   HPSI_TRY_CUDA(cudaMemcpy(h->d_kb_phase_f, pf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   return HPSI_OK;
 }

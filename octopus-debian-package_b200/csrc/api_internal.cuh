@@ -80,6 +80,7 @@ struct hpsi_hamiltonian {
   int4 *d_kb_ent = nullptr;
   // projector phases (k != 0): one complex number per sphere point, or null
   long long kb_npts = 0;
+  std::vector<int> kb_npoints_h;  // sphere points of each matrix
   double *d_kb_phase = nullptr;
   float *d_kb_phase_f = nullptr;
   bool use_tensor_bra = true;
@@ -99,6 +100,7 @@ struct hpsi_hamiltonian {
   hpsi::Workspace slab_in, slab_out;
   // workspaces
   hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small, tdbuf, adjbuf;
-  hpsi::Workspace lzbuf, lzsmall;  // Lanczos: Krylov vectors, reductions and coefficients
+  hpsi::Workspace lzbuf, lzsmall;
+  hpsi::Workspace vstage;  // host potential staged for hpsi_hamiltonian_update_vloc  // Lanczos: Krylov vectors, reductions and coefficients
   void proj_free();
 };

@@ -10,10 +10,14 @@
 //
 // The array below has a fixed maximum size; every GPU that loads the library
 // holds it until the process exits.  Host code never dereferences or passes
-// the symbol itself: its device address is looked up once per device with
-// cudaGetSymbolAddress and that address is handed to the kernels.
+// the symbol itself: its device address is looked up with
+// cudaGetSymbolAddress once per CUDA context (the module, and with it the
+// array, is loaded separately into every context, so a device ordinal is not
+// enough to name it when a host application creates its own contexts) and
+// that address is handed to the kernels.
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "api_internal.cuh"
@@ -31,30 +35,63 @@ constexpr size_t NOALLOC_DOUBLES =
 
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 
-constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
-double *g_scratch_addr[MAX_DEVICES] = {nullptr};
+// (context, device address of the array in it); a handful of entries at most
+std::vector<std::pair<void *, double *>> g_scratch_addr;
 
-// Device address of the scratch array on the current device (set up once per
-// device, with that device current).
+// The current driver context, through the runtime's driver entry point (the
+// library does not link the driver library itself).  nullptr when no context
+// is current yet.
+hpsi_status current_context(void **ctx) {
+  using get_fn = int (*)(void **);
+  static get_fn fn = nullptr;
+  static std::once_flag once;
+  static cudaError_t lookup = cudaSuccess;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    lookup = cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q);
+    if (lookup == cudaSuccess && q == cudaDriverEntryPointSuccess) fn = reinterpret_cast<get_fn>(p);
+  });
+  if (!fn) {
+    set_error("hpsi_nrm2_noalloc: cuCtxGetCurrent is not available from the driver");
+    return HPSI_ERR_CUDA;
+  }
+  *ctx = nullptr;
+  if (fn(ctx) != 0) {
+    set_error("hpsi_nrm2_noalloc: cuCtxGetCurrent failed");
+    return HPSI_ERR_CUDA;
+  }
+  return HPSI_OK;
+}
+
+// Device address of the scratch array in the current context (looked up once
+// per context, with that context current).
 hpsi_status scratch_address(double **out) {
-  int dev = 0;
-  HPSI_TRY_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= MAX_DEVICES) {
-    set_error("hpsi_nrm2_noalloc: device ordinal out of range");
-    return HPSI_ERR_UNSUPPORTED;
-  }
+  void *ctx = nullptr;
+  hpsi_status s = current_context(&ctx);
+  if (s) return s;
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
-    void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      set_error(std::string("hpsi_nrm2_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      return HPSI_ERR_CUDA;
-    }
-    g_scratch_addr[dev] = static_cast<double *>(ptr);
+  if (ctx)
+    for (auto &e : g_scratch_addr)
+      if (e.first == ctx) {
+        *out = e.second;
+        return HPSI_OK;
+      }
+  void *ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    set_error(std::string("hpsi_nrm2_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return HPSI_ERR_CUDA;
   }
-  *out = g_scratch_addr[dev];
+  // with no context current before, the runtime has just made the device's
+  // primary context current: key the entry on it
+  if (!ctx) {
+    s = current_context(&ctx);
+    if (s) return s;
+  }
+  if (ctx) g_scratch_addr.emplace_back(ctx, static_cast<double *>(ptr));
+  *out = static_cast<double *>(ptr);
   return HPSI_OK;
 }
 

@@ -252,6 +252,24 @@ def local_projectors(dom: Domain, projectors):
                         getattr(projectors, "positions", None))
 
 
+def local_projector_phases(dom: Domain, projectors, phases):
+    """The projector phases (k != 0, one complex number per sphere point of
+    each matrix, src/hamiltonian/projector.F90:171-247) restricted with the
+    same point selection as ``local_projectors``: the phases of this
+    partition's own sphere points, in the order of its local maps."""
+    nglob = int(dom.global_rows.max()) + 1 if dom.global_rows.size else 0
+    nglob = max(nglob, max((int(np.max(m)) + 1 for m in projectors.maps if len(m)), default=0))
+    loc = -np.ones(nglob, dtype=np.int64)
+    loc[dom.inner_rows] = np.arange(dom.np_local)
+    out = []
+    for mp, ph in zip(projectors.maps, phases):
+        ph = np.asarray(ph, dtype=np.complex128)
+        if len(ph) != len(mp):
+            raise ValueError("local_projector_phases: one phase per sphere point of each matrix expected")
+        out.append(np.ascontiguousarray(ph[loc[np.asarray(mp, dtype=np.int64)] >= 0]))
+    return out
+
+
 def apply_partitioned(dom: Domain, psi, hpsi, local_apply, bra=None, ket=None, proj=None, nst=None, group=None,
                       pack=None, unpack=None):
     """H psi of one partition; every rank of ``group`` calls it together.
@@ -326,13 +344,20 @@ class DomainHamiltonian:
     """H psi of one partition on its local mesh: kinetic, local and KB terms
     (KB spheres may cross partitions)."""
 
-    def __init__(self, dom: Domain, weights, points, v_global=None, projectors=None):
+    def __init__(self, dom: Domain, weights, points, v_global=None, projectors=None, projector_phases=None):
+        """``projector_phases``: the global phases (one array per matrix, in
+        the global maps' order) for k != 0; each partition keeps those of
+        its own sphere points."""
         from . import lib
         self.dom = dom
         self.dmesh = lib.DeviceMesh(dom.mesh)
         v = None if v_global is None else np.asarray(v_global)[dom.inner_rows]
         self.local_proj = None if projectors is None else local_projectors(dom, projectors)
         self.ham = lib.Hamiltonian(self.dmesh, weights, points, v=v, projectors=self.local_proj)
+        if projector_phases is not None:
+            if projectors is None:
+                raise ValueError("DomainHamiltonian: projector phases without projectors")
+            self.ham.set_projector_phases(local_projector_phases(dom, projectors, projector_phases))
         self.nprojections = self.ham.nprojections()
         self._proj = {}
 

@@ -36,21 +36,31 @@ def dense_lookup(mesh: Mesh, which: str = "inner"):
     return lut, lo
 
 
-def box_filter(mesh: Mesh, f: np.ndarray) -> np.ndarray:
-    """3-point box filter along x, y and z over the inner points (zero outside)."""
+def box_filter(mesh: Mesh, f: np.ndarray, chunk: int = 16) -> np.ndarray:
+    """3-point box filter along x, y and z over the inner points (zero outside),
+    applied to ``chunk`` states at a time."""
     lut, lo = dense_lookup(mesh)
     ii = mesh.lxyz[: mesh.np].astype(np.int64) - lo
-    shape = lut.shape + f.shape[1:]
-    g = np.zeros(tuple(s + 2 for s in lut.shape) + f.shape[1:], dtype=f.dtype)
-    g[1:-1, 1:-1, 1:-1][ii[:, 2], ii[:, 1], ii[:, 0]] = f[: mesh.np]
-    for ax in range(3):
-        g = (np.roll(g, 1, axis=ax) + g + np.roll(g, -1, axis=ax)) / 3.0
-        # keep the zero frame and the region outside the mesh at zero
-        mask = np.zeros(g.shape[:3], dtype=bool)
-        mask[1:-1, 1:-1, 1:-1][ii[:, 2], ii[:, 1], ii[:, 0]] = True
-        g[~mask] = 0
-    del shape
-    return g[1:-1, 1:-1, 1:-1][ii[:, 2], ii[:, 1], ii[:, 0]]
+    mask = np.zeros(tuple(s + 2 for s in lut.shape), dtype=bool)
+    mask[1:-1, 1:-1, 1:-1][ii[:, 2], ii[:, 1], ii[:, 0]] = True
+    f = np.asarray(f)
+    cols = f.shape[1:] if f.ndim > 1 else ()
+    f2 = f.reshape(f.shape[0], -1)
+    out = np.empty((mesh.np, f2.shape[1]), dtype=f2.dtype)
+    for c0 in range(0, f2.shape[1], chunk):
+        c1 = min(c0 + chunk, f2.shape[1])
+        g = np.zeros(mask.shape + (c1 - c0,), dtype=f2.dtype)
+        g[1:-1, 1:-1, 1:-1][ii[:, 2], ii[:, 1], ii[:, 0]] = f2[: mesh.np, c0:c1]
+        for ax in range(3):
+            def sl(a, b):
+                return tuple(slice(a, b) if i == ax else slice(None) for i in range(3))
+            h = np.zeros_like(g)
+            h[sl(1, -1)] = (g[sl(0, -2)] + g[sl(1, -1)] + g[sl(2, None)]) / 3.0
+            # keep the zero frame and the region outside the mesh at zero
+            h[~mask] = 0
+            g = h
+        out[:, c0:c1] = g[1:-1, 1:-1, 1:-1][ii[:, 2], ii[:, 1], ii[:, 0]]
+    return out.reshape((mesh.np,) + cols)
 
 
 def orthonormalize(mesh: Mesh, psi: np.ndarray) -> np.ndarray:
@@ -170,3 +180,31 @@ def config1(seed: int = 1, nst: int = 128, radius: float = 12.0, spacing: float 
     proj = kb_projectors(m, natoms, rng, place_radius=place_radius)
     psi = random_states(m, nst, rng)
     return System(m, v, psi, proj, f"sphere R={radius} h={spacing} nst={nst} atoms={natoms}")
+
+
+def config3(seed: int = 2024, nsys: int = 64):
+    """Uneven batch of independent systems: cubic boxes with sides
+    ~ round-down(exp(U[ln 32, ln 96])), h = 0.25, states per system
+    ~ exp(U[ln 4, ln 64]), 2..16 KB atoms each with the config-1 projectors,
+    soft-Coulomb wells; states are normalised complex Gaussian noise on the
+    inner points.  Returns a list of System (psi holds np_part rows, zero
+    boundary rows, ld = nst rounded up to a multiple of 8)."""
+    rng = np.random.default_rng(seed)
+    sides = np.exp(rng.uniform(np.log(32), np.log(96), nsys)).astype(int)
+    nsts = np.exp(rng.uniform(np.log(4), np.log(64), nsys)).astype(int)
+    atoms = rng.integers(2, 17, nsys)
+    out = []
+    for i in range(nsys):
+        n = int(sides[i])
+        m = index_box_mesh((n, n, n), 0.25)
+        v = soft_coulomb(m, rng)
+        proj = kb_projectors(m, int(atoms[i]), rng, radius=2.0, min_dist=2.0, place_radius=0.45 * n * 0.25)
+        nst = int(nsts[i])
+        ld = 8 * ((nst + 7) // 8)
+        psi = np.zeros((m.np_part, ld), dtype=np.complex128)
+        f = rng.standard_normal((m.np, nst)) + 1j * rng.standard_normal((m.np, nst))
+        psi[: m.np, :nst] = f / np.sqrt(m.np * m.vol_pp)
+        s = System(m, v, psi, proj, f"box{n}^3 h=0.25 nst={nst} atoms={int(atoms[i])}")
+        s.nst = nst
+        out.append(s)
+    return out

@@ -62,12 +62,13 @@ SIGNATURES = {
     "hpsi_hamiltonian_set_kinetic": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
                                                  C.POINTER(C.c_double), C.c_double]),
     "hpsi_hamiltonian_set_vloc": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "hpsi_hamiltonian_update_vloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "hpsi_hamiltonian_set_field": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.c_double]),
     "hpsi_hamiltonian_set_phase_corr": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
     "hpsi_hamiltonian_set_projectors": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
                                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                                     C.POINTER(C.c_double), C.POINTER(C.c_double)]),
-    "hpsi_hamiltonian_set_projector_phases": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "hpsi_hamiltonian_set_projector_phases": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.c_int32]),
     "hpsi_apply_h": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_int32, C.c_int32,
                                  C.c_void_p]),
     "hpsi_boundaries_set": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_void_p]),
@@ -279,6 +280,25 @@ class Hamiltonian:
         v = np.ascontiguousarray(np.asarray(v, dtype=np.float64))
         check(load().hpsi_hamiltonian_set_vloc(self.handle, _dp(v)))
 
+    def update_vloc(self, v, stream=None):
+        """Stream-ordered potential update (hpsi_hamiltonian_update_vloc): ``v``
+        a float64 device tensor of np entries, or a host array."""
+        try:
+            import torch
+            if isinstance(v, torch.Tensor):
+                if v.dtype != torch.float64 or not v.is_contiguous() or v.numel() < self.dmesh.mesh.np:
+                    raise ValueError("update_vloc: contiguous float64 tensor of np entries expected")
+                ptr = C.c_void_p(v.data_ptr())
+                check(load().hpsi_hamiltonian_update_vloc(self.handle, ptr, _stream_ptr(stream)))
+                return
+        except ImportError:  # pragma: no cover
+            pass
+        v = np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+        if v.size < self.dmesh.mesh.np:
+            raise ValueError("update_vloc: np entries expected")
+        self._vhost = v  # kept alive until the next update (pinned copies read it later)
+        check(load().hpsi_hamiltonian_update_vloc(self.handle, C.c_void_p(v.ctypes.data), _stream_ptr(stream)))
+
     def set_field(self, pol, amplitude: float):
         p = np.ascontiguousarray(np.asarray(pol, dtype=np.float64))
         check(load().hpsi_hamiltonian_set_field(self.handle, _dp(p), C.c_double(amplitude)))
@@ -298,17 +318,31 @@ class Hamiltonian:
         sc = np.ascontiguousarray(np.concatenate(scals).astype(np.float64))
         check(load().hpsi_hamiltonian_set_projectors(self.handle, len(maps), _ip(npts), _ip(nproj), _ip(mp),
                                                      _dp(mt), _dp(sc)))
+        self._kb_npoints = [int(n) for n in npts]
 
-    def set_projector_phases(self, phases):
-        """Per sphere point complex phases (a list with one array per matrix,
-        or one concatenated array), or None to remove them."""
+    def set_projector_phases(self, phases, ld_points=0):
+        """Per sphere point complex phases: a list with one array per matrix,
+        one concatenated array (ld_points = 0), or a padded (nmat, ld_points)
+        array / its flattening (point k of matrix m at m * ld_points + k, the
+        reference's projector_phases(:, 1, :, ik)); None removes them."""
         if phases is None:
-            check(load().hpsi_hamiltonian_set_projector_phases(self.handle, None))
+            check(load().hpsi_hamiltonian_set_projector_phases(self.handle, None, 0))
             return
+        npts = getattr(self, "_kb_npoints", None)
+        if npts is None:
+            raise ValueError("set_projector_phases: no projectors set")
         if isinstance(phases, (list, tuple)):
+            if [len(a) for a in phases] != list(npts):
+                raise ValueError("set_projector_phases: one phase per sphere point of each matrix expected")
             phases = np.concatenate([np.asarray(a, dtype=np.complex128) for a in phases])
-        ph = np.ascontiguousarray(np.asarray(phases, dtype=np.complex128))
-        check(load().hpsi_hamiltonian_set_projector_phases(self.handle, _dp(ph.view(np.float64))))
+            ld_points = 0
+        ph = np.ascontiguousarray(np.asarray(phases, dtype=np.complex128)).ravel()
+        need = sum(npts) if ld_points == 0 else len(npts) * int(ld_points)
+        if ld_points and ld_points < max(npts):
+            raise ValueError(f"set_projector_phases: ld_points {ld_points} below the largest sphere ({max(npts)})")
+        if ph.size != need:
+            raise ValueError(f"set_projector_phases: {ph.size} phases given, {need} expected")
+        check(load().hpsi_hamiltonian_set_projector_phases(self.handle, _dp(ph.view(np.float64)), int(ld_points)))
 
     def autotune(self, dtype=HPSI_C128, ld=32, stream=None):
         """Pick the fastest pass shape for batches of width ld; returns

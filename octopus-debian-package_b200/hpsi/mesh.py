@@ -98,15 +98,24 @@ def _build(inner_lo, inner_hi, contains, spacing, order, bsize, periodic=False):
     ii = inner - nr_lo[None, :]
     lut[ii[:, 2], ii[:, 1], ii[:, 0]] = np.arange(len(inner))
 
+    # boundary candidates: star neighbours of inner points that are not inner
+    # points, marked on the dense enlarged grid (each point once)
     pts = star_points(order)
-    nb = (inner[:, None, :] + pts[None, :, :]).reshape(-1, 3)
-    jj = nb - nr_lo[None, :]
-    is_inner = lut[jj[:, 2], jj[:, 1], jj[:, 0]] >= 0
-    cand_b = nb[~is_inner]
+    inner_mask = lut >= 0
+    reach = np.zeros_like(inner_mask)
+    for p in pts:
+        if not p.any():
+            continue
+        dx, dy, dz = (int(c) for c in p)
+        reach[max(dz, 0): ext[2] + min(dz, 0), max(dy, 0): ext[1] + min(dy, 0), max(dx, 0): ext[0] + min(dx, 0)] |= \
+            inner_mask[max(-dz, 0): ext[2] - max(dz, 0), max(-dy, 0): ext[1] - max(dy, 0),
+                       max(-dx, 0): ext[0] - max(dx, 0)]
+    zz, yy, xx = np.nonzero(reach & ~inner_mask)
+    cand_b = np.stack([xx, yy, zz], axis=1).astype(np.int64) + nr_lo[None, :]
     if len(cand_b):
         in_box = contains(cand_b.astype(np.float64) * spacing[None, :])
         cand_b = cand_b[~in_box]
-    bnd = np.unique(cand_b, axis=0) if len(cand_b) else np.zeros((0, 3), dtype=np.int64)
+    bnd = cand_b if len(cand_b) else np.zeros((0, 3), dtype=np.int64)
 
     offset = ext // 2
     nblocks = ext // np.asarray(bsize) + 1

@@ -2,7 +2,7 @@
 
 Run in a container where the reference sources are present:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF=<reference source tree> && python tests/golden/make_golden.py
 
 It compiles nothing itself; it loads oracle/_ref/libref_operate.so (the
 reference's src/grid/operate.c built from source) and records, for small seeded
@@ -31,7 +31,7 @@ from oracle import oracle as O  # noqa: E402
 def ref_stencil(mesh, w, x, ld):
     fn = O.ref_operate()
     if fn is None:
-        raise SystemExit("oracle/_ref/libref_operate.so missing: run `make -C oracle ref` first")
+        raise SystemExit("oracle/_ref/libref_operate.so missing: run `make -C oracle ref REF=<reference source tree>` first")
     op = O.Operator(mesh, star_points())
     wre = np.ascontiguousarray(w * -0.5)
     fi = np.ascontiguousarray(x)

@@ -2,7 +2,7 @@
 
 Run in a container where the reference sources are present:
 
-    make -C oracle ref && python tests/golden/make_indices_obf.py
+    make -C oracle ref REF=<reference source tree> && python tests/golden/make_indices_obf.py
 
 It loads oracle/_ref/libref_io_binary.so and oracle/_ref/libref_hilbert.so
 (the reference's src/basic/io_binary.c and src/grid/hilbert.c built from

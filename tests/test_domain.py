@@ -150,6 +150,35 @@ def test_partitioned_hpsi_with_kb_spheres_across_partitions(nparts):
         assert np.max(np.abs(h - ref[d.inner_rows])) <= 1e-13 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("nparts", [2, 3])
+def test_partitioned_kb_with_projector_phases(nparts):
+    """k != 0: each partition keeps the phases of its own sphere points
+    (local_projector_phases, the selection of local_projectors); the summed
+    shares and the ket on every partition equal the global KB term with
+    phases."""
+    from hpsi.domain import local_projector_phases, local_projectors, partition_z
+    from oracle import oracle as O
+    m, v, proj, psi = small_sphere_system(seed=23, nst=3, natoms=4)
+    rng = np.random.default_rng(24)
+    ph = [np.exp(1j * rng.uniform(0, 2 * np.pi, len(mp))) for mp in proj.maps]
+    full = O.kb_bra(proj.maps, proj.mats, proj.scals, psi, ph)
+    ref = O.kb_ket(proj.maps, proj.mats, full, np.zeros((m.np, 3), complex), ph)
+    doms = partition_z(m, nparts)
+    locs = [d.local_batch(psi) for d in doms]
+    lps = [local_projectors(d, proj) for d in doms]
+    lph = [local_projector_phases(d, proj, ph) for d in doms]
+    for lp, p_ in zip(lps, lph):
+        assert [len(a) for a in lp.maps] == [len(a) for a in p_]
+    total = sum(O.kb_bra(lp.maps, lp.mats, lp.scals, b[: d.np_local], p_)
+                for lp, p_, d, b in zip(lps, lph, doms, locs))
+    assert np.max(np.abs(total - full)) <= 1e-13 * np.max(np.abs(full))
+    for lp, p_, d in zip(lps, lph, doms):
+        h = O.kb_ket(lp.maps, lp.mats, total, np.zeros((d.np_local, 3), complex), p_)
+        assert np.max(np.abs(h - ref[d.inner_rows])) <= 1e-13 * np.max(np.abs(ref))
+    with pytest.raises(ValueError):
+        local_projector_phases(doms[0], proj, [p_[:-1] for p_ in ph])
+
+
 def _rank_kb_main(rank, world, port, out):
     import torch
     import torch.distributed as dist

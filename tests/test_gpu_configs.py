@@ -1,0 +1,149 @@
+"""GPU parity at the full sizes of the benchmark configurations.
+
+The small-mesh parity tests cover every code path on shapes the oracle
+finishes in milliseconds; these run the two configurations the bench measures
+at their real sizes, where the work lists have thousands of items, the
+split-K bra sums many partial blocks and every state chunk of a 128-wide batch
+is in flight:
+
+* sphere R = 12 bohr, h = 0.2 (904,089 inner points), 32 KB atoms x 9
+  projectors, 128 complex128 states (the headline H psi);
+* box 64^3, h = 0.25, 32 states, kinetic + local.
+
+The device computes the whole batch; the oracle (FP64 CPU, the reference's
+compiled stencil) computes a sample of states spread over the state chunks,
+and each sampled state is compared by the parity metric (relative max-norm
+per state): FP64 <= 1e-12, FP32 storage <= 2e-5.  Size-independent checks
+run on the whole batch: the Hermiticity of H on the sampled pairs and the
+norm change of one Taylor step.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_maxnorm_per_state
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 2e-5
+SAMPLE1 = [0, 17, 38, 63, 64, 90, 111, 127]  # states of the 128-wide batch
+SAMPLE0 = [0, 9, 22, 31]
+
+
+class _Sys:
+    pass
+
+
+def _build(cfg, cuda):
+    import torch
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    from oracle import oracle as O
+    s = _Sys()
+    s.cfg = cfg
+    m = cfg.mesh
+    w = laplacian_weights(m.spacing)
+    s.dm = lib.DeviceMesh(m)
+    s.ham = lib.Hamiltonian(s.dm, w, star_points(), v=cfg.v, projectors=cfg.proj)
+    P = None if cfg.proj is None else O.Projectors(cfg.proj.maps, cfg.proj.mats, cfg.proj.scals)
+    s.oracle = O.Hamiltonian(m, w, star_points(), v=cfg.v, projectors=P)
+    s.x = torch.from_numpy(cfg.psi).to(cuda)
+    return s
+
+
+@pytest.fixture(scope="module")
+def sphere128(cuda):
+    from hpsi import fixtures
+    return _build(fixtures.config1(), cuda)
+
+
+@pytest.fixture(scope="module")
+def box64(cuda):
+    from hpsi import fixtures
+    return _build(fixtures.config0(), cuda)
+
+
+def _check_apply(s, sample, dtype, tol):
+    import torch
+    m = s.cfg.mesh
+    nst = s.cfg.psi.shape[1]
+    x = s.x if dtype == torch.complex128 else s.x.to(dtype)
+    y = torch.zeros((m.np, nst), dtype=dtype, device=x.device)
+    s.ham.apply(x, y)
+    got = y[:, sample].cpu().numpy().astype(np.complex128)
+    ref = s.oracle.apply(np.ascontiguousarray(s.cfg.psi[:, sample]))
+    err = rel_maxnorm_per_state(got, ref)
+    assert err <= tol, f"relative max-norm {err:.3e}"
+    return y
+
+
+def _check_taylor(s, sample, dtype, tol, dt):
+    import torch
+    m = s.cfg.mesh
+    x = s.x.clone() if dtype == torch.complex128 else s.x.to(dtype)
+    n0 = s.dm.nrm2(x)
+    s.ham.taylor_step(x, dt)
+    got = x[: m.np, sample].cpu().numpy().astype(np.complex128)
+    ref = s.oracle.taylor(np.ascontiguousarray(s.cfg.psi[:, sample]), dt)
+    err = rel_maxnorm_per_state(got, ref)
+    assert err <= tol, f"relative max-norm {err:.3e}"
+    # whole batch: the norm change of every state (the truncated series is
+    # not unitary at these dt) stays of the size the oracle shows for the
+    # sampled states, statistically alike
+    n1 = s.dm.nrm2(x)
+    ch = np.abs(n1 - n0) / n0
+    ref_ch = np.abs(np.sqrt(np.sum(np.abs(ref) ** 2, axis=0) * m.vol_pp) - n0[sample]) / n0[sample]
+    assert np.all(np.isfinite(n1))
+    assert np.max(np.abs(ch[sample] - ref_ch)) <= (1e-12 if dtype == torch.complex128 else 1e-5)
+    assert np.max(ch) <= 10.0 * np.max(ref_ch) + 1e-12
+
+
+def test_sphere128_hpsi_fp64(sphere128):
+    import torch
+    y = _check_apply(sphere128, SAMPLE1, torch.complex128, TOL64)
+    # H is Hermitian on the inner points: <a|H b> = conj(<b|H a>) for sampled
+    # pairs (the zero boundary holds the whole batch to the same operator)
+    m = sphere128.cfg.mesh
+    a, b = SAMPLE1[1], SAMPLE1[-2]
+    xa = sphere128.x[: m.np, a]
+    xb = sphere128.x[: m.np, b]
+    lhs = torch.vdot(xa, y[:, b]).item()
+    rhs = np.conj(torch.vdot(xb, y[:, a]).item())
+    # Cauchy-Schwarz bound of the summed terms: the scale of the rounding
+    scale = (xa.norm() * y[:, b].norm() + xb.norm() * y[:, a].norm()).item()
+    assert abs(lhs - rhs) <= 1e-12 * scale
+
+
+def test_sphere128_hpsi_fp32(sphere128):
+    import torch
+    _check_apply(sphere128, SAMPLE1, torch.complex64, TOL32)
+
+
+def test_sphere128_taylor_fp64(sphere128):
+    import torch
+    _check_taylor(sphere128, SAMPLE1, torch.complex128, TOL64, 0.005)
+
+
+def test_sphere128_taylor_fp32(sphere128):
+    import torch
+    _check_taylor(sphere128, SAMPLE1, torch.complex64, TOL32, 0.005)
+
+
+def test_box64_hpsi_fp64(box64):
+    import torch
+    _check_apply(box64, SAMPLE0, torch.complex128, TOL64)
+
+
+def test_box64_hpsi_fp32(box64):
+    import torch
+    _check_apply(box64, SAMPLE0, torch.complex64, TOL32)
+
+
+def test_box64_taylor_fp64(box64):
+    import torch
+    _check_taylor(box64, SAMPLE0, torch.complex128, TOL64, 0.01)
+
+
+def test_box64_taylor_fp32(box64):
+    import torch
+    _check_taylor(box64, SAMPLE0, torch.complex64, TOL32, 0.01)

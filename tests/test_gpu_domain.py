@@ -165,6 +165,51 @@ def test_partitioned_hpsi_with_kb_equals_global(cuda, nparts, ld, dtype):
         assert np.max(np.abs(got - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_partitioned_hpsi_with_projector_phases_equals_global(cuda, dtype):
+    """k != 0 on partitions: DomainHamiltonian restricts the global projector
+    phases to each partition's sphere points; the summed projection shares
+    and each partition's ket give the global H psi with phases."""
+    import torch
+    from hpsi import lib
+    from hpsi.domain import DomainHamiltonian, partition_z
+    from hpsi.stencil import laplacian_weights, star_points
+    nst, ld, nparts = 16, 16, 3
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    m, v, proj, psi = small_sphere_system(seed=43, nst=nst, radius=4.5, natoms=4)
+    rng = np.random.default_rng(44)
+    ph = [np.exp(1j * rng.uniform(0, 2 * np.pi, len(mp))) for mp in proj.maps]
+    w = laplacian_weights(m.spacing)
+    H = lib.Hamiltonian(lib.DeviceMesh(m), w, star_points(), v=v, projectors=proj)
+    H.set_projector_phases(ph)
+    x = torch.from_numpy(np.ascontiguousarray(psi)).to(cuda).to(tdt)
+    y = torch.zeros((m.np, ld), dtype=tdt, device=cuda)
+    H.apply(x, y)
+    ref = y.cpu().numpy()
+    doms = partition_z(m, nparts)
+    hams = [DomainHamiltonian(d, w, star_points(), v_global=v, projectors=proj, projector_phases=ph)
+            for d in doms]
+    locs = []
+    for d in doms:
+        b = d.local_batch(psi)
+        b[d.np_local: d.np_local + d.np_ghost] = 0.0
+        locs.append(torch.from_numpy(b).to(cuda).to(tdt))
+    _exchange_on_one_gpu(doms, locs, nst)
+    shares = []
+    for hm, b in zip(hams, locs):
+        pr = torch.zeros((hm.nprojections, ld), dtype=tdt, device=cuda)
+        hm.ham.projector_bra(b, pr)
+        shares.append(pr)
+    total = torch.stack(shares).sum(0)
+    tol = 1e-13 if dtype == "c128" else 2e-6
+    for d, hm, b in zip(doms, hams, locs):
+        out = torch.zeros((d.np_local, ld), dtype=tdt, device=cuda)
+        hm.ham.apply(b, out, terms=lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL, set_bc=False)
+        hm.ham.projector_ket(total, out)
+        got = out.cpu().numpy()
+        assert np.max(np.abs(got - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+
+
 def test_projector_bra_rejects_host_buffers(cuda):
     import torch
     from hpsi import lib

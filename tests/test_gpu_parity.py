@@ -256,3 +256,31 @@ def test_nonfinite_detected(cuda):
     with pytest.raises(lib.HpsiError) as e:
         ham.taylor_step(x, 0.02, observables=True)
     assert e.value.status == 3
+
+
+def test_update_vloc_is_stream_ordered(cuda):
+    """hpsi_hamiltonian_update_vloc on a side stream (host input, then a
+    device tensor), each followed by H psi on the same stream with no host
+    synchronisation between them, against the oracle with that potential."""
+    import torch
+    from hpsi import lib
+    m, v, proj, psi = small_sphere_system(seed=91, nst=8)
+    dm, ham, w, pts = _setup(m, v=None, proj=proj)
+    x = torch.from_numpy(psi).to(cuda)
+    st = torch.cuda.Stream()
+    v2 = torch.from_numpy(2.0 * v - 0.5).to(cuda)
+    outs = []
+    with torch.cuda.stream(st):
+        for vv in (v, v2):
+            ham.update_vloc(vv, stream=st)
+            y = torch.zeros((m.np, 8), dtype=torch.complex128, device=cuda)
+            ham.apply(x, y, stream=st)
+            outs.append(y)
+    st.synchronize()
+    for y, vv in zip(outs, (v, 2.0 * v - 0.5)):
+        ref = _oracle(m, w, pts, v=vv, proj=proj).apply(psi)
+        assert rel_maxnorm_per_state(y.cpu().numpy(), ref) <= TOL64
+    with pytest.raises(lib.HpsiError):
+        bad = v.copy()
+        bad[3] = np.nan
+        ham.update_vloc(bad)
