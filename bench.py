@@ -578,6 +578,12 @@ def main():
     ms_t64 = timed(lambda: ham.taylor_step(xt, 0.02), tk, 1)
     xt32 = x32.clone()
     ms_t32 = timed(lambda: ham.taylor_step(xt32, 0.02), tk, 1)
+    # the Taylor step with the density of the propagated batch fused into its
+    # last pass (the fuse_density_exp_apply of the reference's propagation)
+    rho_t = torch.zeros(m.np, dtype=torch.float64, device=dev)
+    wts = np.full(nst, 2.0)
+    ms_td = timed(lambda: ham.taylor_step_density(xt, 0.02, wts, rho=rho_t), tk, 1)
+    ms_rho = timed(lambda: dm.density(xt, wts, rho=rho_t), tk, 1)
     del xt, xt32
 
     # ---- TD steps (exp_mid + laser): FP64 plain launches vs FP32 graph replay --
@@ -661,6 +667,8 @@ def main():
                 "fp32_storage_hpsi": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps},
                 "taylor4_fp64": {"steps_per_s": tk / (ms_t64 / 1e3), "ms_per_step": ms_t64 / tk},
                 "taylor4_fp32": {"steps_per_s": tk / (ms_t32 / 1e3), "ms_per_step": ms_t32 / tk},
+                "taylor4_fp64_with_density": {"ms_per_step_fused": ms_td / tk,
+                                              "ms_density_pass_alone": ms_rho / tk},
                 **td,
                 "config0_box64": box,
                 "config3_group": group,

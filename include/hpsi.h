@@ -213,6 +213,23 @@ hpsi_status hpsi_taylor_step(hpsi_hamiltonian *ham, hpsi_batch *psi, double dt_r
                              double dt_im, int32_t order, double *energy,
                              double *dipole, double *norm2, void *stream);
 
+/* The Taylor step followed by the density of the propagated batch, as
+ * propagation_ops_elec_fuse_density_exp_apply does per block
+ * (src/td/propagation_ops_elec.F90:261-333, density_calc_accumulate,
+ * src/states/density.F90:279-362):
+ *   psi <- exp(-i dt H) psi (order-`order` Taylor series, as hpsi_taylor_step),
+ *   rho[ip] = (accumulate ? rho[ip] : 0) + sum_i weight[i] |psi_i(ip)|^2.
+ * The density is fused into the last Horner pass, which writes the
+ * propagated rows, and into its KB ket for the rows the projectors cover (no
+ * extra read of the batch); batch widths the register-blocked pass does not
+ * take get one density pass after the step.  FP64 sums in a fixed order.
+ * weight: nst host doubles (kweight x occupation), read before the call
+ * returns; psi and rho (np doubles) device memory; stream ordered. */
+hpsi_status hpsi_taylor_step_density(hpsi_hamiltonian *ham, hpsi_batch *psi,
+                                     double dt_re, double dt_im, int32_t order,
+                                     const double *weight, double *rho,
+                                     int32_t accumulate, void *stream);
+
 /* exponential_apply_batch with its second output (psib2 / deltat2,
  * src/electrons/exponential.F90:695-744, used by the self-consistent ETRS
  * predictor): psi2 <- exp(-i dt2 H) psi, psi <- exp(-i dt H) psi, both by the
@@ -319,6 +336,51 @@ hpsi_status hpsi_adjoint_gradient(hpsi_hamiltonian *ham, const hpsi_batch *psi0,
                                   const double pol[3], int32_t ckpt, double *J_out,
                                   double *grad_eps, double *grad_v,
                                   double *grad_eps_cont, void *stream);
+
+/* The same adjoint one step at a time, for a host that drives the backward
+ * propagation itself (bwd_step / bwd_step_2,
+ * src/opt_control/propagation.F90:477-783, with its own update_field,
+ * :1016-1103, between steps).  Step n of the forward run is
+ * psi_{n+1} = T_n psi_n with T_n = sum_{k<=order} (-i dt H_n)^k / k! and
+ * H_n = H + eps_n pol.r (the Hamiltonian's local potential, kinetic and KB
+ * terms as set; the field of set_field is not used and is left unchanged).
+ *
+ * hpsi_adjoint_step: lambda <- T_n^dagger lambda in place (lambda =
+ *   lambda_{n+1} on entry, lambda_n on return; T_n^dagger = T_n(-dt) as H_n is
+ *   Hermitian), given psi_n (not modified).  It also returns the exact
+ *   vector-Jacobian products of this step:
+ *     grad_eps[0]      = dJ/d eps_n = 2 Re sum_{j+m<=order-1} c_{j+m+1}
+ *                        <H_n^j lambda_{n+1}| pol.r |H_n^m psi_n>,
+ *     grad_eps_cont[0] = its leading term 2 Re c_1 <lambda_{n+1}|pol.r|psi_n>
+ *                        (= 2 dt Im <lambda_{n+1}|pol.r|psi_n>, calculate_g),
+ *     grad_v[r]       += dJ/dv(r) contribution of the step (2 dV Re sum ...).
+ *   grad_eps and grad_eps_cont: one double each, host or device, may be NULL
+ *   (host outputs make the call wait for the stream); grad_v: np doubles of
+ *   device memory, accumulated, may be NULL.  complex128 device batches with
+ *   at least np rows and equal nst and ld.  For J = sum_i |<phi_i|psi_i(N)>|^2
+ *   the backward run starts from lambda_N = phi_i <phi_i|psi_i(N)> and calls
+ *   this for n = N-1 .. 0; the summed results equal hpsi_adjoint_gradient.
+ *   The first call on a handle allocates its scratch (2 order - 1 batches).
+ * hpsi_vjp_field: out[2i], out[2i+1] = Re, Im of dV sum_r conj(chi_i(r))
+ *   (pol.r) psi_i(r) for every state i (host or device, 2 nst doubles): the
+ *   dipole-coupling matrix element calculate_g sums
+ *   (src/opt_control/propagation.F90:932-998, vlaser_operator_linear).
+ * hpsi_vjp_vloc: grad_v[r] = (accumulate ? grad_v[r] : 0)
+ *   + scale * sum_i Re(conj(lambda_i(r)) psi_i(r)) over the inner rows
+ *   (device, np doubles): the local-potential VJP of one H application.
+ * Both VJPs take complex128 or complex64 device batches (FP64 sums) and are
+ * stream ordered. */
+hpsi_status hpsi_adjoint_step(hpsi_hamiltonian *ham, hpsi_batch *lambda,
+                              const hpsi_batch *psi_n, double eps_n,
+                              const double pol[3], double dt, int32_t order,
+                              double *grad_eps, double *grad_eps_cont,
+                              double *grad_v, void *stream);
+hpsi_status hpsi_vjp_field(hpsi_hamiltonian *ham, const hpsi_batch *chi,
+                           const hpsi_batch *psi, const double pol[3],
+                           double *out, void *stream);
+hpsi_status hpsi_vjp_vloc(hpsi_hamiltonian *ham, const hpsi_batch *lambda,
+                          const hpsi_batch *psi, double scale, double *grad_v,
+                          int32_t accumulate, void *stream);
 
 /* ------------------------------------------------------------------ */
 /* FP64 reductions over the np inner points (dV = vol_pp), results in host

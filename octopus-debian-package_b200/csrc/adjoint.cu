@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256) adj_accumulate_kernel(double2 *L0, const 
       wc += __shfl_xor_sync(0xffffffffu, wc, off);
     }
     if (lane == 0) {
-      gv[r] += 2.0 * dv * wr;
+      if (gv) gv[r] += 2.0 * dv * wr;
       kadd(ke, 2.0 * dv * wr * zrow[r]);
       kadd(kc, 2.0 * dv * wc * zrow[r]);
     }
@@ -147,6 +147,95 @@ __global__ void adj_init_lambda(double2 *lam, const double2 *phi, long long ldph
   lam[i] = make_double2(f.x * ar - f.y * ai, f.x * ai + f.y * ar);
 }
 
+// pol . r of every inner row (cell coordinates of the padded box)
+__global__ void zrow_kernel(const int *cell_of_row, int np, int NX, int NY, int lo0, int lo1, int lo2, double h0,
+                            double h1, double h2, double p0, double p1, double p2, double *z) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= np) return;
+  const int c = cell_of_row[r];
+  const int x = c % NX, y = (c / NX) % NY, zz = c / (NX * NY);
+  z[r] = p0 * (x + lo0) * h0 + p1 * (y + lo1) * h1 + p2 * (zz + lo2) * h2;
+}
+
+// Per-state partial sums of conj(chi_i(r)) z(r) psi_i(r) over the rows a
+// block visits: blockDim = (tx states, ty rows); compensated per thread, the
+// ty row groups folded in a fixed order.  partial[block][state] = {re s, re c,
+// im s, im c}.
+template <typename T>
+__global__ void vjp_field_kernel(const T *chi, long long ldc, const T *psi, long long ldp, const double *z, int np,
+                                 int nst, double *partial) {
+  extern __shared__ double red[];  // ty * tx * 4
+  const int tx = blockDim.x, ty = blockDim.y;
+  for (int s0 = 0; s0 < nst; s0 += tx) {
+    const int s = s0 + threadIdx.x;
+    Kahan re = {0, 0}, im = {0, 0};
+    if (s < nst)
+      for (long long r = (long long)blockIdx.x * ty + threadIdx.y; r < np; r += (long long)gridDim.x * ty) {
+        const double cr = chi[2 * (r * ldc + s)], ci = chi[2 * (r * ldc + s) + 1];
+        const double pr = psi[2 * (r * ldp + s)], pi = psi[2 * (r * ldp + s) + 1];
+        const double zr = z[r];
+        kadd(re, zr * (cr * pr + ci * pi));
+        kadd(im, zr * (cr * pi - ci * pr));
+      }
+    double *o = red + 4 * (threadIdx.y * tx + threadIdx.x);
+    o[0] = re.s;
+    o[1] = re.c;
+    o[2] = im.s;
+    o[3] = im.c;
+    __syncthreads();
+    if (threadIdx.y == 0 && s < nst) {
+      Kahan a = {0, 0}, b = {0, 0};
+      for (int y = 0; y < ty; ++y) {
+        const double *q = red + 4 * (y * tx + threadIdx.x);
+        kadd(a, q[0]);
+        a.c += q[1];
+        kadd(b, q[2]);
+        b.c += q[3];
+      }
+      double *d = partial + 4 * ((long long)blockIdx.x * nst + s);
+      d[0] = a.s;
+      d[1] = a.c;
+      d[2] = b.s;
+      d[3] = b.c;
+    }
+    __syncthreads();
+  }
+}
+
+// out[2 i] + i out[2 i + 1] = scale * sum over the blocks' partials of state i
+__global__ void vjp_field_finalize(const double *partial, int nblk, int nst, double scale, double *out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nst) return;
+  Kahan a = {0, 0}, b = {0, 0};
+  for (int k = 0; k < nblk; ++k) {
+    const double *q = partial + 4 * ((long long)k * nst + s);
+    kadd(a, q[0]);
+    a.c += q[1];
+    kadd(b, q[2]);
+    b.c += q[3];
+  }
+  out[2 * s] = scale * (a.s + a.c);
+  out[2 * s + 1] = scale * (b.s + b.c);
+}
+
+// g[r] = (acc ? g[r] : 0) + scale * sum_i Re(conj(lam_i(r)) psi_i(r)): one warp
+// per row, states over the lanes, a fixed shuffle order
+template <typename T>
+__global__ void vjp_vloc_kernel(const T *lam, long long ldl, const T *psi, long long ldp, int np, int nst,
+                                double scale, int acc, double *g) {
+  const int lane = threadIdx.x & 31;
+  const long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= np) return;
+  double w = 0.0;
+  for (int s = lane; s < nst; s += 32) {
+    const double lr = lam[2 * (r * ldl + s)], li = lam[2 * (r * ldl + s) + 1];
+    const double pr = psi[2 * (r * ldp + s)], pi = psi[2 * (r * ldp + s) + 1];
+    w += lr * pr + li * pi;
+  }
+  for (int off = 16; off > 0; off >>= 1) w += __shfl_xor_sync(0xffffffffu, w, off);
+  if (lane == 0) g[r] = (acc ? g[r] : 0.0) + scale * w;
+}
+
 }  // namespace
 
 struct AdjointRun {
@@ -166,6 +255,78 @@ static hpsi_status adj_apply(const AdjointRun &R, double eps, const double2 *in,
 static hpsi_status adj_step_forward(const AdjointRun &R, double eps, double2 *psi) {
   for (int a = 0; a < 3; ++a) R.h->fld[a] = R.pol[a] * eps;
   return taylor_dev<double>(R.h, reinterpret_cast<double *>(psi), R.ld, R.nst, R.dt, 0.0, R.K, nullptr, R.st);
+}
+
+// Scratch of one backward step: H^k lambda (k = 1..K), H^m psi (m = 1..K-1),
+// z per row and the block partials.
+struct AdjStepBufs {
+  double2 *L[KMAX + 1];
+  double2 *P[KMAX];
+  double *zrow, *part, *partc;
+};
+constexpr int ADJ_NBLK = 296;
+
+static size_t adj_step_bytes(const hpsi_mesh *m, long long ld, int K) {
+  const size_t batch = size_t(m->np) * ld;
+  return batch * size_t(2 * K - 1) * sizeof(double2) + (size_t(m->np) + 4 * ADJ_NBLK + 8) * sizeof(double);
+}
+
+static AdjStepBufs adj_step_carve(void *base, const hpsi_mesh *m, long long ld, int K) {
+  AdjStepBufs B;
+  std::memset(&B, 0, sizeof(B));
+  const size_t batch = size_t(m->np) * ld;
+  double2 *q = static_cast<double2 *>(base);
+  for (int k = 1; k <= K; ++k, q += batch) B.L[k] = q;
+  for (int k = 1; k < K; ++k, q += batch) B.P[k] = q;
+  B.zrow = reinterpret_cast<double *>(q);
+  B.part = B.zrow + m->np;
+  B.partc = B.part + 2 * ADJ_NBLK;
+  return B;
+}
+
+static hpsi_status adj_zrow(const hpsi_mesh *m, const double pol[3], double *z, cudaStream_t st) {
+  const CellBox &b = m->box;
+  zrow_kernel<<<(m->np + 255) / 256, 256, 0, st>>>(m->d_cell_of_row, m->np, b.NX, b.NY, b.lo[0], b.lo[1], b.lo[2],
+                                                  b.h[0], b.h[1], b.h[2], pol[0], pol[1], pol[2], z);
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
+}
+
+// One backward step of the exact discrete adjoint: lam <- T_n^dagger lam in
+// place (lam = lambda_{n+1} on entry), with psi = psi_n the state the forward
+// step n started from; adds the step's dJ/d eps_n into geps[0] and the
+// leading (continuous-adjoint) term into gcont[0] (device scalars, written),
+// and dJ/dv(r) into gv (device, accumulated; may be null).  B.zrow holds
+// pol . r.
+static hpsi_status adjoint_step_dev(const AdjointRun &R, double eps, double2 *lam, const double2 *psi,
+                                    const AdjStepBufs &B, double *geps, double *gcont, double *gv) {
+  AdjCoef coef;
+  coef.K = R.K;
+  std::complex<double> ck(1.0, 0.0);
+  for (int k = 0; k <= R.K; ++k) {
+    if (k > 0) ck *= std::complex<double>(0.0, -R.dt) / double(k);
+    coef.cre[k] = ck.real();
+    coef.cim[k] = ck.imag();
+  }
+  AdjPtrs ptr;
+  std::memset(&ptr, 0, sizeof(ptr));
+  ptr.L[0] = lam;
+  ptr.P[0] = psi;
+  for (int k = 1; k <= R.K; ++k) ptr.L[k] = B.L[k];
+  for (int k = 1; k < R.K; ++k) ptr.P[k] = B.P[k];
+  hpsi_status s = HPSI_OK;
+  for (int k = 1; k < R.K && !s; ++k) s = adj_apply(R, eps, ptr.P[k - 1], B.P[k]);
+  for (int k = 1; k <= R.K && !s; ++k) s = adj_apply(R, eps, ptr.L[k - 1], B.L[k]);
+  if (s) return s;
+  const double dv = R.h->mesh->box.h[0] * R.h->mesh->box.h[1] * R.h->mesh->box.h[2];
+  adj_accumulate_kernel<<<ADJ_NBLK, 256, 0, R.st>>>(lam, ptr, R.ld, R.nst, R.np, coef, B.zrow, dv, gv, B.part,
+                                                     B.partc);
+  HPSI_CHECK_LAUNCH();
+  adj_sum_partials<<<1, 32, 0, R.st>>>(B.part, ADJ_NBLK, geps);
+  HPSI_CHECK_LAUNCH();
+  adj_sum_partials<<<1, 32, 0, R.st>>>(B.partc, ADJ_NBLK, gcont);
+  HPSI_CHECK_LAUNCH();
+  return HPSI_OK;
 }
 
 }  // namespace hpsi
@@ -202,38 +363,27 @@ extern "C" hpsi_status hpsi_adjoint_gradient(hpsi_hamiltonian *h, const hpsi_bat
   const size_t batch = size_t(m->np) * R.ld;  // complex numbers of one batch
   const int nseg = (nsteps + ckpt - 1) / ckpt;
   const int seglen = std::min(ckpt, nsteps);
-  const int nblk = 296;
-  // complex buffers: checkpoints nseg, segment seglen, L[K+1], P[1..K-1]
-  const size_t ncplx = batch * (size_t(nseg) + seglen + (order + 1) + order);
-  // doubles: zrow np, gv np, 2 partials 2*nblk each, ov 2*ld, ov partial 4*ld, geps nsteps, gcont nsteps
-  const size_t ndbl = size_t(m->np) * 2 + 4 * size_t(nblk) + 6 * size_t(R.ld) + 2 * size_t(nsteps) + 8;
-  hpsi_status s = h->adjbuf.ensure(ncplx * sizeof(double2) + ndbl * sizeof(double));
+  // complex buffers: checkpoints nseg, segment seglen, lambda; then the step
+  // scratch; doubles: gv np, ov 2*ld, ov partial 4*ld, geps nsteps, gcont nsteps
+  const size_t ncplx = batch * (size_t(nseg) + seglen + 1);
+  const size_t ndbl = size_t(m->np) + 6 * size_t(R.ld) + 2 * size_t(nsteps) + 8;
+  const size_t stepb = adj_step_bytes(m, R.ld, order);
+  hpsi_status s = h->adjbuf.ensure(ncplx * sizeof(double2) + ndbl * sizeof(double) + 256 + stepb);
   if (s) return s;
   double2 *ckp = static_cast<double2 *>(h->adjbuf.ptr);
   double2 *seg = ckp + batch * nseg;
   double2 *Lb = seg + batch * seglen;
-  double2 *Pb = Lb + batch * (order + 1);
-  double *zrow = reinterpret_cast<double *>(Pb + batch * order);
-  double *gv = zrow + m->np;
-  double *part = gv + m->np;
-  double *partc = part + 2 * nblk;
-  double *ov = partc + 2 * nblk;     // 2*ld
+  double *gv = reinterpret_cast<double *>(Lb + batch);
+  double *ov = gv + m->np;           // 2*ld
   double *ovpart = ov + 2 * R.ld;    // 4*ld (state_sum partial of one block)
   double *geps = ovpart + 4 * R.ld;  // nsteps
   double *gcont = geps + nsteps;     // nsteps
-
-  // Z = pol . r per inner row
-  {
-    std::vector<double> z(m->np);
-    for (int r = 0; r < m->np; ++r) {
-      const int c = m->cell_of_row_h[r];
-      const int x = c % m->box.NX, y = (c / m->box.NX) % m->box.NY, zz = c / (m->box.NX * m->box.NY);
-      z[r] = pol[0] * (x + m->box.lo[0]) * m->box.h[0] + pol[1] * (y + m->box.lo[1]) * m->box.h[1] +
-             pol[2] * (zz + m->box.lo[2]) * m->box.h[2];
-    }
-    HPSI_TRY_CUDA(cudaMemcpyAsync(zrow, z.data(), z.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    HPSI_TRY_CUDA(cudaStreamSynchronize(st));
-  }
+  // the step scratch starts on the next 256-byte boundary (room reserved above)
+  void *stepbase = reinterpret_cast<void *>((reinterpret_cast<uintptr_t>(gcont + nsteps + 8) + 255) &
+                                            ~uintptr_t(255));
+  const AdjStepBufs B = adj_step_carve(stepbase, m, R.ld, order);
+  s = adj_zrow(m, pol, B.zrow, st);
+  if (s) return s;
   HPSI_TRY_CUDA(cudaMemsetAsync(gv, 0, size_t(m->np) * sizeof(double), st));
   const double dv = m->box.h[0] * m->box.h[1] * m->box.h[2];
   const double save_fld[3] = {h->fld[0], h->fld[1], h->fld[2]};
@@ -269,21 +419,6 @@ extern "C" hpsi_status hpsi_adjoint_gradient(hpsi_hamiltonian *h, const hpsi_bat
                                                                 targets->ld, R.ld, R.nst, m->np, ov);
     HPSI_CHECK_LAUNCH();
   }
-  // coefficients c_k = (-i dt)^k / k!
-  AdjCoef coef;
-  coef.K = order;
-  {
-    std::complex<double> ck(1.0, 0.0);
-    for (int k = 0; k <= order; ++k) {
-      if (k > 0) ck *= std::complex<double>(0.0, -dt) / double(k);
-      coef.cre[k] = ck.real();
-      coef.cim[k] = ck.imag();
-    }
-  }
-  AdjPtrs ptr;
-  std::memset(&ptr, 0, sizeof(ptr));
-  for (int k = 0; k <= order; ++k) ptr.L[k] = Lb + batch * k;
-  for (int k = 1; k < order; ++k) ptr.P[k] = Pb + batch * k;
 
   // ---- backward, one checkpoint segment at a time --------------------------------
   for (int sgi = nseg - 1; sgi >= 0; --sgi) {
@@ -297,17 +432,8 @@ extern "C" hpsi_status hpsi_adjoint_gradient(hpsi_hamiltonian *h, const hpsi_bat
       if (s) return fail(s);
     }
     for (int n = n1 - 1; n >= n0; --n) {
-      ptr.P[0] = seg + batch * (n - n0);
-      for (int k = 1; k < order && !s; ++k) s = adj_apply(R, eps[n], ptr.P[k - 1], const_cast<double2 *>(ptr.P[k]));
-      for (int k = 1; k <= order && !s; ++k)
-        s = adj_apply(R, eps[n], ptr.L[k - 1], const_cast<double2 *>(ptr.L[k]));
+      s = adjoint_step_dev(R, eps[n], Lb, seg + batch * (n - n0), B, geps + n, gcont + n, gv);
       if (s) return fail(s);
-      adj_accumulate_kernel<<<nblk, 256, 0, st>>>(Lb, ptr, R.ld, R.nst, m->np, coef, zrow, dv, gv, part, partc);
-      HPSI_CHECK_LAUNCH();
-      adj_sum_partials<<<1, 32, 0, st>>>(part, nblk, geps + n);
-      HPSI_CHECK_LAUNCH();
-      adj_sum_partials<<<1, 32, 0, st>>>(partc, nblk, gcont + n);
-      HPSI_CHECK_LAUNCH();
     }
   }
   if (grad_eps) HPSI_TRY_CUDA(cudaMemcpyAsync(grad_eps, geps, nsteps * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -316,5 +442,132 @@ extern "C" hpsi_status hpsi_adjoint_gradient(hpsi_hamiltonian *h, const hpsi_bat
   if (grad_v) HPSI_TRY_CUDA(cudaMemcpyAsync(grad_v, gv, size_t(m->np) * sizeof(double), cudaMemcpyDeviceToHost, st));
   HPSI_TRY_CUDA(cudaStreamSynchronize(st));
   for (int a = 0; a < 3; ++a) h->fld[a] = save_fld[a];
+  return HPSI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Per-step primitives for a host-driven backward propagation (bwd_step /
+// bwd_step_2, src/opt_control/propagation.F90:477-783).
+
+static hpsi_status adj_check_pair(const hpsi_mesh *m, const hpsi_batch *a, const hpsi_batch *b, bool c128_only,
+                                  const char *who) {
+  if (!a || !b || !a->ptr || !b->ptr || a->dtype != b->dtype || a->nst != b->nst || a->nst < 1 ||
+      a->ld < a->nst || b->ld < b->nst || a->npts < m->np || b->npts < m->np || !is_device_ptr(a->ptr) ||
+      !is_device_ptr(b->ptr) || (a->dtype != HPSI_C128 && a->dtype != HPSI_C64) ||
+      (c128_only && a->dtype != HPSI_C128)) {
+    set_error(std::string(who) + ": two device batches of one dtype" + (c128_only ? " (complex128)" : "") +
+              ", equal nst and at least np rows expected");
+    return HPSI_ERR_ARG;
+  }
+  return HPSI_OK;
+}
+
+extern "C" hpsi_status hpsi_adjoint_step(hpsi_hamiltonian *h, hpsi_batch *lambda, const hpsi_batch *psi_n,
+                                         double eps_n, const double pol[3], double dt, int32_t order,
+                                         double *grad_eps, double *grad_eps_cont, double *grad_v, void *stream) {
+  if (!h || !pol || !(dt > 0.0) || order < 1 || order > KMAX || !std::isfinite(eps_n)) {
+    set_error("hpsi_adjoint_step: bad argument");
+    return HPSI_ERR_ARG;
+  }
+  hpsi_mesh *m = h->mesh;
+  hpsi_status s = adj_check_pair(m, lambda, psi_n, true, "hpsi_adjoint_step");
+  if (s) return s;
+  if (lambda->ld != psi_n->ld) {
+    set_error("hpsi_adjoint_step: lambda and psi_n must have the same ld");
+    return HPSI_ERR_ARG;
+  }
+  if (!h->have_kinetic) {
+    set_error("hpsi_adjoint_step: kinetic weights not set");
+    return HPSI_ERR_STATE;
+  }
+  if (grad_v && !is_device_ptr(grad_v)) {
+    set_error("hpsi_adjoint_step: grad_v must be device memory (np doubles, accumulated)");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  AdjointRun R{h, lambda->ld, lambda->nst, m->np, order, dt, {pol[0], pol[1], pol[2]}, st};
+  const size_t stepb = adj_step_bytes(m, R.ld, order);
+  s = h->adjstep.ensure(stepb + 4 * sizeof(double));
+  if (s) return s;
+  const AdjStepBufs B = adj_step_carve(h->adjstep.ptr, m, R.ld, order);
+  double *g2 = reinterpret_cast<double *>(static_cast<char *>(h->adjstep.ptr) + stepb);
+  s = adj_zrow(m, pol, B.zrow, st);
+  if (s) return s;
+  const double save_fld[3] = {h->fld[0], h->fld[1], h->fld[2]};
+  s = adjoint_step_dev(R, eps_n, static_cast<double2 *>(lambda->ptr), static_cast<const double2 *>(psi_n->ptr), B,
+                       g2, g2 + 1, grad_v);
+  for (int a = 0; a < 3; ++a) h->fld[a] = save_fld[a];
+  if (s) return s;
+  bool host_out = false;
+  for (double *o : {grad_eps, grad_eps_cont})
+    if (o) {
+      HPSI_TRY_CUDA(cudaMemcpyAsync(o, o == grad_eps ? g2 : g2 + 1, sizeof(double), cudaMemcpyDefault, st));
+      host_out = host_out || !is_device_ptr(o);
+    }
+  if (host_out) HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  return HPSI_OK;
+}
+
+extern "C" hpsi_status hpsi_vjp_field(hpsi_hamiltonian *h, const hpsi_batch *chi, const hpsi_batch *psi,
+                                      const double pol[3], double *out, void *stream) {
+  if (!h || !pol || !out) {
+    set_error("hpsi_vjp_field: bad argument");
+    return HPSI_ERR_ARG;
+  }
+  hpsi_mesh *m = h->mesh;
+  hpsi_status s = adj_check_pair(m, chi, psi, false, "hpsi_vjp_field");
+  if (s) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nst = chi->nst;
+  const int tx = nst >= 32 ? 32 : nst, ty = 256 / tx;
+  const int nblk = std::max(1, std::min(2 * m->num_sms, (m->np + ty - 1) / ty));
+  const size_t part_d = size_t(nblk) * nst * 4, out_d = 2 * size_t(nst);
+  s = h->vjpbuf.ensure((size_t(m->np) + part_d + out_d) * sizeof(double));
+  if (s) return s;
+  double *z = static_cast<double *>(h->vjpbuf.ptr), *part = z + m->np, *res = part + part_d;
+  s = adj_zrow(m, pol, z, st);
+  if (s) return s;
+  const size_t shm = size_t(tx) * ty * 4 * sizeof(double);
+  if (chi->dtype == HPSI_C128)
+    vjp_field_kernel<double><<<nblk, dim3(tx, ty), shm, st>>>(static_cast<const double *>(chi->ptr), chi->ld,
+                                                             static_cast<const double *>(psi->ptr), psi->ld, z,
+                                                             m->np, nst, part);
+  else
+    vjp_field_kernel<float><<<nblk, dim3(tx, ty), shm, st>>>(static_cast<const float *>(chi->ptr), chi->ld,
+                                                            static_cast<const float *>(psi->ptr), psi->ld, z, m->np,
+                                                            nst, part);
+  HPSI_CHECK_LAUNCH();
+  const double dv = m->box.h[0] * m->box.h[1] * m->box.h[2];
+  vjp_field_finalize<<<(nst + 127) / 128, 128, 0, st>>>(part, nblk, nst, dv, res);
+  HPSI_CHECK_LAUNCH();
+  HPSI_TRY_CUDA(cudaMemcpyAsync(out, res, out_d * sizeof(double), cudaMemcpyDefault, st));
+  if (!is_device_ptr(out)) HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  return HPSI_OK;
+}
+
+extern "C" hpsi_status hpsi_vjp_vloc(hpsi_hamiltonian *h, const hpsi_batch *lambda, const hpsi_batch *psi,
+                                     double scale, double *grad_v, int32_t accumulate, void *stream) {
+  if (!h || !grad_v || !std::isfinite(scale)) {
+    set_error("hpsi_vjp_vloc: bad argument");
+    return HPSI_ERR_ARG;
+  }
+  hpsi_mesh *m = h->mesh;
+  hpsi_status s = adj_check_pair(m, lambda, psi, false, "hpsi_vjp_vloc");
+  if (s) return s;
+  if (!is_device_ptr(grad_v)) {
+    set_error("hpsi_vjp_vloc: grad_v must be device memory (np doubles)");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned nb = unsigned((m->np + 7) / 8);
+  if (lambda->dtype == HPSI_C128)
+    vjp_vloc_kernel<double><<<nb, 256, 0, st>>>(static_cast<const double *>(lambda->ptr), lambda->ld,
+                                                static_cast<const double *>(psi->ptr), psi->ld, m->np, lambda->nst,
+                                                scale, accumulate ? 1 : 0, grad_v);
+  else
+    vjp_vloc_kernel<float><<<nb, 256, 0, st>>>(static_cast<const float *>(lambda->ptr), lambda->ld,
+                                               static_cast<const float *>(psi->ptr), psi->ld, m->np, lambda->nst,
+                                               scale, accumulate ? 1 : 0, grad_v);
+  HPSI_CHECK_LAUNCH();
   return HPSI_OK;
 }

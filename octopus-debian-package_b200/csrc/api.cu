@@ -73,6 +73,22 @@ __global__ void scatter_cells_kernel(const double *v, const int *cell_of_row, in
   if (i < n) vcell[cell_of_row[i]] = v[i];
 }
 
+// rho[r] (+)= the density of row r from the fused partials: the KB ket's row
+// sums for covered rows (their final values), the pass's chunk sums elsewhere;
+// fixed summation order.
+__global__ void rho_finalize_kernel(const double *part, int chunks, const double *ket, int kxb, int nk,
+                                    const int *kidx, int np, int acc, double *rho) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= np) return;
+  double v = 0.0;
+  const int k = kidx ? kidx[r] : -1;
+  if (k >= 0)
+    for (int b = 0; b < kxb; ++b) v += ket[(long long)b * nk + k];
+  else
+    for (int c = 0; c < chunks; ++c) v += part[(long long)c * np + r];
+  rho[r] = acc ? rho[r] + v : v;
+}
+
 template <typename T>
 __global__ void boundaries_kernel(T *psi, long long ld, int np, int nb, const int *per_inner, const T *phase,
                                   int periodic) {
@@ -469,6 +485,9 @@ hpsi_status hpsi_hamiltonian_create(hpsi_mesh *mesh, hpsi_hamiltonian **out) {
   if (!mesh || !out) return HPSI_ERR_ARG;
   hpsi_hamiltonian *h = new hpsi_hamiltonian();
   h->mesh = mesh;
+  // experiment override: HPSI_BRA_OVERLAP=0 runs the KB bra on the caller's
+  // stream before the pass
+  if (const char *e = std::getenv("HPSI_BRA_OVERLAP")) h->overlap_bra = std::atoi(e) != 0;
   *out = h;
   return HPSI_OK;
 }
@@ -489,7 +508,13 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   h->adjbuf.release();
   h->lzbuf.release();
   h->vstage.release();
+  h->adjstep.release();
+  h->vjpbuf.release();
+  h->rhobuf.release();
   h->lzsmall.release();
+  if (h->bra_stream) cudaStreamDestroy(h->bra_stream);
+  if (h->bra_fork) cudaEventDestroy(h->bra_fork);
+  if (h->bra_join) cudaEventDestroy(h->bra_join);
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   if (h->capture_event) cudaEventDestroy(h->capture_event);
   if (h->xfer_in) cudaStreamDestroy(h->xfer_in);
@@ -503,6 +528,14 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   return HPSI_OK;
 }
 
+hpsi_status hpsi_hamiltonian::ensure_bra_stream() {
+  if (bra_stream) return HPSI_OK;
+  HPSI_TRY_CUDA(cudaStreamCreateWithFlags(&bra_stream, cudaStreamNonBlocking));
+  HPSI_TRY_CUDA(cudaEventCreateWithFlags(&bra_fork, cudaEventDisableTiming));
+  HPSI_TRY_CUDA(cudaEventCreateWithFlags(&bra_join, cudaEventDisableTiming));
+  return HPSI_OK;
+}
+
 void hpsi_hamiltonian::proj_free() {
   dev_free(d_mat);
   dev_free(d_proj_row);
@@ -512,6 +545,8 @@ void hpsi_hamiltonian::proj_free() {
   dev_free(d_scal);
   dev_free(d_scal_f);
   dev_free(d_krows);
+  dev_free(d_kidx);
+  d_kidx = nullptr;
   dev_free(d_kptr);
   dev_free(d_kb_ent);
   dev_free(d_kb_phase);
@@ -747,6 +782,11 @@ hpsi_status hpsi_hamiltonian_set_projectors(hpsi_hamiltonian *h, int32_t nmat, c
   up(reinterpret_cast<void **>(&h->d_scal), scal, size_t(nproj_tot) * sizeof(double));
   up(reinterpret_cast<void **>(&h->d_scal_f), scf.data(), scf.size() * sizeof(float));
   up(reinterpret_cast<void **>(&h->d_krows), krows.data(), krows.size() * sizeof(int));
+  {
+    std::vector<int> kidx(m->np, -1);
+    for (size_t i = 0; i < krows.size(); ++i) kidx[krows[i]] = int(i);
+    up(reinterpret_cast<void **>(&h->d_kidx), kidx.data(), kidx.size() * sizeof(int));
+  }
   up(reinterpret_cast<void **>(&h->d_kptr), kptr.data(), kptr.size() * sizeof(int));
   up(reinterpret_cast<void **>(&h->d_kb_ent), ent.data(), ent.size() * sizeof(int4));
   if (s) {
@@ -932,8 +972,11 @@ hpsi_status run_bra(hpsi_hamiltonian *h, const T *psi, long long ld, T *proj, cu
 
 template <typename T>
 hpsi_status run_ket(hpsi_hamiltonian *h, const T *proj, long long ld, int nst, T *out, long long out_ld, int mode,
-                    double a_re, double a_im, const T *psi0, long long psi0_ld, double *obs, cudaStream_t st) {
+                    double a_re, double a_im, const T *psi0, long long psi0_ld, double *obs, cudaStream_t st,
+                    double *rho_ket = nullptr, const double *rho_w = nullptr) {
   KetArgs k;
+  k.rho_ket = rho_ket;
+  k.rho_w = rho_w;
   k.nk = h->nk;
   k.krows = h->d_krows;
   k.kptr = h->d_kptr;
@@ -1005,11 +1048,19 @@ hpsi_status launch_pass_any(const PassArgs &a, const PassShape &shape, long long
 template hpsi_status launch_pass_any<double>(const PassArgs &, const PassShape &, long long, cudaStream_t);
 template hpsi_status launch_pass_any<float>(const PassArgs &, const PassShape &, long long, cudaStream_t);
 
+// Density of a pass output, fused into the pass (blocked kernel) and the ket.
+struct RhoSpec {
+  const double *w;    // per state weight, ld entries (zero beyond nst)
+  double *part;       // [chunks][np]
+  double *ket;        // [ceil(nst / 64)][nk]
+  bool fused = false;  // set when the pass took it
+};
+
 // One fused pass with its KB bra before and ket after.
 template <typename T>
 hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T *in, long long in_ld, T *out,
                      long long out_ld, long long ld, int mode, const T *psi0, long long psi0_ld, double a_re,
-                     double a_im, double *obs_partial, int *ncta_out, cudaStream_t st) {
+                     double a_im, double *obs_partial, int *ncta_out, cudaStream_t st, RhoSpec *rho = nullptr) {
   PassArgs a;
   const int dtype = sizeof(T) == 8 ? HPSI_C128 : HPSI_C64;
   PassShape shape = pass_shape(h, dtype, ld);
@@ -1028,12 +1079,29 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
     }
   }
   const bool nl = (terms & HPSI_TERM_NON_LOCAL_POTENTIAL) && h->nmat > 0;
+  // The bra reads only psi, like the pass: it runs on the handle's side
+  // stream, forked from and joined back into `st` (a legal fork/join inside a
+  // stream capture too), so that its CTAs fill the SMs the pass leaves idle.
+  bool forked = false;
   if (nl) {
     const size_t pbytes = size_t(h->nprojections) * ld * 2 * sizeof(T);
     hpsi_status s = h->projbuf.ensure(pbytes);
     if (s) return s;
-    s = run_bra<T>(h, in, in_ld, static_cast<T *>(h->projbuf.ptr), st);
-    if (s) return s;
+    cudaStream_t bst = st;
+    if (h->overlap_bra) {
+      s = h->ensure_bra_stream();
+      if (s) return s;
+      HPSI_TRY_CUDA(cudaEventRecord(h->bra_fork, st));
+      HPSI_TRY_CUDA(cudaStreamWaitEvent(h->bra_stream, h->bra_fork, 0));
+      bst = h->bra_stream;
+      forked = true;
+    }
+    s = run_bra<T>(h, in, in_ld, static_cast<T *>(h->projbuf.ptr), bst);
+    if (forked) HPSI_TRY_CUDA(cudaEventRecord(h->bra_join, bst));
+    if (s) {
+      if (forked) cudaStreamWaitEvent(st, h->bra_join, 0);
+      return s;
+    }
   }
   if (obs_partial) {
     a.obs = obs_partial;
@@ -1041,9 +1109,16 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
   }
   if (ncta_out) *ncta_out = a.nitems;
   if (obs_partial && !psi0) a.psi0 = in, a.psi0_ld = in_ld;
+  if (rho && shape.blk && mode == PASS_HORNER && !obs_partial) {
+    a.rho_part = rho->part;
+    a.rho_w = rho->w;
+    rho->fused = true;
+  }
+  const bool rho_fused = rho && rho->fused;
   {
     ProfScope prof(sizeof(T) == 8 ? "pass_fp64" : "pass_fp32", st);
     hpsi_status s = launch_pass_any<T>(a, shape, pass_in_rows(h, src_map), st);
+    if (forked) HPSI_TRY_CUDA(cudaStreamWaitEvent(st, h->bra_join, 0));
     if (s) return s;
   }
   if (nl) {
@@ -1054,7 +1129,8 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
       kobs = static_cast<double *>(h->ketobs.ptr);
     }
     hpsi_status s = run_ket<T>(h, static_cast<const T *>(h->projbuf.ptr), ld, int(ld), out, out_ld, mode, a_re, a_im,
-                               static_cast<const T *>(a.psi0), a.psi0_ld, kobs, st);
+                               static_cast<const T *>(a.psi0), a.psi0_ld, kobs, st, rho_fused ? rho->ket : nullptr,
+                               rho_fused ? rho->w : nullptr);
     if (s) return s;
   }
   return HPSI_OK;
@@ -1069,9 +1145,11 @@ template hpsi_status build_pass_args<float>(hpsi_hamiltonian *, int, const int *
 template hpsi_status run_bra<double>(hpsi_hamiltonian *, const double *, long long, double *, cudaStream_t);
 template hpsi_status run_bra<float>(hpsi_hamiltonian *, const float *, long long, float *, cudaStream_t);
 template hpsi_status run_ket<double>(hpsi_hamiltonian *, const double *, long long, int, double *, long long, int,
-                                     double, double, const double *, long long, double *, cudaStream_t);
+                                     double, double, const double *, long long, double *, cudaStream_t, double *,
+                                     const double *);
 template hpsi_status run_ket<float>(hpsi_hamiltonian *, const float *, long long, int, float *, long long, int,
-                                    double, double, const float *, long long, double *, cudaStream_t);
+                                    double, double, const float *, long long, double *, cudaStream_t, double *,
+                                    const double *);
 
 const int *load_map(const hpsi_hamiltonian *h, int set_bc) {
   const hpsi_mesh *m = h->mesh;
@@ -1138,10 +1216,11 @@ hpsi_status apply_h_dev(hpsi_hamiltonian *h, const T *psi, long long ld, T *hpsi
                      nullptr, nullptr, st);
 }
 
-// Horner form of the order-K Taylor polynomial, K fused passes.
+// Horner form of the order-K Taylor polynomial, K fused passes; with `rho`
+// the last pass (and its ket) also writes the density partials of the result.
 template <typename T>
-hpsi_status taylor_dev(hpsi_hamiltonian *h, T *psi, long long ld, int nst, double dt_re, double dt_im, int order,
-                       double *obs_dev, cudaStream_t st) {
+hpsi_status taylor_dev_impl(hpsi_hamiltonian *h, T *psi, long long ld, int nst, double dt_re, double dt_im,
+                            int order, double *obs_dev, cudaStream_t st, RhoSpec *rho) {
   hpsi_mesh *m = h->mesh;
   const size_t ubytes = size_t(m->np) * ld * 2 * sizeof(T);
   for (auto &w : h->u) {
@@ -1165,7 +1244,8 @@ hpsi_status taylor_dev(hpsi_hamiltonian *h, T *psi, long long ld, int nst, doubl
     T *out = (k == 1 && order > 1) ? psi : ((order - k) % 2 == 0 ? u0 : u1);
     const long long out_ld = (out == psi) ? ld : ld;
     hpsi_status s = run_pass<T>(h, HPSI_TERM_ALL, map, in, in_ld, out, out_ld, ld, PASS_HORNER, psi, ld, are, aim,
-                                k == order ? obs_partial : nullptr, k == order ? &ncta : nullptr, st);
+                                k == order ? obs_partial : nullptr, k == order ? &ncta : nullptr, st,
+                                k == 1 ? rho : nullptr);
     if (s) return s;
     in = out;
     in_ld = out_ld;
@@ -1183,6 +1263,12 @@ hpsi_status taylor_dev(hpsi_hamiltonian *h, T *psi, long long ld, int nst, doubl
     if (s) return s;
   }
   return HPSI_OK;
+}
+
+template <typename T>
+hpsi_status taylor_dev(hpsi_hamiltonian *h, T *psi, long long ld, int nst, double dt_re, double dt_im, int order,
+                       double *obs_dev, cudaStream_t st) {
+  return taylor_dev_impl<T>(h, psi, ld, nst, dt_re, dt_im, order, obs_dev, st, nullptr);
 }
 
 template hpsi_status apply_h_dev<double>(hpsi_hamiltonian *, const double *, long long, double *, long long, int, int,
@@ -1407,6 +1493,74 @@ hpsi_status hpsi_taylor_step(hpsi_hamiltonian *h, hpsi_batch *psi, double dt_re,
     }
   } else if (!dev) {
     HPSI_TRY_CUDA(cudaStreamSynchronize(st));
+  }
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_taylor_step_density(hpsi_hamiltonian *h, hpsi_batch *psi, double dt_re, double dt_im, int32_t order,
+                                     const double *weight, double *rho, int32_t accumulate, void *stream) {
+  if (!h || !weight || !rho) return HPSI_ERR_ARG;
+  hpsi_mesh *m = h->mesh;
+  hpsi_status s = check_batch(m, psi, m->np, "hpsi_taylor_step_density");
+  if (s) return s;
+  if (order < 1 || order > 32 || !std::isfinite(dt_re) || !std::isfinite(dt_im)) {
+    set_error("hpsi_taylor_step_density: order must be 1..32 and dt finite");
+    return HPSI_ERR_ARG;
+  }
+  if (!h->have_kinetic) {
+    set_error("hpsi_taylor_step_density: kinetic weights not set");
+    return HPSI_ERR_STATE;
+  }
+  if (!is_device_ptr(psi->ptr) || !is_device_ptr(rho)) {
+    set_error("hpsi_taylor_step_density: device batch and density expected");
+    return HPSI_ERR_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long long ld = psi->ld;
+  const PassShape sh = pass_shape(h, psi->dtype, ld);
+  const int chunks = int(ld / std::max(1, sh.sc)) + 1;
+  const int kxb = (psi->nst + 63) / 64;
+  const size_t nw = size_t(ld), npart = size_t(chunks) * m->np, nket = size_t(kxb) * std::max(1, h->nk);
+  s = h->rhobuf.ensure((nw + npart + nket) * sizeof(double));
+  if (s) return s;
+  double *w = static_cast<double *>(h->rhobuf.ptr);
+  std::vector<double> wh(nw, 0.0);
+  for (int i = 0; i < psi->nst; ++i) {
+    if (!std::isfinite(weight[i])) {
+      set_error("hpsi_taylor_step_density: non-finite weight");
+      return HPSI_ERR_NONFINITE;
+    }
+    wh[i] = weight[i];
+  }
+  HPSI_TRY_CUDA(cudaMemcpyAsync(w, wh.data(), nw * sizeof(double), cudaMemcpyHostToDevice, st));
+  RhoSpec R;
+  R.w = w;
+  R.part = w + nw;
+  R.ket = R.part + npart;
+  if (psi->dtype == HPSI_C128)
+    s = taylor_dev_impl<double>(h, static_cast<double *>(psi->ptr), ld, psi->nst, dt_re, dt_im, order, nullptr, st,
+                                &R);
+  else
+    s = taylor_dev_impl<float>(h, static_cast<float *>(psi->ptr), ld, psi->nst, dt_re, dt_im, order, nullptr, st,
+                               &R);
+  if (s) return s;
+  if (R.fused) {
+    const bool kb = h->nmat > 0 && h->nk > 0;
+    rho_finalize_kernel<<<(m->np + 255) / 256, 256, 0, st>>>(R.part, int(ld / sh.sc), R.ket, kxb, h->nk,
+                                                             kb ? h->d_kidx : nullptr, m->np, accumulate ? 1 : 0,
+                                                             rho);
+    g_launches++;
+    HPSI_CHECK_LAUNCH();
+  } else {
+    // widths the register-blocked pass does not take: the density kernel
+    // reads the propagated batch once more
+    if (psi->dtype == HPSI_C128)
+      s = launch_density<double>(static_cast<const double *>(psi->ptr), ld, m->np, psi->nst, w, rho,
+                                 accumulate != 0, st);
+    else
+      s = launch_density<float>(static_cast<const float *>(psi->ptr), ld, m->np, psi->nst, w, rho,
+                                accumulate != 0, st);
+    if (s) return s;
   }
   return HPSI_OK;
 }

@@ -77,6 +77,7 @@ struct hpsi_hamiltonian {
   // rows covered by at least one sphere: krows[nk], entries kptr[nk+1] -> kb_ent
   int nk = 0, min_npoints = 0;
   int *d_krows = nullptr, *d_kptr = nullptr;
+  int *d_kidx = nullptr;  // per inner row: its index among the covered rows, or -1
   int4 *d_kb_ent = nullptr;
   // projector phases (k != 0): one complex number per sphere point, or null
   long long kb_npts = 0;
@@ -91,6 +92,11 @@ struct hpsi_hamiltonian {
     double ms = 0.0;
   } tuned[2];
   const double *fld_scale_dev = nullptr;  // set while a TD run replays steps
+  // side stream of the KB bra (forked from the caller's stream, joined before the ket)
+  bool overlap_bra = true;
+  cudaStream_t bra_stream = nullptr;
+  cudaEvent_t bra_fork = nullptr, bra_join = nullptr;
+  hpsi_status ensure_bra_stream();
   cudaStream_t capture_stream = nullptr;  // graph capture / replay stream of TD runs
   cudaEvent_t capture_event = nullptr;
   // host-batch pipeline: copy-in and copy-out streams, per-buffer events
@@ -101,6 +107,8 @@ struct hpsi_hamiltonian {
   // workspaces
   hpsi::Workspace u[2], projbuf, bra_partial, obsbuf, ketobs, small, tdbuf, adjbuf;
   hpsi::Workspace lzbuf, lzsmall;
-  hpsi::Workspace vstage;  // host potential staged for hpsi_hamiltonian_update_vloc  // Lanczos: Krylov vectors, reductions and coefficients
+  hpsi::Workspace vstage;  // host potential staged for hpsi_hamiltonian_update_vloc
+  hpsi::Workspace adjstep, vjpbuf;  // per-step adjoint scratch, field VJP partials
+  hpsi::Workspace rhobuf;  // fused density: weights, pass and ket partials  // Lanczos: Krylov vectors, reductions and coefficients
   void proj_free();
 };

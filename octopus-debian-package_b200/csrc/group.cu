@@ -39,7 +39,8 @@ template <typename T>
 hpsi_status run_bra(hpsi_hamiltonian *h, const T *psi, long long ld, T *proj, cudaStream_t st);
 template <typename T>
 hpsi_status run_ket(hpsi_hamiltonian *h, const T *proj, long long ld, int nst, T *out, long long out_ld, int mode,
-                    double a_re, double a_im, const T *psi0, long long psi0_ld, double *obs, cudaStream_t st);
+                    double a_re, double a_im, const T *psi0, long long psi0_ld, double *obs, cudaStream_t st,
+                    double *rho_ket = nullptr, const double *rho_w = nullptr);
 template <typename T>
 hpsi_status launch_pass(PassArgs a, const PassShape &shape, cudaStream_t st);
 template <typename T>

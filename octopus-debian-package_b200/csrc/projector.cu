@@ -268,7 +268,10 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
   const int per = (k.nk + gridDim.y - 1) / gridDim.y;
   const int r0 = blockIdx.y * per, r1 = min(k.nk, r0 + per);
   for (int i = r0 + threadIdx.y; i < r1; i += 8) {
-    if (!act[0]) continue;
+    // density of the final row (each warp is one row: the shuffle below is
+    // reached by all its lanes, active or not)
+    double rs = 0.0;
+    if (act[0]) {
     const int row = k.krows[i];
     // the output elements are loaded before the sums, so their latency
     // overlaps theirs (prefetching the next row's metadata as well, or four
@@ -333,10 +336,16 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
         y[u].y += h[u].y;
       }
       o[32 * u] = y[u];
+      if (k.rho_ket) rs += k.rho_w[sb + 32 * u] * (double(y[u].x) * double(y[u].x) + double(y[u].y) * double(y[u].y));
       if (k.obs) {
         const C2 x = psi0[(long long)row * k.psi0_ld + sb + 32 * u];
         kadd(ke[u], double(x.x) * double(h[u].x) + double(x.y) * double(h[u].y));
       }
+    }
+    }
+    if (k.rho_ket) {
+      for (int off = 16; off > 0; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
+      if (threadIdx.x == 0) k.rho_ket[(long long)blockIdx.x * k.nk + i] = rs;
     }
   }
   if (k.obs) {

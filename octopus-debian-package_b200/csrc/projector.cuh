@@ -43,6 +43,10 @@ struct KetArgs {
   double *obs;           // [ket_row_blocks][obs_ld][2] or null
   int obs_ld;
   const void *phase = nullptr;  // per sphere point complex phase (storage type), or null
+  // density of the final rows: rho_ket[blockIdx.x][covered row] = sum over the
+  // CTA's states of w_i |out_i(row)|^2, or null
+  double *rho_ket = nullptr;
+  const double *rho_w = nullptr;
 };
 
 int bra_ksplit(const ProjArgs &p, int num_sms);

@@ -42,6 +42,11 @@ struct PassArgs {
   int obs_ld;
   double obs_pol[3];      // dipole direction
 
+  // density of the pass output (last Horner pass of a Taylor step):
+  // rho_part[chunk][row] = sum over the chunk's states of w_i |out_i(row)|^2
+  double *rho_part;       // [chunks][np], or null
+  const double *rho_w;    // per state weight (ld entries)
+
   const int2 *col_z;      // per (y, x) cell column: {first, last} z of its inner points
   const int4 *items;      // work items {tile x, tile y, first plane, end plane}
   int nitems;

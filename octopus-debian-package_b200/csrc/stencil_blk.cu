@@ -167,7 +167,7 @@ __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, i
 // k % NSIDE.  Iteration k computes plane k and issues the data of plane
 // k + NBUF - 1 and the side data of plane k + 2 NBUF - 2 (one commit group).
 // One work unit: item ih (16 x 8 tile, z block) and state chunk `chunk`.
-template <typename T, bool HORNER, bool OBS, int U, int RX_, int RY_, bool CPLX, int TY_, int CB_>
+template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX_, int RY_, bool CPLX, int TY_, int CB_>
 __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const int chunk, unsigned char *smem) {
   constexpr bool X0 = HORNER || OBS;
   using LY = BlkLayout<T, X0, RX_, RY_, CPLX, TY_, CB_>;
@@ -476,7 +476,23 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
             }
           }
           const int row = rowv[cx][r];
-          if (row < 0 || row >= p.np) continue;
+          const bool ok = row >= 0 && row < p.np;
+          if constexpr (RHO) {
+            // density of the output: w_i |val_i|^2 summed over the SLE lanes of
+            // this cell chunk (one aligned lane group, fixed shuffle order)
+            double c = 0.0;
+            if (ok) {
+              const double w = p.rho_w[col / 2 + (CPLX ? l : l / 2)];
+              if constexpr (CPLX)
+                c = w * (double(val.x) * double(val.x) + double(val.y) * double(val.y));
+              else
+                c = w * double(val) * double(val);
+            }
+#pragma unroll
+            for (int off = SLE / 2; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+            if (ok && l == 0) p.rho_part[(long long)chunk * p.np + row] = c;
+          }
+          if (!ok) continue;
           if constexpr (OBS) {
             const E x0 = x0s[cell * SLE];
             double eh, n2;
@@ -579,12 +595,12 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   }
 }
 
-template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX, int TY, int CB>
+template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB>
 __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::NT,
                                   BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::CTAS)
     pass_blk_kernel(const __grid_constant__ PassArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
-  blk_body<T, HORNER, OBS, U, RX, RY, CPLX, TY, CB>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem);
+  blk_body<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem);
 }
 
 // Many systems in one persistent launch (Horner passes): each CTA takes
@@ -602,15 +618,15 @@ __global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT,
     __syncthreads();
     if (u >= g.nunits) break;
     const int4 W = g.units[u];  // {system, item, chunk, -}
-    blk_body<T, true, false, U, RX, RY, CPLX, TY, CB>(g.sys[W.x], W.y, W.z, smem);
+    blk_body<T, true, false, false, U, RX, RY, CPLX, TY, CB>(g.sys[W.x], W.y, W.z, smem);
     __syncthreads();
   }
 }
 
-template <typename T, bool HORNER, bool OBS, int U, int RX, int RY, bool CPLX, int TY, int CB>
+template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB>
 hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
   using LY = BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>;
-  auto kern = pass_blk_kernel<T, HORNER, OBS, U, RX, RY, CPLX, TY, CB>;
+  auto kern = pass_blk_kernel<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
@@ -627,11 +643,16 @@ hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
 
 template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
 hpsi_status launch_blk_u(const PassArgs &a, cudaStream_t st) {
-  const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr;
-  if (horner && obs) return launch_blk_mode<T, true, true, U, RX, RY, CPLX, TY, CB>(a, st);
-  if (horner) return launch_blk_mode<T, true, false, U, RX, RY, CPLX, TY, CB>(a, st);
-  if (obs) return launch_blk_mode<T, false, true, U, RX, RY, CPLX, TY, CB>(a, st);
-  return launch_blk_mode<T, false, false, U, RX, RY, CPLX, TY, CB>(a, st);
+  const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr, rho = a.rho_part != nullptr;
+  if (rho && (!horner || obs)) {
+    set_error("launch_pass_blk: the density is fused into Horner passes without observables only");
+    return HPSI_ERR_UNSUPPORTED;
+  }
+  if (horner && obs) return launch_blk_mode<T, true, true, false, U, RX, RY, CPLX, TY, CB>(a, st);
+  if (horner && rho) return launch_blk_mode<T, true, false, true, U, RX, RY, CPLX, TY, CB>(a, st);
+  if (horner) return launch_blk_mode<T, true, false, false, U, RX, RY, CPLX, TY, CB>(a, st);
+  if (obs) return launch_blk_mode<T, false, true, false, U, RX, RY, CPLX, TY, CB>(a, st);
+  return launch_blk_mode<T, false, false, false, U, RX, RY, CPLX, TY, CB>(a, st);
 }
 
 template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>

@@ -83,6 +83,8 @@ SIGNATURES = {
                                            C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_lanczos_step": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_double, C.c_int32, C.c_double,
                                       C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_taylor_step_density": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_double, C.c_double, C.c_int32,
+                                             C.POINTER(C.c_double), C.c_void_p, C.c_int32, C.c_void_p]),
     "hpsi_taylor_step_dual": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_int32, C.c_void_p]),
     "hpsi_ghost_pack": (C.c_int32, [C.POINTER(Batch), C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
@@ -103,6 +105,13 @@ SIGNATURES = {
                                           C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32,
                                           C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_double), C.c_void_p]),
+    "hpsi_adjoint_step": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_double,
+                                      C.POINTER(C.c_double), C.c_double, C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]),
+    "hpsi_vjp_field": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(C.c_double),
+                                   C.c_void_p, C.c_void_p]),
+    "hpsi_vjp_vloc": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_double, C.c_void_p,
+                                  C.c_int32, C.c_void_p]),
     "hpsi_nrm2": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(C.c_double), C.c_void_p]),
     "hpsi_density_accumulate": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(C.c_double), C.c_void_p,
                                             C.c_int32, C.c_void_p]),
@@ -367,6 +376,36 @@ class Hamiltonian:
                                            _dp(gc), _stream_ptr(stream)))
         return float(J.value), ge, gv, gc
 
+    # per-step adjoint primitives (host-driven backward propagation)
+    def adjoint_step(self, lam, psi_n, eps_n, dt, order=4, pol=(0.0, 0.0, 1.0), grad_v=None, stream=None):
+        """lam <- T_n^dagger lam in place; returns (dJ/d eps_n, continuous-adjoint
+        term) and accumulates dJ/dv into the float64 device tensor grad_v."""
+        bl, bp = as_batch(lam), as_batch(psi_n)
+        p = np.ascontiguousarray(np.asarray(pol, dtype=np.float64))
+        ge, gc = np.zeros(1), np.zeros(1)
+        gv = C.c_void_p(grad_v.data_ptr()) if grad_v is not None else None
+        check(load().hpsi_adjoint_step(self.handle, C.byref(bl), C.byref(bp), float(eps_n), _dp(p), float(dt),
+                                       int(order), C.c_void_p(ge.ctypes.data), C.c_void_p(gc.ctypes.data), gv,
+                                       _stream_ptr(stream)))
+        return float(ge[0]), float(gc[0])
+
+    def vjp_field(self, chi, psi, pol=(0.0, 0.0, 1.0), nst=None, stream=None) -> np.ndarray:
+        """Per-state dV <chi_i|pol.r|psi_i> (complex, host array)."""
+        bc, bp = as_batch(chi, nst=nst), as_batch(psi, nst=nst)
+        p = np.ascontiguousarray(np.asarray(pol, dtype=np.float64))
+        out = np.zeros(bc.nst, dtype=np.complex128)
+        check(load().hpsi_vjp_field(self.handle, C.byref(bc), C.byref(bp), _dp(p),
+                                    C.c_void_p(out.ctypes.data), _stream_ptr(stream)))
+        return out
+
+    def vjp_vloc(self, lam, psi, grad_v, scale=1.0, accumulate=False, nst=None, stream=None):
+        """grad_v (+)= scale sum_i Re(conj(lam_i) psi_i) on the inner rows
+        (float64 device tensor of np entries)."""
+        bl, bp = as_batch(lam, nst=nst), as_batch(psi, nst=nst)
+        check(load().hpsi_vjp_vloc(self.handle, C.byref(bl), C.byref(bp), float(scale),
+                                   C.c_void_p(grad_v.data_ptr()), 1 if accumulate else 0, _stream_ptr(stream)))
+        return grad_v
+
     # exponential-midpoint time propagation (td_run with TDPropagator = exp_mid)
     def td_propagate(self, psi, nsteps, dt, order=4, E0=0.0, omega=0.0, T=0.0, pol=(0.0, 0.0, 1.0), t0=0.0,
                      graph=True, nst=None, stream=None, propagator="exp_mid"):
@@ -449,6 +488,21 @@ class Hamiltonian:
         check(load().hpsi_lanczos_step(self.handle, C.byref(b), float(dt), int(max_order), float(tol), C.byref(it),
                                        C.byref(res), _stream_ptr(stream)))
         return int(it.value), float(res.value)
+
+    def taylor_step_density(self, psi, dt, weight, rho=None, accumulate=False, order=4, nst=None, stream=None):
+        """Taylor step, then rho (+)= sum_i weight[i] |psi_i|^2 of the propagated
+        batch, fused into the last pass (hpsi_taylor_step_density); rho a
+        float64 device tensor of np entries (allocated when None)."""
+        import torch
+        b = as_batch(psi, nst=nst)
+        w = np.ascontiguousarray(np.asarray(weight, dtype=np.float64)[: b.nst])
+        if rho is None:
+            rho = torch.zeros(self.dmesh.mesh.np, dtype=torch.float64, device=psi.device)
+        dt = complex(dt)
+        check(load().hpsi_taylor_step_density(self.handle, C.byref(b), dt.real, dt.imag, int(order), _dp(w),
+                                              C.c_void_p(rho.data_ptr()), 1 if accumulate else 0,
+                                              _stream_ptr(stream)))
+        return rho
 
     # Taylor branch of exponential_apply_batch
     def taylor_step(self, psi, dt, order=4, nst=None, observables=False, stream=None):

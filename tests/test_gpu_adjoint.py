@@ -108,3 +108,68 @@ def test_torch_autograd_wrapper(cuda):
     (g,) = torch.autograd.grad(J, e)
     _, ge, _, _ = ham.adjoint_gradient(x, t, eps, 0.02, want_v=False)
     assert np.array_equal(g.numpy(), ge)
+
+
+def test_per_step_adjoint_equals_gradient(cuda):
+    """A host-driven backward run (the shape of the reference's bwd_step loop):
+    forward steps with hpsi_taylor_step under the field eps_n z, lambda_N from
+    the target overlaps, then hpsi_adjoint_step for n = N-1 .. 0.  The per-step
+    VJPs equal hpsi_adjoint_gradient (checkpointed, recomputing) to 1e-13."""
+    import torch
+    nsteps, dt = 12, 0.02
+    m, v, psi, phi, eps, dm, ham, x, t = _setup(cuda, nsteps=nsteps)
+    J, ge_ref, gv_ref, gc_ref = ham.adjoint_gradient(x, t, eps, dt, ckpt=5)
+    xs = [x.clone()]
+    cur = x.clone()
+    for n in range(nsteps):
+        ham.set_field((0.0, 0.0, 1.0), eps[n])
+        ham.taylor_step(cur, dt)
+        xs.append(cur.clone())
+    ham.set_field((0.0, 0.0, 1.0), 0.0)
+    yN = xs[-1][: m.np].cpu().numpy()
+    ov = m.vol_pp * np.sum(phi[: m.np].conj() * yN, axis=0)
+    assert abs(float(np.sum(np.abs(ov) ** 2)) - J) <= 1e-12 * J
+    lam = torch.zeros_like(x)
+    lam[: m.np] = torch.from_numpy(phi[: m.np] * ov[None, :]).to(cuda)
+    gv = torch.zeros(m.np, dtype=torch.float64, device=cuda)
+    ge, gc = np.zeros(nsteps), np.zeros(nsteps)
+    for n in range(nsteps - 1, -1, -1):
+        ge[n], gc[n] = ham.adjoint_step(lam, xs[n], eps[n], dt, grad_v=gv)
+    assert np.max(np.abs(ge - ge_ref)) <= 1e-13 * np.max(np.abs(ge_ref))
+    assert np.max(np.abs(gc - gc_ref)) <= 1e-13 * np.max(np.abs(gc_ref))
+    gvh = gv.cpu().numpy()
+    assert np.max(np.abs(gvh - gv_ref)) <= 1e-13 * np.max(np.abs(gv_ref))
+    # the continuous-adjoint term is the reference's 2 dt Im <lambda|z|psi_n>:
+    # one call of the field VJP on the same pair gives it
+    lam_n1 = torch.zeros_like(x)
+    lam_n1[: m.np] = torch.from_numpy(phi[: m.np] * ov[None, :]).to(cuda)
+    d = ham.vjp_field(lam_n1, xs[nsteps - 1])
+    assert abs(2 * dt * np.sum(d).imag - gc[nsteps - 1]) <= 1e-13 * abs(gc[nsteps - 1]) + 1e-18
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_vjp_field_and_vloc_match_numpy(cuda, dtype):
+    import torch
+    from hpsi import lib
+    from hpsi.mesh import index_box_mesh
+    from hpsi.stencil import laplacian_weights, star_points
+    rng = np.random.default_rng(17)
+    m = index_box_mesh((11, 9, 7), 0.3)
+    nst = 37  # more states than a warp
+    cdt = np.complex128 if dtype == "c128" else np.complex64
+    a = (rng.standard_normal((m.np_part, nst)) + 1j * rng.standard_normal((m.np_part, nst))).astype(cdt)
+    b = (rng.standard_normal((m.np_part, nst)) + 1j * rng.standard_normal((m.np_part, nst))).astype(cdt)
+    ham = lib.Hamiltonian(lib.DeviceMesh(m), laplacian_weights(m.spacing), star_points())
+    ta, tb = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+    pol = np.array([0.3, -0.5, 0.8])
+    z = m.x[: m.np] @ pol
+    A, Bm = a[: m.np].astype(np.complex128), b[: m.np].astype(np.complex128)
+    ref = m.vol_pp * np.sum(A.conj() * z[:, None] * Bm, axis=0)
+    got = ham.vjp_field(ta, tb, pol=pol)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+    g = torch.full((m.np,), 7.0, dtype=torch.float64, device=cuda)
+    ham.vjp_vloc(ta, tb, g, scale=0.25)
+    refv = 0.25 * np.sum((A.conj() * Bm).real, axis=1)
+    assert np.max(np.abs(g.cpu().numpy() - refv)) <= 1e-12 * np.max(np.abs(refv))
+    ham.vjp_vloc(ta, tb, g, scale=0.25, accumulate=True)
+    assert np.max(np.abs(g.cpu().numpy() - 2 * refv)) <= 1e-12 * np.max(np.abs(refv))

@@ -55,3 +55,45 @@ def test_density_of_propagated_states(cuda):
     # Taylor series is not unitary: the norms move at the 1e-3 level here)
     norms = m.vol_pp * np.sum(np.abs(ref_psi[: m.np]) ** 2, axis=0)
     assert abs(m.vol_pp * float(rho.sum()) - float(w @ norms)) <= 1e-12 * float(w @ norms)
+
+
+@pytest.mark.parametrize("dtype,nst,ld", [("c128", 16, 16), ("c64", 32, 32), ("c128", 6, 6), ("c64", 40, 48)])
+def test_taylor_step_density_fused(cuda, dtype, nst, ld):
+    """hpsi_taylor_step_density: the propagated batch equals hpsi_taylor_step's
+    bit for bit, and the density (fused into the last Horner pass, KB-covered
+    rows from the ket's final values; widths the blocked pass does not take
+    run the density kernel after the step) equals the density kernel on the
+    propagated batch and the oracle's step + density."""
+    import torch
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    from oracle import oracle as O
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    m, v, proj, psi = small_sphere_system(seed=53, nst=nst, radius=4.0, natoms=3)
+    w = laplacian_weights(m.spacing)
+    dm = lib.DeviceMesh(m)
+    H = lib.Hamiltonian(dm, w, star_points(), v=v, projectors=proj)
+    g = np.zeros((m.np_part, ld), dtype=np.complex128)
+    g[:, :nst] = psi
+    wt = np.random.default_rng(54).uniform(0.5, 2.0, nst)
+    a = torch.from_numpy(g).to(cuda).to(tdt)
+    b = a.clone()
+    dt = 0.01
+    H.taylor_step(a, dt, nst=nst)
+    rho = H.taylor_step_density(b, dt, wt, nst=nst)
+    assert torch.equal(a[: m.np], b[: m.np])
+    ref = dm.density(a, wt, nst=nst)
+    tol = 1e-13
+    assert torch.max(torch.abs(rho - ref)).item() <= tol * torch.max(ref).item()
+    rho2 = H.taylor_step_density(b.clone(), dt, wt, rho=rho.clone(), accumulate=True, nst=nst)
+    ref2 = dm.density(a, wt, nst=nst)
+    H.taylor_step(a, dt, nst=nst)
+    ref2 = dm.density(a, wt, rho=ref2, accumulate=True, nst=nst)
+    assert torch.max(torch.abs(rho2 - ref2)).item() <= tol * torch.max(ref2).item()
+    if dtype == "c128":
+        P = O.Projectors(proj.maps, proj.mats, proj.scals)
+        y = O.Hamiltonian(m, w, star_points(), v=v, projectors=P).taylor(psi, dt)
+        yp = np.zeros((m.np_part, nst), dtype=np.complex128)
+        yp[: m.np] = y
+        ro = O.density_accumulate(m, yp, wt)
+        assert np.max(np.abs(rho.cpu().numpy() - ro)) <= 1e-12 * np.max(ro)
