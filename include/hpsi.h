@@ -219,10 +219,10 @@ hpsi_status hpsi_taylor_step(hpsi_hamiltonian *ham, hpsi_batch *psi, double dt_r
  * src/states/density.F90:279-362):
  *   psi <- exp(-i dt H) psi (order-`order` Taylor series, as hpsi_taylor_step),
  *   rho[ip] = (accumulate ? rho[ip] : 0) + sum_i weight[i] |psi_i(ip)|^2.
- * The density is fused into the last Horner pass, which writes the
- * propagated rows, and into its KB ket for the rows the projectors cover (no
- * extra read of the batch); batch widths the register-blocked pass does not
- * take get one density pass after the step.  FP64 sums in a fixed order.
+ * The density is one pass over the propagated batch after the step (a form
+ * fused into the last Horner pass and its KB ket exists, but its cross-lane
+ * sums slow the stencil pass by more than the separate pass costs).  FP64
+ * sums in a fixed order.
  * weight: nst host doubles (kweight x occupation), read before the call
  * returns; psi and rho (np doubles) device memory; stream ordered. */
 hpsi_status hpsi_taylor_step_density(hpsi_hamiltonian *ham, hpsi_batch *psi,

@@ -488,6 +488,9 @@ hpsi_status hpsi_hamiltonian_create(hpsi_mesh *mesh, hpsi_hamiltonian **out) {
   // experiment override: HPSI_BRA_OVERLAP=0 runs the KB bra on the caller's
   // stream before the pass
   if (const char *e = std::getenv("HPSI_BRA_OVERLAP")) h->overlap_bra = std::atoi(e) != 0;
+  // experiment override: HPSI_FUSED_DENSITY=1 fuses the density of
+  // hpsi_taylor_step_density into the last pass
+  if (const char *e = std::getenv("HPSI_FUSED_DENSITY")) h->fuse_density = std::atoi(e) != 0;
   *out = h;
   return HPSI_OK;
 }
@@ -1537,12 +1540,20 @@ hpsi_status hpsi_taylor_step_density(hpsi_hamiltonian *h, hpsi_batch *psi, doubl
   R.w = w;
   R.part = w + nw;
   R.ket = R.part + npart;
+  // The fused form (density partials written by the last Horner pass, the
+  // ket's rows from their final values) measured slower on the 904,089-point
+  // sphere with 128 states than the step followed by the density pass
+  // (FP64 +0.42 ms against +0.29 ms per step, FP32 +0.27 against +0.17): its
+  // cross-lane sums share the MIO pipe with the stencil's shared-memory
+  // loads.  The default is therefore the separate pass; fuse_density selects
+  // the fused form.
+  RhoSpec *rp = h->fuse_density ? &R : nullptr;
   if (psi->dtype == HPSI_C128)
     s = taylor_dev_impl<double>(h, static_cast<double *>(psi->ptr), ld, psi->nst, dt_re, dt_im, order, nullptr, st,
-                                &R);
+                                rp);
   else
     s = taylor_dev_impl<float>(h, static_cast<float *>(psi->ptr), ld, psi->nst, dt_re, dt_im, order, nullptr, st,
-                               &R);
+                               rp);
   if (s) return s;
   if (R.fused) {
     const bool kb = h->nmat > 0 && h->nk > 0;
@@ -1552,8 +1563,8 @@ hpsi_status hpsi_taylor_step_density(hpsi_hamiltonian *h, hpsi_batch *psi, doubl
     g_launches++;
     HPSI_CHECK_LAUNCH();
   } else {
-    // widths the register-blocked pass does not take: the density kernel
-    // reads the propagated batch once more
+    // the density kernel reads the propagated batch once more (the default,
+    // and widths the register-blocked pass does not take)
     if (psi->dtype == HPSI_C128)
       s = launch_density<double>(static_cast<const double *>(psi->ptr), ld, m->np, psi->nst, w, rho,
                                  accumulate != 0, st);

@@ -94,6 +94,7 @@ struct hpsi_hamiltonian {
   const double *fld_scale_dev = nullptr;  // set while a TD run replays steps
   // side stream of the KB bra (forked from the caller's stream, joined before the ket)
   bool overlap_bra = true;
+  bool fuse_density = false;  // hpsi_taylor_step_density: density in the last pass (slower, kept for measurement)
   cudaStream_t bra_stream = nullptr;
   cudaEvent_t bra_fork = nullptr, bra_join = nullptr;
   hpsi_status ensure_bra_stream();

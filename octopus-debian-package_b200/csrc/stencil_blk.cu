@@ -326,6 +326,8 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   const bool has_field = fz != 0.0 || fx0 != 0.0 || fy0 != 0.0;  // uniform over the grid
   const T are = static_cast<T>(p.a_re), aim = static_cast<T>(p.a_im);
   const bool odd = !CPLX && (l & 1) != 0;
+  // density weight of this lane's state (fused density of the output)
+  [[maybe_unused]] const double wrho = RHO ? p.rho_w[col / 2 + (CPLX ? l : l / 2)] : 0.0;
   E *out = static_cast<E *>(p.out);
   const long long out_lde = 2 * p.out_ld / LY::LW;  // elements per output row
   const int ocol = col / LY::LW + l;
@@ -457,6 +459,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
       (void)pe;
       (void)pn;
       (void)pd;
+      [[maybe_unused]] double rc[RX * RY];
 #pragma unroll
       for (int cx = 0; cx < RX; ++cx)
 #pragma unroll
@@ -478,19 +481,11 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
           const int row = rowv[cx][r];
           const bool ok = row >= 0 && row < p.np;
           if constexpr (RHO) {
-            // density of the output: w_i |val_i|^2 summed over the SLE lanes of
-            // this cell chunk (one aligned lane group, fixed shuffle order)
-            double c = 0.0;
-            if (ok) {
-              const double w = p.rho_w[col / 2 + (CPLX ? l : l / 2)];
-              if constexpr (CPLX)
-                c = w * (double(val.x) * double(val.x) + double(val.y) * double(val.y));
-              else
-                c = w * double(val) * double(val);
-            }
-#pragma unroll
-            for (int off = SLE / 2; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
-            if (ok && l == 0) p.rho_part[(long long)chunk * p.np + row] = c;
+            // this lane's share of the output's density, w_i |val_i|^2
+            if constexpr (CPLX)
+              rc[cx * RY + r] = ok ? wrho * (double(val.x) * double(val.x) + double(val.y) * double(val.y)) : 0.0;
+            else
+              rc[cx * RY + r] = ok ? wrho * double(val) * double(val) : 0.0;
           }
           if (!ok) continue;
           if constexpr (OBS) {
@@ -509,6 +504,36 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
           }
           out[row * out_lde + ocol] = val;
         }
+      if constexpr (RHO) {
+        // sum the NC = RX RY cell shares over the SLE lanes of the chunk: a
+        // transposing butterfly halves the values a lane holds at each of the
+        // first log2(NC) steps (one shuffle per kept pair), then a plain
+        // reduction over the remaining lanes; lane l ends with the total of
+        // cell sum_s hi_s NC / 2^(s+1).  5 double shuffles for 4 cells instead
+        // of 16 (the shuffles share the MIO pipe with the stencil's loads).
+        constexpr int NC = RX * RY;
+        static_assert((NC & (NC - 1)) == 0 && NC <= SLE, "cells per thread: a power of 2 up to the lane group");
+        int cell = 0;
+#pragma unroll
+        for (int st = 0; (NC >> st) > 1; ++st) {
+          const int half = (NC >> st) / 2, off = SLE >> (st + 1);
+          const bool hi = (l & off) != 0;
+#pragma unroll
+          for (int j = 0; j < half; ++j) {
+            const double send = hi ? rc[j] : rc[j + half];
+            const double keep = hi ? rc[j + half] : rc[j];
+            rc[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+          }
+          if (hi) cell += half;
+        }
+        constexpr int LOGNC = NC >= 8 ? 3 : NC >= 4 ? 2 : NC >= 2 ? 1 : 0;
+#pragma unroll
+        for (int off = SLE >> (LOGNC + 1); off > 0; off >>= 1) rc[0] += __shfl_xor_sync(0xffffffffu, rc[0], off);
+        if ((l & ((SLE >> LOGNC) - 1)) == 0) {
+          const int row = rowv[cell / RY][cell % RY];
+          if (row >= 0 && row < p.np) p.rho_part[(long long)chunk * p.np + row] = rc[0];
+        }
+      }
       if constexpr (OBS) {
         // the plane's cells summed first, then one add per plane and sum;
         // dipole weight of a cell = dxy00 + its x/y offset terms (in pd) + z term

@@ -57,17 +57,20 @@ def test_density_of_propagated_states(cuda):
     assert abs(m.vol_pp * float(rho.sum()) - float(w @ norms)) <= 1e-12 * float(w @ norms)
 
 
+@pytest.mark.parametrize("fused", [False, True])
 @pytest.mark.parametrize("dtype,nst,ld", [("c128", 16, 16), ("c64", 32, 32), ("c128", 6, 6), ("c64", 40, 48)])
-def test_taylor_step_density_fused(cuda, dtype, nst, ld):
+def test_taylor_step_density(cuda, dtype, nst, ld, fused, monkeypatch):
     """hpsi_taylor_step_density: the propagated batch equals hpsi_taylor_step's
-    bit for bit, and the density (fused into the last Horner pass, KB-covered
-    rows from the ket's final values; widths the blocked pass does not take
-    run the density kernel after the step) equals the density kernel on the
-    propagated batch and the oracle's step + density."""
+    bit for bit, and the density equals the density kernel on the propagated
+    batch and the oracle's step + density.  Both forms: the density pass after
+    the step (default), and the density fused into the last Horner pass with
+    the KB-covered rows from the ket's final values (widths the blocked pass
+    does not take use the density pass in either form)."""
     import torch
     from hpsi import lib
     from hpsi.stencil import laplacian_weights, star_points
     from oracle import oracle as O
+    monkeypatch.setenv("HPSI_FUSED_DENSITY", "1" if fused else "0")
     tdt = torch.complex128 if dtype == "c128" else torch.complex64
     m, v, proj, psi = small_sphere_system(seed=53, nst=nst, radius=4.0, natoms=3)
     w = laplacian_weights(m.spacing)
