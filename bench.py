@@ -238,7 +238,48 @@ def run_reference(args, rank, world):
                                    "operate.c compiled from source; vpsi and KB restated)"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    gpu = reference_gpu_rate(sysm, args)
+    if gpu is not None:
+        line["extra"] = {"reference_gpu_kernels": gpu}
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_rate(sysm, args):
+    """The reference's own GPU H.psi on the same batch: its share/opencl
+    kernels (operate_map, vpsi, dprojector_bra, dprojector_ket per matrix with
+    a synchronisation each) compiled from source for sm_100a and launched as
+    the reference launches them; CUDA events over the steps.  None without a
+    GPU or without the compiled kernels."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        from oracle import refgpu
+        if not refgpu.available():
+            return None
+    except Exception:
+        return None
+    from hpsi.stencil import laplacian_weights, star_points
+    dev = torch.device("cuda", 0)
+    m = sysm.mesh
+    R = refgpu.RefHamiltonian(m, laplacian_weights(m.spacing), star_points(), sysm.v, sysm.proj, dev)
+    x = torch.from_numpy(sysm.psi).to(dev)
+    y = torch.zeros((m.np, x.shape[1]), dtype=torch.complex128, device=dev)
+    proj = R.projection_buffer(x)
+    for _ in range(args.warmup):
+        R.apply(x, y, proj)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        R.apply(x, y, proj)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    return {"value": m.np * x.shape[1] / ms / 1e6, "unit": UNIT, "ms_per_step": ms,
+            "kernels": "reference share/opencl operate_map + vpsi + dprojector_bra + dprojector_ket "
+                       "(one launch per matrix, synchronised), NVRTC-compiled for sm_100a with the "
+                       "reference's flags"}
 
 
 class Ranks:

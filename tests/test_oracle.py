@@ -299,3 +299,51 @@ def test_kb_with_projector_phases_is_hermitian():
     x = psi[: m.np]
     assert np.allclose(K(x, ones), K(x, None), rtol=0, atol=1e-13 * np.abs(K(x, None)).max())
     assert np.abs(K(x, ph) - K(x, None)).max() > 1e-3 * np.abs(K(x, None)).max()
+
+
+REF_GPU_GOLDEN = os.path.join(HERE, "golden", "ref_gpu_kernels.npz")
+
+
+def _ref_gpu_golden():
+    if not os.path.exists(REF_GPU_GOLDEN):
+        pytest.skip("reference GPU kernel golden file not generated")
+    g = np.load(REF_GPU_GOLDEN)
+    from hpsi.fixtures import ProjectorSet
+    from hpsi.mesh import Mesh
+    m = Mesh(lxyz=g["lxyz"], np=int(g["np"]), spacing=g["spacing"])
+    npts, nprj = g["npoints"], g["nprojs"]
+    maps, mats, scals = [], [], []
+    o = om = os_ = 0
+    for a, b in zip(npts, nprj):
+        maps.append(g["maps"][o: o + a])
+        mats.append(g["mats"][om: om + a * b].reshape(a, b))
+        scals.append(g["scals"][os_: os_ + b])
+        o, om, os_ = o + a, om + a * b, os_ + b
+    return g, m, ProjectorSet(maps, mats, scals, None)
+
+
+def test_restated_kernels_match_reference_gpu_kernels():
+    """The oracle's restatements of the stencil (times -1/2), vpsi, the KB bra
+    and ket and the axpy against the reference's own GPU kernels
+    (share/opencl operate.cl operate_map, vpsi.cl vpsi, projector.cl
+    dprojector_bra/dprojector_ket, axpy.cl daxpy), built from source for
+    sm_100a and run on a B200 (tests/golden/make_ref_gpu_golden.py)."""
+    from oracle import oracle as O
+    from hpsi.stencil import star_points
+    g, m, proj = _ref_gpu_golden()
+    psi = g["psi"]
+    w = g["weights"]
+    nst = psi.shape[1]
+    kin = O.Hamiltonian(m, w, star_points(), v=None, use_ref=False).apply(psi)
+    assert rel_maxnorm_per_state(kin[:, :4], g["kinetic"][:, :4]) <= 1e-13
+    vpsi = g["v"][:, None] * psi[: m.np]
+    assert np.max(np.abs(vpsi - g["vpsi"])) <= 1e-14 * np.max(np.abs(vpsi))
+    pr = O.kb_bra(proj.maps, proj.mats, proj.scals, psi)
+    assert np.max(np.abs(pr - g["projections"])) <= 1e-13 * np.max(np.abs(pr))
+    ket = O.kb_ket(proj.maps, proj.mats, g["projections"], np.zeros((m.np, nst), complex))
+    assert np.max(np.abs(ket - g["ket"])) <= 1e-13 * np.max(np.abs(ket))
+    P = O.Projectors(proj.maps, proj.mats, proj.scals)
+    h = O.Hamiltonian(m, w, star_points(), v=g["v"], projectors=P, use_ref=False).apply(psi[:, :4])
+    assert rel_maxnorm_per_state(h, g["hpsi"][:, :4]) <= 1e-13
+    ax = g["axpy_in"] + float(g["axpy_a"]) * psi[: m.np]
+    assert np.max(np.abs(ax - g["axpy_out"])) <= 1e-15 * np.max(np.abs(ax))
