@@ -485,6 +485,38 @@ hpsi_status hpsi_apply_h_horner(hpsi_hamiltonian *ham, const hpsi_batch *psi,
                                 double a_re, double a_im, int32_t terms,
                                 int32_t set_bc, void *stream);
 
+/* Inner/outer split of a domain-parallel pass, so that the points whose
+ * stencil reads no ghost row run while the ghost rows are in flight
+ * (X(derivatives_batch_start/finish) with the ghost update overlapped,
+ * src/grid/derivatives_inc.F90:82-102, op%inner / op%outer of
+ * src/grid/nl_operator.F90:458-514).
+ * hpsi_mesh_set_ghost_rows: rows [first, first + count) of the mesh (between
+ * np and np_part) are ghost rows (par_vec_t order: local points, ghosts,
+ * boundary); count = 0 clears it.
+ * hpsi_apply_h_points / hpsi_apply_h_horner_points: hpsi_apply_h /
+ * hpsi_apply_h_horner restricted to
+ *   HPSI_POINTS_INNER  output rows whose stencil reads no ghost row (the
+ *                      ghost rows are not read at all: they may change while
+ *                      this runs),
+ *   HPSI_POINTS_OUTER  the other output rows,
+ *   HPSI_POINTS_ALL    every row (the plain call).
+ * INNER then OUTER writes every row once, the same values as ALL.  Rows are
+ * split per 16-cell tile column and z plane, conservatively (a plane whose
+ * widened tile box holds a ghost cell is outer).  Device batches only; the KB
+ * term must go through hpsi_projector_bra / hpsi_projector_ket (it is added
+ * once, after both parts). */
+#define HPSI_POINTS_ALL 0
+#define HPSI_POINTS_INNER 1
+#define HPSI_POINTS_OUTER 2
+hpsi_status hpsi_mesh_set_ghost_rows(hpsi_mesh *mesh, int32_t first, int32_t count);
+hpsi_status hpsi_apply_h_points(hpsi_hamiltonian *ham, const hpsi_batch *psi,
+                                hpsi_batch *hpsi, int32_t terms, int32_t set_bc,
+                                int32_t points, void *stream);
+hpsi_status hpsi_apply_h_horner_points(hpsi_hamiltonian *ham, const hpsi_batch *psi,
+                                       const hpsi_batch *psi0, hpsi_batch *out,
+                                       double a_re, double a_im, int32_t terms,
+                                       int32_t set_bc, int32_t points, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Library-wide controls and diagnostics. */
 const char *hpsi_last_error_string(void);

@@ -463,6 +463,7 @@ hpsi_status hpsi_mesh_destroy(hpsi_mesh *m) {
   m->scratch.release();
   m->scratch2.release();
   for (auto &kv : m->items) dev_free(kv.second.first);
+  for (auto &kv : m->items_part) dev_free(kv.second.first);
   m->stage_in.release();
   m->stage_out.release();
   delete m;
@@ -912,6 +913,75 @@ hpsi_status mesh_items(hpsi_mesh *m, int zb, const int4 **items, int *nitems) {
   return mesh_items(m, zb, 16, items, nitems);
 }
 
+// Work list of one part of a domain-parallel mesh (part 1: output planes of a
+// tile column whose stencil reads no ghost row; part 2: the others), the
+// split the reference makes between op%inner and op%outer
+// (src/grid/nl_operator.F90:458-514) so that the inner points run while the
+// ghost rows are in flight (src/grid/derivatives_inc.F90:82-102).  A plane of
+// a tile column is marked ghost-reading, conservatively, when a ghost cell lies
+// in the tile's box widened by the stencil half-width in x, y and z.
+hpsi_status mesh_items_part(hpsi_mesh *m, int zb, int ty, int part, const int4 **items, int *nitems) {
+  const int key = (2 * zb + (ty == 8 ? 1 : 0)) * 4 + part;
+  auto it = m->items_part.find(key);
+  if (it == m->items_part.end()) {
+    const CellBox &B = m->box;
+    const int HAL = 4;
+    const int tyn = ty == 8 ? m->tiles_y8 : m->tiles_y;
+    const auto &tz = ty == 8 ? m->tile_z8 : m->tile_z;
+    // dirty[tile][z - z0(tile)]: plane z of the tile column reads a ghost cell
+    std::vector<std::vector<char>> dirty(tz.size());
+    for (size_t t = 0; t < tz.size(); ++t)
+      if (tz[t].y >= 0) dirty[t].assign(size_t(tz[t].y - tz[t].x + 1), 0);
+    for (int r = m->ghost_first; r < m->ghost_first + m->ghost_count; ++r) {
+      const int c = m->cell_of_row_h[r];
+      const int x = c % B.NX, y = (c / B.NX) % B.NY, z = c / (B.NX * B.NY);
+      // tiles whose widened box [x0 - 4, x0 + 16 + 4) x [y0 - 4, y0 + ty + 4) holds (x, y)
+      const int bx0 = std::max(0, (x - HAL - (PASS_TILE + HAL - 1)) / PASS_TILE - 1);
+      const int bx1 = std::min(m->tiles_x - 1, (x - HAL + HAL) / PASS_TILE + 1);
+      const int by0 = std::max(0, (y - HAL - (ty + HAL - 1)) / ty - 1);
+      const int by1 = std::min(tyn - 1, (y - HAL + HAL) / ty + 1);
+      for (int by = by0; by <= by1; ++by)
+        for (int bx = bx0; bx <= bx1; ++bx) {
+          const int x0 = HAL + bx * PASS_TILE, y0 = HAL + by * ty;
+          if (x < x0 - HAL || x >= x0 + PASS_TILE + HAL || y < y0 - HAL || y >= y0 + ty + HAL) continue;
+          const size_t t = size_t(by) * m->tiles_x + bx;
+          if (tz[t].y < 0) continue;
+          for (int zz = std::max(tz[t].x, z - HAL); zz <= std::min(tz[t].y, z + HAL); ++zz)
+            dirty[t][size_t(zz - tz[t].x)] = 1;
+        }
+    }
+    std::vector<int4> v;
+    for (int by = 0; by < tyn; ++by)
+      for (int bx = 0; bx < m->tiles_x; ++bx) {
+        const size_t t = size_t(by) * m->tiles_x + bx;
+        const int2 c = tz[t];
+        if (c.y < 0) continue;
+        int z = c.x;
+        while (z <= c.y) {
+          const char d = dirty[t][size_t(z - c.x)];
+          int e = z;
+          while (e <= c.y && dirty[t][size_t(e - c.x)] == d && e - z < zb) ++e;
+          if ((part == 1 && !d) || (part == 2 && d)) v.push_back(make_int4(bx, by, z, e));
+          z = e;
+        }
+      }
+    std::stable_sort(v.begin(), v.end(), [zb](const int4 &a, const int4 &b) {
+      const int za = a.z / zb, zbb = b.z / zb;
+      if (za != zbb) return za < zbb;
+      if (a.y != b.y) return a.y < b.y;
+      return a.x < b.x;
+    });
+    int4 *d = nullptr;
+    hpsi_status s = dev_alloc(reinterpret_cast<void **>(&d), std::max<size_t>(1, v.size()) * sizeof(int4));
+    if (s) return s;
+    if (!v.empty()) HPSI_TRY_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    it = m->items_part.emplace(key, std::make_pair(d, int(v.size()))).first;
+  }
+  *items = it->second.first;
+  *nitems = it->second.second;
+  return HPSI_OK;
+}
+
 // Build the pass arguments shared by apply and Taylor passes.
 void base_pass_args(const hpsi_hamiltonian *h, int terms, const int *src_map, PassArgs &a) {
   const hpsi_mesh *m = h->mesh;
@@ -1063,7 +1133,8 @@ struct RhoSpec {
 template <typename T>
 hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T *in, long long in_ld, T *out,
                      long long out_ld, long long ld, int mode, const T *psi0, long long psi0_ld, double a_re,
-                     double a_im, double *obs_partial, int *ncta_out, cudaStream_t st, RhoSpec *rho = nullptr) {
+                     double a_im, double *obs_partial, int *ncta_out, cudaStream_t st, RhoSpec *rho = nullptr,
+                     int points = 0) {
   PassArgs a;
   const int dtype = sizeof(T) == 8 ? HPSI_C128 : HPSI_C64;
   PassShape shape = pass_shape(h, dtype, ld);
@@ -1080,6 +1151,12 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
                               a);
       if (si) return si;
     }
+  }
+  if (points != 0) {
+    // one part of a domain-parallel mesh (no KB term, no observables)
+    const int ty = shape.blk ? shape.ty : 16;
+    si = mesh_items_part(h->mesh, a.zb, ty, points, &a.items, &a.nitems);
+    if (si) return si;
   }
   const bool nl = (terms & HPSI_TERM_NON_LOCAL_POTENTIAL) && h->nmat > 0;
   // The bra reads only psi, like the pass: it runs on the handle's side
@@ -1794,6 +1871,94 @@ hpsi_status hpsi_apply_h_horner(hpsi_hamiltonian *h, const hpsi_batch *psi, cons
   return run_pass<float>(h, terms, load_map(h, set_bc), static_cast<const float *>(psi->ptr), ld,
                          static_cast<float *>(out->ptr), ld, ld, PASS_HORNER, static_cast<const float *>(psi0->ptr),
                          ld, a_re, a_im, nullptr, nullptr, st);
+}
+
+
+hpsi_status hpsi_mesh_set_ghost_rows(hpsi_mesh *m, int32_t first, int32_t count) {
+  if (!m || count < 0 || (count > 0 && (first < m->np || first + (long long)count > m->np_part))) {
+    set_error("hpsi_mesh_set_ghost_rows: the ghost rows must lie in [np, np_part)");
+    return HPSI_ERR_ARG;
+  }
+  for (auto &kv : m->items_part) dev_free(kv.second.first);
+  m->items_part.clear();
+  m->ghost_first = count ? first : 0;
+  m->ghost_count = count;
+  return HPSI_OK;
+}
+
+static hpsi_status check_points(const hpsi_hamiltonian *h, int32_t terms, int32_t points, const char *who) {
+  if (points < 0 || points > 2) {
+    set_error(std::string(who) + ": points must be HPSI_POINTS_ALL, _INNER or _OUTER");
+    return HPSI_ERR_ARG;
+  }
+  if (points != 0 && (terms & HPSI_TERM_NON_LOCAL_POTENTIAL) && h->nmat > 0) {
+    set_error(std::string(who) +
+              ": the KB term is added once after both parts (hpsi_projector_bra / hpsi_projector_ket)");
+    return HPSI_ERR_ARG;
+  }
+  return HPSI_OK;
+}
+
+hpsi_status hpsi_apply_h_points(hpsi_hamiltonian *h, const hpsi_batch *psi, hpsi_batch *hpsi, int32_t terms,
+                                int32_t set_bc, int32_t points, void *stream) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_status s = check_points(h, terms, points, "hpsi_apply_h_points");
+  if (s) return s;
+  if (points == 0) return hpsi_apply_h(h, psi, hpsi, terms, set_bc, stream);
+  hpsi_mesh *m = h->mesh;
+  s = check_batch(m, psi, m->np_part, "hpsi_apply_h_points(psi)");
+  if (!s) s = check_batch(m, hpsi, m->np, "hpsi_apply_h_points(hpsi)");
+  if (s) return s;
+  if (psi->dtype != hpsi->dtype || psi->nst != hpsi->nst || !is_device_ptr(psi->ptr) || !is_device_ptr(hpsi->ptr)) {
+    set_error("hpsi_apply_h_points: device batches of one dtype and nst expected");
+    return HPSI_ERR_ARG;
+  }
+  if ((terms & HPSI_TERM_KINETIC) && !h->have_kinetic) {
+    set_error("hpsi_apply_h_points: kinetic weights not set");
+    return HPSI_ERR_STATE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (psi->dtype == HPSI_C128)
+    return run_pass<double>(h, terms, load_map(h, set_bc), static_cast<const double *>(psi->ptr), psi->ld,
+                            static_cast<double *>(hpsi->ptr), hpsi->ld, psi->ld, PASS_APPLY, nullptr, 0, 0.0, 0.0,
+                            nullptr, nullptr, st, nullptr, points);
+  return run_pass<float>(h, terms, load_map(h, set_bc), static_cast<const float *>(psi->ptr), psi->ld,
+                         static_cast<float *>(hpsi->ptr), hpsi->ld, psi->ld, PASS_APPLY, nullptr, 0, 0.0, 0.0,
+                         nullptr, nullptr, st, nullptr, points);
+}
+
+hpsi_status hpsi_apply_h_horner_points(hpsi_hamiltonian *h, const hpsi_batch *psi, const hpsi_batch *psi0,
+                                       hpsi_batch *out, double a_re, double a_im, int32_t terms, int32_t set_bc,
+                                       int32_t points, void *stream) {
+  if (!h) return HPSI_ERR_ARG;
+  hpsi_status s = check_points(h, terms, points, "hpsi_apply_h_horner_points");
+  if (s) return s;
+  if (points == 0) return hpsi_apply_h_horner(h, psi, psi0, out, a_re, a_im, terms, set_bc, stream);
+  hpsi_mesh *m = h->mesh;
+  s = check_batch(m, psi, m->np_part, "hpsi_apply_h_horner_points(psi)");
+  if (!s) s = check_batch(m, psi0, m->np, "hpsi_apply_h_horner_points(psi0)");
+  if (!s) s = check_batch(m, out, m->np, "hpsi_apply_h_horner_points(out)");
+  if (s) return s;
+  if (psi->dtype != out->dtype || psi0->dtype != out->dtype || psi->ld != out->ld || psi0->ld != out->ld ||
+      psi->nst != out->nst || psi0->nst != out->nst || !is_device_ptr(psi->ptr) || !is_device_ptr(psi0->ptr) ||
+      !is_device_ptr(out->ptr) || psi->ptr == out->ptr) {
+    set_error("hpsi_apply_h_horner_points: device batches of one dtype, ld and nst, out not psi");
+    return HPSI_ERR_ARG;
+  }
+  if ((terms & HPSI_TERM_KINETIC) && !h->have_kinetic) {
+    set_error("hpsi_apply_h_horner_points: kinetic weights not set");
+    return HPSI_ERR_STATE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long long ld = out->ld;
+  if (out->dtype == HPSI_C128)
+    return run_pass<double>(h, terms, load_map(h, set_bc), static_cast<const double *>(psi->ptr), ld,
+                            static_cast<double *>(out->ptr), ld, ld, PASS_HORNER,
+                            static_cast<const double *>(psi0->ptr), ld, a_re, a_im, nullptr, nullptr, st, nullptr,
+                            points);
+  return run_pass<float>(h, terms, load_map(h, set_bc), static_cast<const float *>(psi->ptr), ld,
+                         static_cast<float *>(out->ptr), ld, ld, PASS_HORNER, static_cast<const float *>(psi0->ptr),
+                         ld, a_re, a_im, nullptr, nullptr, st, nullptr, points);
 }
 
 }  // extern "C"

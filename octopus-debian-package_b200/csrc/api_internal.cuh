@@ -54,6 +54,11 @@ struct hpsi_mesh {
   long long column_planes = 0;          // sum of the tile z extents
   // work list per (z block depth, tile height): key 2 * zb + (height == 8)
   std::map<int, std::pair<int4 *, int>> items;
+  // domain-parallel meshes: rows [ghost_first, ghost_first + ghost_count) hold
+  // other partitions' points; work lists split into the tiles/planes whose
+  // stencil reads no ghost row (part 1) and the rest (part 2), per (zb, ty)
+  int ghost_first = 0, ghost_count = 0;
+  std::map<int, std::pair<int4 *, int>> items_part;
   int2 *d_col_z = nullptr;  // per (y, x) cell column: z range of its inner points
 };
 

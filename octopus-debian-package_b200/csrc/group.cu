@@ -128,6 +128,23 @@ static hpsi_status group_build(hpsi_group *g, int dtype, const std::vector<long 
     g->shapes[s].zb = 0;
   }
   g->sc = sc;
+  // z block depth: whole tile columns (each item re-reads a 4-plane halo above
+  // and below its block, 8 planes per item) unless the group as a whole would
+  // then give fewer than four waves of units, in which case every system takes
+  // the depth it would take alone
+  {
+    long long units_full = 0;
+    for (int s = 0; s < n; ++s) {
+      const int ty = g->blk ? g->shapes[s].ty : 16;
+      const auto &tz = ty == 8 ? g->hams[s]->mesh->tile_z8 : g->hams[s]->mesh->tile_z;
+      long long t = 0;
+      for (auto &c : tz) t += c.y >= 0;
+      units_full += t * (ld[s] / sc);
+    }
+    if (units_full >= 4LL * g->num_sms)
+      for (int s = 0; s < n; ++s)
+        if (g->shapes[s].zb <= 0) g->shapes[s].zb = 1 << 20;
+  }
   for (int first = 0; first < n; first += GROUP_MAX) {
     hpsi_group::Launch L;
     L.first = first;

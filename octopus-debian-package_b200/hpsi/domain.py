@@ -184,6 +184,15 @@ def ghost_update(dom: Domain, psi, nst=None, group=None, pack=None, unpack=None,
     for every partition with ghost rows here, sends for every partition that
     holds rows of this one, all at once (torch.distributed.batch_isend_irecv,
     the reference's ring of irecv/isend), then waited for."""
+    ghost_update_finish(ghost_update_start(dom, psi, nst=nst, group=group, pack=pack, unpack=unpack,
+                                           sendbuf=sendbuf, recvbuf=recvbuf))
+
+
+def ghost_update_start(dom: Domain, psi, nst=None, group=None, pack=None, unpack=None, sendbuf=None, recvbuf=None):
+    """Post the ghost exchange of ``psi`` (X(ghost_update_batch_start),
+    src/grid/boundaries_inc.F90:57-148) and return its handle for
+    ``ghost_update_finish``; the ghost rows of ``psi`` are undefined until
+    then.  Every rank of ``group`` calls it together."""
     import torch
     import torch.distributed as dist
     from . import lib
@@ -222,11 +231,20 @@ def ghost_update(dom: Domain, psi, nst=None, group=None, pack=None, unpack=None,
             continue
         off = int(dom.ghost_sdispls[q])
         ops.append(dist.P2POp(dist.isend, torch.view_as_real(sendbuf[off: off + n]), q, group=group))
-    if ops:
-        for r in dist.batch_isend_irecv(ops):
-            r.wait()
-    if not direct and dom.np_ghost:
-        unpack(recvbuf, ghost_pos, psi, nst=nst)
+    reqs = dist.batch_isend_irecv(ops) if ops else []
+    return {"reqs": reqs, "dom": dom, "psi": psi, "nst": nst, "direct": direct, "recvbuf": recvbuf,
+            "ghost_pos": ghost_pos, "unpack": unpack, "sendbuf": sendbuf}
+
+
+def ghost_update_finish(handle):
+    """Wait for the exchange ``ghost_update_start`` posted and land the
+    messages in the ghost rows (X(ghost_update_batch_finish),
+    src/grid/boundaries_inc.F90:150-231)."""
+    for r in handle["reqs"]:
+        r.wait()
+    dom = handle["dom"]
+    if not handle["direct"] and dom.np_ghost:
+        handle["unpack"](handle["recvbuf"], handle["ghost_pos"], handle["psi"], nst=handle["nst"])
 
 
 def local_projectors(dom: Domain, projectors):
@@ -270,8 +288,11 @@ def local_projector_phases(dom: Domain, projectors, phases):
     return out
 
 
+POINTS_ALL, POINTS_INNER, POINTS_OUTER = 0, 1, 2
+
+
 def apply_partitioned(dom: Domain, psi, hpsi, local_apply, bra=None, ket=None, proj=None, nst=None, group=None,
-                      pack=None, unpack=None):
+                      pack=None, unpack=None, overlap=False):
     """H psi of one partition; every rank of ``group`` calls it together.
 
     1. ghost update of ``psi`` (``ghost_update``);
@@ -280,21 +301,35 @@ def apply_partitioned(dom: Domain, psi, hpsi, local_apply, bra=None, ket=None, p
        asynchronous all-reduce sums the shares over the ranks
        (X(hamiltonian_elec_base_nlocal_start) and the mesh%allreduce of
        hamiltonian_elec_base_inc.F90:836);
-    3. ``local_apply(psi, hpsi)``: kinetic and local terms on the local mesh,
-       overlapping the all-reduce;
+    3. ``local_apply(psi, hpsi, points)``: kinetic and local terms on the local
+       mesh, overlapping the all-reduce;
     4. wait for the sum, then ``ket(proj, hpsi)`` adds the KB term on the
        covered rows (X(hamiltonian_elec_base_nlocal_finish)).
-    With NCCL the all-reduce runs on its own stream after the bra and the
-    ket's stream waits for it; nothing synchronises the host."""
+    With ``overlap`` the ghost exchange is only posted in step 1 and the bra
+    (which reads this partition's own points only) and the pass over the
+    points whose stencil reads no ghost row (``points = POINTS_INNER``) run
+    while the messages are in flight; the exchange is then finished and the
+    other points follow (``POINTS_OUTER``), as X(derivatives_batch_start/
+    finish) overlap them (src/grid/derivatives_inc.F90:82-102).  Without it
+    ``local_apply`` gets ``POINTS_ALL``.  With NCCL the all-reduce runs on its
+    own stream after the bra and the ket's stream waits for it; nothing
+    synchronises the host."""
     import torch
     import torch.distributed as dist
-    ghost_update(dom, psi, nst=nst, group=group, pack=pack, unpack=unpack)
+    handle = ghost_update_start(dom, psi, nst=nst, group=group, pack=pack, unpack=unpack)
+    if not overlap:
+        ghost_update_finish(handle)
     work = None
     if bra is not None:
         bra(psi, proj)
         if dom.nparts > 1:
             work = dist.all_reduce(torch.view_as_real(proj), group=group, async_op=True)
-    local_apply(psi, hpsi)
+    if overlap:
+        local_apply(psi, hpsi, POINTS_INNER)
+        ghost_update_finish(handle)
+        local_apply(psi, hpsi, POINTS_OUTER)
+    else:
+        local_apply(psi, hpsi, POINTS_ALL)
     if bra is not None:
         if work is not None:
             work.wait()
@@ -302,7 +337,7 @@ def apply_partitioned(dom: Domain, psi, hpsi, local_apply, bra=None, ket=None, p
 
 
 def taylor_partitioned(dom: Domain, psi, work, horner, bra=None, ket=None, proj=None, dt=0.0, order=4, nst=None,
-                       group=None, pack=None, unpack=None):
+                       group=None, pack=None, unpack=None, overlap=False):
     """psi <- sum_{k=0..order} (-i dt H)^k / k! psi on this partition's inner
     rows, every rank of ``group`` calling it together: the Taylor series of
     exponential_taylor_series_batch (src/electrons/exponential.F90:677-757)
@@ -311,10 +346,12 @@ def taylor_partitioned(dom: Domain, psi, work, horner, bra=None, ket=None, proj=
     inside every H psi of the reference's domain-parallel run).
 
     ``work`` holds two (npts, ld) batches like ``psi`` whose boundary rows are
-    zero; ``horner(x, psi0, out, a)`` writes out = psi0 + a (T + V) x
-    (hpsi_apply_h_horner, set_bc = 0); with KB projectors ``bra(x, proj)``
-    writes this partition's projection share, summed over the ranks while the
-    pass runs, and ``ket(proj, out, a)`` adds a P proj."""
+    zero; ``horner(x, psi0, out, a, points)`` writes out = psi0 + a (T + V) x
+    on the points of ``points`` (hpsi_apply_h_horner_points, set_bc = 0);
+    with KB projectors ``bra(x, proj)`` writes this partition's projection
+    share, summed over the ranks while the pass runs, and ``ket(proj, out, a)``
+    adds a P proj.  ``overlap`` runs the inner points of each level while its
+    ghost rows are in flight, as ``apply_partitioned`` does."""
     import torch
     import torch.distributed as dist
     if order < 1:
@@ -324,13 +361,20 @@ def taylor_partitioned(dom: Domain, psi, work, horner, bra=None, ket=None, proj=
     for k in range(order, 0, -1):
         a = -1j * dt / k
         out = work[(order - k) % 2] if (k > 1 or order == 1) else psi
-        ghost_update(dom, x, nst=nst, group=group, pack=pack, unpack=unpack)
+        handle = ghost_update_start(dom, x, nst=nst, group=group, pack=pack, unpack=unpack)
+        if not overlap:
+            ghost_update_finish(handle)
         work_ar = None
         if bra is not None:
             bra(x, proj)
             if dom.nparts > 1:
                 work_ar = dist.all_reduce(torch.view_as_real(proj), group=group, async_op=True)
-        horner(x, psi, out, a)
+        if overlap:
+            horner(x, psi, out, a, POINTS_INNER)
+            ghost_update_finish(handle)
+            horner(x, psi, out, a, POINTS_OUTER)
+        else:
+            horner(x, psi, out, a, POINTS_ALL)
         if bra is not None:
             if work_ar is not None:
                 work_ar.wait()
@@ -354,6 +398,8 @@ class DomainHamiltonian:
         v = None if v_global is None else np.asarray(v_global)[dom.inner_rows]
         self.local_proj = None if projectors is None else local_projectors(dom, projectors)
         self.ham = lib.Hamiltonian(self.dmesh, weights, points, v=v, projectors=self.local_proj)
+        # the ghost rows follow the partition's own points (par_vec_t order)
+        self.dmesh.set_ghost_rows(dom.np_local, dom.np_ghost)
         if projector_phases is not None:
             if projectors is None:
                 raise ValueError("DomainHamiltonian: projector phases without projectors")
@@ -370,22 +416,23 @@ class DomainHamiltonian:
             self._proj[key] = torch.zeros((self.nprojections, psi.shape[1]), dtype=psi.dtype, device=psi.device)
         return self._proj[key]
 
-    def apply(self, psi, hpsi, nst=None, group=None):
+    def apply(self, psi, hpsi, nst=None, group=None, overlap=True):
         """Ghost update of ``psi`` (boundary rows must be zero), then H psi of
-        the inner rows into ``hpsi``: hpsi_apply_h (set_bc = 0) for the
-        kinetic and local terms, the projections summed over the ranks of
-        ``group`` and the KB ket (``apply_partitioned``)."""
+        the inner rows into ``hpsi``: hpsi_apply_h_points (set_bc = 0) for the
+        kinetic and local terms, the points that read no ghost row while the
+        ghost rows are in flight (``overlap``), the projections summed over
+        the ranks of ``group`` and the KB ket (``apply_partitioned``)."""
         from . import lib
         kb = self.nprojections > 0
         terms = lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL
         apply_partitioned(
             self.dom, psi, hpsi,
-            lambda x, y: self.ham.apply(x, y, nst=nst, terms=terms, set_bc=False),
+            lambda x, y, pts: self.ham.apply(x, y, nst=nst, terms=terms, set_bc=False, points=pts),
             bra=self.ham.projector_bra if kb else None,
             ket=(lambda p, y: self.ham.projector_ket(p, y, nst=nst)) if kb else None,
-            proj=self.projection_buffer(psi) if kb else None, nst=nst, group=group)
+            proj=self.projection_buffer(psi) if kb else None, nst=nst, group=group, overlap=overlap)
 
-    def taylor_step(self, psi, dt, order=4, nst=None, group=None):
+    def taylor_step(self, psi, dt, order=4, nst=None, group=None, overlap=True):
         """psi <- exp(-i dt H) psi (order-``order`` Taylor) on the partition's
         inner rows; ``psi`` is the local (np_part, ld) device batch with zero
         boundary rows (``taylor_partitioned``)."""
@@ -398,7 +445,9 @@ class DomainHamiltonian:
         terms = lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL
         taylor_partitioned(
             self.dom, psi, self._proj[key],
-            lambda x, p0, y, a: self.ham.apply_horner(x, p0, y, a, nst=nst, terms=terms, set_bc=False),
+            lambda x, p0, y, a, pts: self.ham.apply_horner(x, p0, y, a, nst=nst, terms=terms, set_bc=False,
+                                                           points=pts),
             bra=self.ham.projector_bra if kb else None,
             ket=(lambda p, y, a: self.ham.projector_ket(p, y, nst=nst, a=a)) if kb else None,
-            proj=self.projection_buffer(psi) if kb else None, dt=dt, order=order, nst=nst, group=group)
+            proj=self.projection_buffer(psi) if kb else None, dt=dt, order=order, nst=nst, group=group,
+            overlap=overlap)

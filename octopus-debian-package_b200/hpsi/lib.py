@@ -24,6 +24,9 @@ TERM_KINETIC = 1
 TERM_LOCAL_POTENTIAL = 2
 TERM_NON_LOCAL_POTENTIAL = 4
 TERM_ALL = 0x7FFFFFFF
+POINTS_ALL = 0
+POINTS_INNER = 1
+POINTS_OUTER = 2
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_INDEX", 3: "ERR_NONFINITE", 4: "ERR_CUDA", 5: "ERR_TIMEOUT",
           6: "ERR_STATE", 7: "ERR_NOMEM", 8: "ERR_RUNAWAY", 9: "ERR_UNSUPPORTED"}
@@ -95,6 +98,12 @@ SIGNATURES = {
                                        C.c_void_p]),
     "hpsi_apply_h_horner": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(Batch),
                                         C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_void_p]),
+    "hpsi_mesh_set_ghost_rows": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32]),
+    "hpsi_apply_h_points": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_int32, C.c_int32,
+                                        C.c_int32, C.c_void_p]),
+    "hpsi_apply_h_horner_points": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(Batch),
+                                               C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                                               C.c_void_p]),
     "hpsi_group_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "hpsi_group_destroy": (C.c_int32, [C.c_void_p]),
     "hpsi_group_taylor_steps": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.c_int32, C.c_double, C.c_int32,
@@ -220,6 +229,10 @@ class DeviceMesh:
         h = C.c_void_p()
         check(L.hpsi_mesh_create(C.byref(d), C.byref(h)))
         self.handle = h
+
+    def set_ghost_rows(self, first: int, count: int):
+        """Rows [first, first + count) are ghost rows (domain-parallel mesh)."""
+        check(load().hpsi_mesh_set_ghost_rows(self.handle, int(first), int(count)))
 
     def info(self):
         dims = (C.c_int32 * 6)()
@@ -433,11 +446,17 @@ class Hamiltonian:
             pass
 
     # X(hamiltonian_elec_apply_batch)
-    def apply(self, psi, hpsi, nst=None, terms=TERM_ALL, set_bc=True, stream=None):
+    def apply(self, psi, hpsi, nst=None, terms=TERM_ALL, set_bc=True, stream=None, points=POINTS_ALL):
+        """points: POINTS_ALL, or POINTS_INNER / POINTS_OUTER on a mesh with
+        ghost rows (hpsi_apply_h_points)."""
         bi = as_batch(psi, nst=nst)
         bo = as_batch(hpsi, nst=nst)
-        check(load().hpsi_apply_h(self.handle, C.byref(bi), C.byref(bo), terms, 1 if set_bc else 0,
-                                  _stream_ptr(stream)))
+        if points == POINTS_ALL:
+            check(load().hpsi_apply_h(self.handle, C.byref(bi), C.byref(bo), terms, 1 if set_bc else 0,
+                                      _stream_ptr(stream)))
+        else:
+            check(load().hpsi_apply_h_points(self.handle, C.byref(bi), C.byref(bo), terms, 1 if set_bc else 0,
+                                             int(points), _stream_ptr(stream)))
 
     def nprojections(self) -> int:
         n = C.c_int32()
@@ -460,12 +479,19 @@ class Hamiltonian:
         check(load().hpsi_projector_ket(self.handle, C.c_void_p(proj.data_ptr()), a.real, a.imag, C.byref(b),
                                         _stream_ptr(stream)))
 
-    def apply_horner(self, psi, psi0, out, a, nst=None, terms=TERM_ALL, set_bc=True, stream=None):
-        """out = psi0 + a H psi on the inner rows (hpsi_apply_h_horner)."""
+    def apply_horner(self, psi, psi0, out, a, nst=None, terms=TERM_ALL, set_bc=True, stream=None,
+                     points=POINTS_ALL):
+        """out = psi0 + a H psi on the inner rows (hpsi_apply_h_horner; with
+        points INNER / OUTER the part of hpsi_apply_h_horner_points)."""
         bi, b0, bo = as_batch(psi, nst=nst), as_batch(psi0, nst=nst), as_batch(out, nst=nst)
         a = complex(a)
-        check(load().hpsi_apply_h_horner(self.handle, C.byref(bi), C.byref(b0), C.byref(bo), a.real, a.imag,
-                                         terms, 1 if set_bc else 0, _stream_ptr(stream)))
+        if points == POINTS_ALL:
+            check(load().hpsi_apply_h_horner(self.handle, C.byref(bi), C.byref(b0), C.byref(bo), a.real, a.imag,
+                                             terms, 1 if set_bc else 0, _stream_ptr(stream)))
+        else:
+            check(load().hpsi_apply_h_horner_points(self.handle, C.byref(bi), C.byref(b0), C.byref(bo), a.real,
+                                                    a.imag, terms, 1 if set_bc else 0, int(points),
+                                                    _stream_ptr(stream)))
 
     def boundaries_set(self, psi, nst=None, stream=None):
         b = as_batch(psi, nst=nst)

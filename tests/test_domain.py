@@ -211,9 +211,22 @@ def _rank_kb_main(rank, world, port, out):
     Hl = O.Hamiltonian(d.mesh, w, star_points(), v=v[d.inner_rows], bc="none")
     b = d.local_batch(psi)
     b[d.np_local: d.np_local + d.np_ghost] = 0.0
-    x = torch.from_numpy(b)
-    y = torch.zeros((d.np_local, 3), dtype=torch.complex128)
     pr = torch.zeros((sum(mt.shape[1] for mt in lp.mats), 3), dtype=torch.complex128)
+    # the partition's points whose star reads no ghost row; the inner part
+    # runs on a copy whose ghost rows are NaN, so reading one would show
+    ghost = np.zeros(d.mesh.np_part, dtype=bool)
+    ghost[d.np_local: d.np_local + d.np_ghost] = True
+    clean = ~ghost[O.neighbour_table(d.mesh, star_points())].any(axis=1)
+
+    def part_rows(pts):
+        return slice(None) if pts == 0 else (clean if pts == 1 else ~clean)
+
+    def local_in(a, pts):
+        an = a.numpy()
+        if pts == 1:
+            an = an.copy()
+            an[ghost] = np.nan
+        return an
 
     def bra(a, p):
         p.copy_(torch.from_numpy(O.kb_bra(lp.maps, lp.mats, lp.scals, a.numpy()[: d.np_local])))
@@ -222,9 +235,18 @@ def _rank_kb_main(rank, world, port, out):
         hn = h.numpy()
         O.kb_ket(lp.maps, lp.mats, p.numpy(), hn)
 
-    apply_partitioned(d, x, y, lambda a, h: h.copy_(torch.from_numpy(Hl.apply(a.numpy()))),
-                      bra=bra, ket=ket, proj=pr, pack=pack, unpack=unpack)
-    err = float(np.max(np.abs(y.numpy() - ref[d.inner_rows])) / np.max(np.abs(ref)))
+    def local_apply(a, h, pts):
+        r = Hl.apply(local_in(a, pts))
+        h.numpy()[part_rows(pts)] = r[part_rows(pts)]
+
+    errs = []
+    for overlap in (False, True):
+        x = torch.from_numpy(b.copy())
+        y = torch.zeros((d.np_local, 3), dtype=torch.complex128)
+        apply_partitioned(d, x, y, local_apply, bra=bra, ket=ket, proj=pr, pack=pack, unpack=unpack,
+                          overlap=overlap)
+        errs.append(float(np.max(np.abs(y.numpy() - ref[d.inner_rows])) / np.max(np.abs(ref))))
+    err = max(errs)
 
     # Taylor step level by level (ghost update and projection sum per level)
     from hpsi.domain import taylor_partitioned
@@ -232,18 +254,23 @@ def _rank_kb_main(rank, world, port, out):
     ref_t = O.Hamiltonian(m, w, star_points(), v=v,
                           projectors=O.Projectors(proj.maps, proj.mats, proj.scals)).taylor(psi, dt)
 
-    def horner(a_in, p0, o, a):
-        o[: d.np_local] = p0[: d.np_local] + a * torch.from_numpy(Hl.apply(a_in.numpy()))
+    def horner(a_in, p0, o, a, pts):
+        r = p0.numpy()[: d.np_local] + a * Hl.apply(local_in(a_in, pts))
+        o.numpy()[: d.np_local][part_rows(pts)] = r[part_rows(pts)]
 
     def ket_a(p, h, a):
         hn = h.numpy()
         hn[: d.np_local] += a * O.kb_ket(lp.maps, lp.mats, p.numpy(), np.zeros((d.np_local, 3), complex))
 
-    x = torch.from_numpy(b.copy())
-    x[d.np_local: d.np_local + d.np_ghost] = 0.0
-    work = [torch.zeros_like(x), torch.zeros_like(x)]
-    taylor_partitioned(d, x, work, horner, bra=bra, ket=ket_a, proj=pr, dt=dt, order=4, pack=pack, unpack=unpack)
-    err_t = float(np.max(np.abs(x.numpy()[: d.np_local] - ref_t[d.inner_rows])) / np.max(np.abs(ref_t)))
+    errs_t = []
+    for overlap in (False, True):
+        x = torch.from_numpy(b.copy())
+        x[d.np_local: d.np_local + d.np_ghost] = 0.0
+        work = [torch.zeros_like(x), torch.zeros_like(x)]
+        taylor_partitioned(d, x, work, horner, bra=bra, ket=ket_a, proj=pr, dt=dt, order=4, pack=pack,
+                           unpack=unpack, overlap=overlap)
+        errs_t.append(float(np.max(np.abs(x.numpy()[: d.np_local] - ref_t[d.inner_rows])) / np.max(np.abs(ref_t))))
+    err_t = max(errs_t)
     dist.barrier()
     dist.destroy_process_group()
     out.put((rank, (err, err_t)))
@@ -287,7 +314,8 @@ def test_taylor_partitioned_single_partition_orders(order):
     work = [torch.zeros_like(x), torch.zeros_like(x)]
     pr = torch.zeros((sum(mt.shape[1] for mt in lp.mats), 2), dtype=torch.complex128)
 
-    def horner(a_in, p0, o, a):
+    def horner(a_in, p0, o, a, pts):
+        assert pts == 0
         o[: d.np_local] = p0[: d.np_local] + a * torch.from_numpy(Hl.apply(a_in.numpy()))
 
     def bra(a_in, p):

@@ -326,3 +326,76 @@ def test_domain_hamiltonian_methods_single_partition(cuda, dtype):
     tol_t = 1e-12 if dtype == "c128" else 1e-5
     got_t = xl.cpu().numpy()[: d.np_local]
     assert np.max(np.abs(got_t - ref_t[d.inner_rows])) <= tol_t * np.max(np.abs(ref_t))
+
+
+@pytest.mark.parametrize("dtype,horner", [("c128", False), ("c128", True), ("c64", False)])
+def test_inner_outer_split_reads_no_ghost_and_covers_every_row(cuda, dtype, horner):
+    """hpsi_apply_h_points / hpsi_apply_h_horner_points on the partitions of a
+    slab decomposition: the INNER part runs on batches whose ghost rows are
+    NaN (the exchange still in flight) and must not read them; the ghost rows
+    are then filled and the OUTER part runs; together they equal the ALL pass
+    on the filled batch bit for bit (the same arithmetic per output row) and
+    the global H psi."""
+    import torch
+    from hpsi import lib
+    from hpsi.domain import POINTS_INNER, POINTS_OUTER, DomainHamiltonian, partition_z
+    from hpsi.stencil import laplacian_weights, star_points
+    nst = 16
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    m, v, proj, psi = small_sphere_system(seed=59, nst=nst, radius=5.0, natoms=0)
+    w = laplacian_weights(m.spacing)
+    terms = lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL
+    H = lib.Hamiltonian(lib.DeviceMesh(m), w, star_points(), v=v)
+    xg = torch.from_numpy(np.ascontiguousarray(psi)).to(cuda).to(tdt)
+    yg = torch.zeros((m.np, nst), dtype=tdt, device=cuda)
+    H.apply(xg, yg, terms=terms)
+    ref = yg.cpu().numpy()
+    doms = partition_z(m, 3)
+    hams = [DomainHamiltonian(d, w, star_points(), v_global=v) for d in doms]
+    locs = [torch.from_numpy(d.local_batch(psi)).to(cuda).to(tdt) for d in doms]
+    for d, b in zip(doms, locs):
+        b[d.np_local: d.np_local + d.np_ghost] = float("nan")
+    a = 0.3 - 0.2j
+    outs = []
+    for d, hm, b in zip(doms, hams, locs):
+        y = torch.zeros((d.np_local, nst), dtype=tdt, device=cuda)
+        if horner:
+            p0 = b[: d.np_local].clone()
+            hm.ham.apply_horner(b, p0, y, a, terms=terms, set_bc=False, points=POINTS_INNER)
+        else:
+            hm.ham.apply(b, y, terms=terms, set_bc=False, points=POINTS_INNER)
+        outs.append(y)
+    _exchange_on_one_gpu(doms, locs, nst)
+    tol = 1e-13 if dtype == "c128" else 2e-6
+    n_inner = 0
+    for d, hm, b, y in zip(doms, hams, locs, outs):
+        ninner_rows = int(torch.count_nonzero(y.abs().sum(1)).item())
+        n_inner += ninner_rows
+        if horner:
+            p0 = b[: d.np_local].clone()
+            hm.ham.apply_horner(b, p0, y, a, terms=terms, set_bc=False, points=POINTS_OUTER)
+            full = torch.zeros_like(y)
+            hm.ham.apply_horner(b, p0, full, a, terms=terms, set_bc=False)
+        else:
+            hm.ham.apply(b, y, terms=terms, set_bc=False, points=POINTS_OUTER)
+            full = torch.zeros_like(y)
+            hm.ham.apply(b, full, terms=terms, set_bc=False)
+        assert not torch.isnan(y).any()
+        assert torch.equal(y, full)
+        if not horner:
+            assert np.max(np.abs(y.cpu().numpy() - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+    # the inner part holds a real share of the points (the overlap has work to hide the exchange)
+    assert n_inner >= m.np // 10
+
+
+def test_points_reject_kb_term(cuda):
+    import torch
+    from hpsi import lib
+    from hpsi.domain import POINTS_INNER
+    from hpsi.stencil import laplacian_weights, star_points
+    m, v, proj, psi = small_sphere_system(seed=61, nst=4)
+    H = lib.Hamiltonian(lib.DeviceMesh(m), laplacian_weights(m.spacing), star_points(), v=v, projectors=proj)
+    x = torch.from_numpy(psi).to(cuda)
+    y = torch.zeros((m.np, 4), dtype=torch.complex128, device=cuda)
+    with pytest.raises(lib.HpsiError):
+        H.apply(x, y, points=POINTS_INNER)
