@@ -519,6 +519,11 @@ hpsi_status hpsi_apply_h_horner_points(hpsi_hamiltonian *ham, const hpsi_batch *
 
 /* ------------------------------------------------------------------ */
 /* Library-wide controls and diagnostics. */
+/* Status word of the kernels of a Hamiltonian that wait on the hardware with a
+ * bound (the TMA fill of the stencil pass): HPSI_OK, or HPSI_ERR_TIMEOUT when a
+ * wait gave up (its pass's results are then invalid).  Waits for the device,
+ * returns the word and clears it. */
+hpsi_status hpsi_hamiltonian_status(hpsi_hamiltonian *ham, int32_t *status);
 const char *hpsi_last_error_string(void);
 /* Number of this library's kernels launched since load (diagnostic). */
 int64_t hpsi_kernel_launch_count(void);

@@ -228,11 +228,11 @@ PassShape blk_shape(int dtype) {
 
 PassShape default_shape(int dtype, long long ld) {
   PassShape s = ld % blk_shape(dtype).sc == 0 ? blk_shape(dtype) : legacy_shape(dtype, ld);
-  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx,cplx,ty"
+  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx,cplx,ty,tma"
   const char *env = std::getenv(dtype == HPSI_C128 ? "HPSI_PASS_SHAPE64" : "HPSI_PASS_SHAPE32");
   if (env) {
-    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0, cx = -1, ty = 0;
-    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx, &ty) >= 2 && a > 0 &&
+    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0, cx = -1, ty = 0, tm = 0;
+    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx, &ty, &tm) >= 2 && a > 0 &&
         ld % a == 0) {
       if (t) {
         s = blk_shape(dtype);  // chunk (128 or 64 bytes), block, element, z depth and group are taken
@@ -244,6 +244,7 @@ PassShape default_shape(int dtype, long long ld) {
         if (x > 0) s.rx = x;
         if (b > 0) s.ry = b;
         if (cx >= 0) s.cplx = cx;
+        s.tma = tm ? 1 : 0;
       } else {
         s = legacy_shape(dtype, ld);
         s.sc = a;
@@ -411,6 +412,7 @@ hpsi_status hpsi_mesh_create(const hpsi_mesh_desc *d, hpsi_mesh **out) {
   m->box = B;
   m->per_inner_h = per;
   m->cell_of_row_h = cell_of_row;
+  m->cell_row_h = cell_row;
   cudaGetDevice(&m->device);
   cudaDeviceGetAttribute(&m->num_sms, cudaDevAttrMultiProcessorCount, m->device);
   hpsi_status s = HPSI_OK;
@@ -464,6 +466,7 @@ hpsi_status hpsi_mesh_destroy(hpsi_mesh *m) {
   m->scratch2.release();
   for (auto &kv : m->items) dev_free(kv.second.first);
   for (auto &kv : m->items_part) dev_free(kv.second.first);
+  for (auto &kv : m->seg_masks) dev_free(kv.second);
   m->stage_in.release();
   m->stage_out.release();
   delete m;
@@ -515,6 +518,7 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   h->adjstep.release();
   h->vjpbuf.release();
   h->rhobuf.release();
+  dev_free(h->d_err);
   h->lzsmall.release();
   if (h->bra_stream) cudaStreamDestroy(h->bra_stream);
   if (h->bra_fork) cudaEventDestroy(h->bra_fork);
@@ -982,6 +986,83 @@ hpsi_status mesh_items_part(hpsi_mesh *m, int zb, int ty, int part, const int4 *
   return HPSI_OK;
 }
 
+// Per (16 x 8 tile column, cell plane) of the padded box, bit s set when star
+// segment s of the tile's halo plane (star cells 8 s .. 8 s + 7 in the order
+// of the blocked pass: 4 rows of 16 above, 8 rows of 24, 4 rows of 16 below,
+// HAL = 4) maps to eight consecutive rows of the batch through `src`.
+static std::vector<unsigned long long> seg_mask_table(const hpsi_mesh *m, const std::vector<int> &src) {
+  const CellBox &B = m->box;
+  const int HAL = 4, TX = 16, TY = 8, HX = TX + 2 * HAL;
+  std::vector<unsigned long long> t(size_t(m->tiles_y8) * m->tiles_x * B.NZ, 0ull);
+  for (int by = 0; by < m->tiles_y8; ++by)
+    for (int bx = 0; bx < m->tiles_x; ++bx) {
+      const int cx0 = HAL + bx * TX, cy0 = HAL + by * TY;
+      for (int q = 0; q < B.NZ; ++q) {
+        unsigned long long mask = 0;
+        for (int sgi = 0; sgi < 40; ++sgi) {
+          int first = -1;
+          bool ok = true;
+          for (int k = 0; k < 8 && ok; ++k) {
+            int i = 8 * sgi + k, hx, hy;  // star cell -> halo-plane coordinates
+            if (i < HAL * TX) {
+              hy = i / TX;
+              hx = HAL + i % TX;
+            } else if ((i -= HAL * TX) < TY * HX) {
+              hy = HAL + i / HX;
+              hx = i % HX;
+            } else {
+              i -= TY * HX;
+              hy = HAL + TY + i / TX;
+              hx = HAL + i % TX;
+            }
+            const int x = cx0 - HAL + hx, y = cy0 - HAL + hy;
+            const int r = (x < 0 || y < 0 || x >= B.NX || y >= B.NY) ? -1
+                                                                      : src[(size_t(q) * B.NY + y) * B.NX + x];
+            if (k == 0) first = r;
+            ok = r >= 0 && r == first + k;
+          }
+          if (ok) mask |= 1ull << sgi;
+        }
+        t[(size_t(by) * m->tiles_x + bx) * B.NZ + q] = mask;
+      }
+    }
+  return t;
+}
+
+hpsi_status prepare_tma(hpsi_hamiltonian *h, const int *src_map, long long in_rows, PassShape &shape, PassArgs &a) {
+  hpsi_mesh *m = h->mesh;
+  a.in_rows = in_rows;
+  if (!shape.tma) return HPSI_OK;
+  // tables exist for the raw and the zero-boundary maps; periodic images
+  // (and their Bloch phases) keep the per-cell copies
+  if (a.phase_corr || (src_map != m->d_src_raw && src_map != m->d_src_zero) || m->cell_row_h.empty()) {
+    shape.tma = 0;
+    return HPSI_OK;
+  }
+  auto it = m->seg_masks.find(src_map);
+  if (it == m->seg_masks.end()) {
+    std::vector<int> src(m->cell_row_h);
+    if (src_map == m->d_src_zero)
+      for (auto &r : src)
+        if (r >= m->np) r = -1;
+    const std::vector<unsigned long long> t = seg_mask_table(m, src);
+    unsigned long long *d = nullptr;
+    hpsi_status s = dev_alloc(reinterpret_cast<void **>(&d), std::max<size_t>(1, t.size()) * sizeof(unsigned long long));
+    if (s) return s;
+    HPSI_TRY_CUDA(cudaMemcpy(d, t.data(), t.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    it = m->seg_masks.emplace(src_map, d).first;
+  }
+  if (!h->d_err) {
+    hpsi_status s = dev_alloc(reinterpret_cast<void **>(&h->d_err), sizeof(int));
+    if (s) return s;
+    HPSI_TRY_CUDA(cudaMemset(h->d_err, 0, sizeof(int)));
+  }
+  a.seg_mask = it->second;
+  a.seg_tiles_x = m->tiles_x;
+  a.err = h->d_err;
+  return HPSI_OK;
+}
+
 // Build the pass arguments shared by apply and Taylor passes.
 void base_pass_args(const hpsi_hamiltonian *h, int terms, const int *src_map, PassArgs &a) {
   const hpsi_mesh *m = h->mesh;
@@ -1151,6 +1232,12 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
                               a);
       if (si) return si;
     }
+  }
+  if (shape.blk) {
+    si = prepare_tma(h, src_map, pass_in_rows(h, src_map), shape, a);
+    if (si) return si;
+  } else {
+    a.in_rows = pass_in_rows(h, src_map);
   }
   if (points != 0) {
     // one part of a domain-parallel mesh (no KB term, no observables)
@@ -1959,6 +2046,17 @@ hpsi_status hpsi_apply_h_horner_points(hpsi_hamiltonian *h, const hpsi_batch *ps
   return run_pass<float>(h, terms, load_map(h, set_bc), static_cast<const float *>(psi->ptr), ld,
                          static_cast<float *>(out->ptr), ld, ld, PASS_HORNER, static_cast<const float *>(psi0->ptr),
                          ld, a_re, a_im, nullptr, nullptr, st, nullptr, points);
+}
+
+hpsi_status hpsi_hamiltonian_status(hpsi_hamiltonian *h, int32_t *status) {
+  if (!h || !status) return HPSI_ERR_ARG;
+  *status = HPSI_OK;
+  if (!h->d_err) return HPSI_OK;
+  int v = 0;
+  HPSI_TRY_CUDA(cudaMemcpy(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  HPSI_TRY_CUDA(cudaMemset(h->d_err, 0, sizeof(int)));
+  *status = v;
+  return HPSI_OK;
 }
 
 }  // extern "C"

@@ -10,6 +10,11 @@
 namespace hpsi {
 
 hpsi_status dev_alloc(void **p, size_t bytes);
+struct PassArgs;
+struct PassShape;
+// TMA fill of a blocked pass: segment masks, status word and input extent in
+// `a`; clears shape.tma where the load map has no table (periodic images)
+hpsi_status prepare_tma(hpsi_hamiltonian *h, const int *src_map, long long in_rows, PassShape &shape, PassArgs &a);
 void dev_free(void *p);
 bool is_device_ptr(const void *p);
 
@@ -59,6 +64,10 @@ struct hpsi_mesh {
   // stencil reads no ghost row (part 1) and the rest (part 2), per (zb, ty)
   int ghost_first = 0, ghost_count = 0;
   std::map<int, std::pair<int4 *, int>> items_part;
+  // TMA fill: own row of every cell (host), and per load map the device table
+  // of contiguous star segments (PassArgs::seg_mask)
+  std::vector<int> cell_row_h;
+  std::map<const int *, unsigned long long *> seg_masks;
   int2 *d_col_z = nullptr;  // per (y, x) cell column: z range of its inner points
 };
 
@@ -115,6 +124,7 @@ struct hpsi_hamiltonian {
   hpsi::Workspace lzbuf, lzsmall;
   hpsi::Workspace vstage;  // host potential staged for hpsi_hamiltonian_update_vloc
   hpsi::Workspace adjstep, vjpbuf;  // per-step adjoint scratch, field VJP partials
-  hpsi::Workspace rhobuf;  // fused density: weights, pass and ket partials  // Lanczos: Krylov vectors, reductions and coefficients
+  hpsi::Workspace rhobuf;  // fused density: weights, pass and ket partials
+  int *d_err = nullptr;     // status word of the passes' bounded waits  // Lanczos: Krylov vectors, reductions and coefficients
   void proj_free();
 };

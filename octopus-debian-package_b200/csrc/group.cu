@@ -378,6 +378,11 @@ static hpsi_status autotune_t(hpsi_hamiltonian *h, int dtype, long long ld, cuda
       b4.ty = 8;
       blocks.push_back(b4);
     }
+    if (ld % b0.sc == 0) {
+      PassShape bt = b0;  // the default block with the TMA fill of contiguous halo runs
+      bt.tma = 1;
+      blocks.push_back(bt);
+    }
     for (const auto &b : blocks)
       for (int zb : {0, 16, 32, 48, 64, 1 << 20}) {
         PassShape c = b;
@@ -390,12 +395,15 @@ static hpsi_status autotune_t(hpsi_hamiltonian *h, int dtype, long long ld, cuda
   cudaEventCreate(&e1);
   double best = 1e30;
   PassShape best_shape = default_shape(dtype, ld);
-  for (const auto &sh : cands) {
+  for (const auto &sh0 : cands) {
     PassArgs a;
+    PassShape sh = sh0;
     r = build_pass_args<T>(h, HPSI_TERM_KINETIC | HPSI_TERM_LOCAL_POTENTIAL, load_map(h, 1),
                            static_cast<const T *>(in), ld, static_cast<T *>(out), ld, ld, PASS_APPLY, nullptr, 0,
                            0.0, 0.0, sh, a);
+    if (!r && sh.blk) r = prepare_tma(h, load_map(h, 1), m->np_part, sh, a);
     if (r) break;
+    if (sh0.tma && !sh.tma) continue;  // no TMA table for this load map
     for (int i = 0; i < 2 && !r; ++i) r = launch_pass_any<T>(a, sh, m->np, st);
     cudaEventRecord(e0, st);
     const int reps = 5;

@@ -22,6 +22,7 @@ struct PassArgs {
 
   const void *in;         // stencil input batch
   long long in_ld;        // complex numbers per row
+  long long in_rows;      // rows the input holds (the TMA fill's tensor extent)
   void *out;
   long long out_ld;
   const void *psi0;       // Horner: the untouched psi (pointwise term)
@@ -47,6 +48,13 @@ struct PassArgs {
   double *rho_part;       // [chunks][np], or null
   const double *rho_w;    // per state weight (ld entries)
 
+  // TMA fill of the blocked pass: per (16 x 8 tile, cell plane) a mask whose
+  // bit s marks star segment s (eight consecutive halo cells of one row) as
+  // eight consecutive rows of the input; [tiles_y][seg_tiles_x][NZ]
+  const unsigned long long *seg_mask;
+  int seg_tiles_x;
+  int *err;               // device status word of bounded waits (HPSI_ERR_TIMEOUT), or null
+
   const int2 *col_z;      // per (y, x) cell column: {first, last} z of its inner points
   const int4 *items;      // work items {tile x, tile y, first plane, end plane}
   int nitems;
@@ -63,6 +71,7 @@ struct PassShape {
   int blk = 0;     // 1: register-blocked real-lane pass (sc = its chunk, tiles 16 x 8)
   int rx = 0;      // blocked pass: cells per thread along x (ry along y)
   int cplx = 0;    // blocked pass: 1 = a thread owns a complex state, 0 = one real lane
+  int tma = 0;     // blocked pass: contiguous halo runs filled by TMA box copies
 };
 
 // Launch the fused pass for a storage type (double -> FP64, float -> FP32).

@@ -27,6 +27,8 @@
 // (src/grid/nl_operator_inc.F90:21-130), the local potential
 // (src/hamiltonian/hamiltonian_elec_base_inc.F90:233-242) and the Taylor
 // axpys (src/electrons/exponential.F90:738-746).
+#include <string>
+
 #include "stencil_blk_impl.cuh"
 
 namespace hpsi {
@@ -35,16 +37,20 @@ using namespace blk;
 
 namespace blk {
 // instantiated in stencil_blk_shapes.cu, one object per shape
-extern template hpsi_status launch_blk_u<double, 9, 2, 2, false, 8, 128>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<double, 3, 2, 2, false, 8, 128>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<double, 9, 2, 2, true, 8, 128>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<double, 9, 1, 4, false, 8, 64>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<double, 9, 1, 4, false, 16, 64>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<float, 9, 2, 2, true, 8, 128>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<float, 3, 2, 2, true, 8, 128>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<float, 1, 2, 4, false, 8, 128>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<float, 9, 1, 4, true, 8, 64>(const PassArgs &, cudaStream_t);
-extern template hpsi_status launch_blk_u<float, 9, 1, 4, true, 16, 64>(const PassArgs &, cudaStream_t);
+extern template hpsi_status launch_blk_u<double, 9, 2, 2, false, 8, 128>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<double, 3, 2, 2, false, 8, 128>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<double, 9, 2, 2, true, 8, 128>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<double, 9, 1, 4, false, 8, 64>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<double, 9, 1, 4, false, 16, 64>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<float, 9, 2, 2, true, 8, 128>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<float, 3, 2, 2, true, 8, 128>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<float, 1, 2, 4, false, 8, 128>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<float, 9, 1, 4, true, 8, 64>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<float, 9, 1, 4, true, 16, 64>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+extern template hpsi_status launch_blk_u<double, 9, 2, 2, false, 8, 128, true>(const PassArgs &, const CUtensorMap *,
+                                                                               cudaStream_t);
+extern template hpsi_status launch_blk_u<float, 9, 2, 2, true, 8, 128, true>(const PassArgs &, const CUtensorMap *,
+                                                                             cudaStream_t);
 }  // namespace blk
 
 
@@ -88,32 +94,85 @@ bool blk_pass_eligible(const PassArgs &a, long long ld, int sc) {
 //     FP64 real lanes, FP32 complex states (groups of 9);
 //   64-byte chunks, 16 x 8 tiles, 1 x 4 cells, 256 threads and two CTAs per
 //     SM (faster on small meshes: twice the CTAs per state chunk).
+// Tensor map of a pass input for the TMA fill: [in_rows][2 in_ld] elements of
+// the storage type, box 8 rows x one 128-byte chunk, no swizzle, zero fill
+// outside (never reached: only runs of eight existing rows are copied).
+// cuTensorMapEncodeTiled comes through the runtime's driver entry point.
+template <typename T>
+static hpsi_status encode_input_map(const PassArgs &a, CUtensorMap *tm) {
+  using enc_fn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static enc_fn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<enc_fn>(p);
+  });
+  if (!fn) {
+    set_error("launch_pass_blk: cuTensorMapEncodeTiled unavailable");
+    return HPSI_ERR_UNSUPPORTED;
+  }
+  const cuuint64_t dims[2] = {cuuint64_t(2 * a.in_ld), cuuint64_t(a.in_rows)};
+  const cuuint64_t strides[1] = {cuuint64_t(2 * a.in_ld) * sizeof(T)};
+  const cuuint32_t box[2] = {cuuint32_t(128 / sizeof(T)), 8};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(tm, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                        const_cast<void *>(a.in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("launch_pass_blk: cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+    return HPSI_ERR_CUDA;
+  }
+  return HPSI_OK;
+}
+
 template <typename T>
 hpsi_status launch_pass_blk(const PassArgs &a, const PassShape &s, cudaStream_t st) {
   if (a.nitems == 0) return HPSI_OK;
   const int cb = shape_cb<T>(s), g = s.unroll;
+  if (s.tma) {
+    // TMA fill: the default cell blocks (FP64 2 x 2 real lanes, FP32 2 x 2
+    // complex states), 16 x 8 tiles, 128-byte chunks, no Bloch phase
+    if (s.ty != 8 || cb != 128 || s.rx != 2 || s.ry != 2 || g != 9 || a.phase_corr || !a.seg_mask ||
+        s.cplx != (sizeof(T) == 8 ? 0 : 1) || a.in_rows <= 0) {
+      set_error("launch_pass_blk: no TMA-fill kernel for this pass");
+      return HPSI_ERR_UNSUPPORTED;
+    }
+    alignas(64) CUtensorMap tm;
+    hpsi_status r = encode_input_map<T>(a, &tm);
+    if (r) return r;
+    if constexpr (sizeof(T) == 8)
+      return launch_blk_u<T, 9, 2, 2, false, 8, 128, true>(a, &tm, st);
+    else
+      return launch_blk_u<T, 9, 2, 2, true, 8, 128, true>(a, &tm, st);
+  }
   if (s.ty == 8 && cb == 128) {
     if constexpr (sizeof(T) == 8) {
-      if (!s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, false, 8, 128>(a, st);
-      if (!s.cplx && s.rx == 2 && s.ry == 2 && g == 3) return launch_blk_u<T, 3, 2, 2, false, 8, 128>(a, st);
-      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, true, 8, 128>(a, st);
+      if (!s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, false, 8, 128>(a, nullptr, st);
+      if (!s.cplx && s.rx == 2 && s.ry == 2 && g == 3) return launch_blk_u<T, 3, 2, 2, false, 8, 128>(a, nullptr, st);
+      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, true, 8, 128>(a, nullptr, st);
     } else {
-      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, true, 8, 128>(a, st);
-      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 3) return launch_blk_u<T, 3, 2, 2, true, 8, 128>(a, st);
-      if (!s.cplx && s.rx == 2 && s.ry == 4 && g == 1) return launch_blk_u<T, 1, 2, 4, false, 8, 128>(a, st);
+      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 9) return launch_blk_u<T, 9, 2, 2, true, 8, 128>(a, nullptr, st);
+      if (s.cplx && s.rx == 2 && s.ry == 2 && g == 3) return launch_blk_u<T, 3, 2, 2, true, 8, 128>(a, nullptr, st);
+      if (!s.cplx && s.rx == 2 && s.ry == 4 && g == 1) return launch_blk_u<T, 1, 2, 4, false, 8, 128>(a, nullptr, st);
     }
   } else if (s.ty == 8 && cb == 64 && s.rx == 1 && s.ry == 4 && g == 9) {
     // 256-thread blocks, two CTAs per SM
     if constexpr (sizeof(T) == 8) {
-      if (!s.cplx) return launch_blk_u<T, 9, 1, 4, false, 8, 64>(a, st);
+      if (!s.cplx) return launch_blk_u<T, 9, 1, 4, false, 8, 64>(a, nullptr, st);
     } else {
-      if (s.cplx) return launch_blk_u<T, 9, 1, 4, true, 8, 64>(a, st);
+      if (s.cplx) return launch_blk_u<T, 9, 1, 4, true, 8, 64>(a, nullptr, st);
     }
   } else if (s.ty == 16 && cb == 64 && s.rx == 1 && s.ry == 4 && g == 9) {
     if constexpr (sizeof(T) == 8) {
-      if (!s.cplx) return launch_blk_u<T, 9, 1, 4, false, 16, 64>(a, st);
+      if (!s.cplx) return launch_blk_u<T, 9, 1, 4, false, 16, 64>(a, nullptr, st);
     } else {
-      if (s.cplx) return launch_blk_u<T, 9, 1, 4, true, 16, 64>(a, st);
+      if (s.cplx) return launch_blk_u<T, 9, 1, 4, true, 16, 64>(a, nullptr, st);
     }
   }
   set_error("launch_pass_blk: no kernel for this cell block");

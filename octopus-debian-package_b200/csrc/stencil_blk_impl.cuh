@@ -4,8 +4,11 @@
 // the shapes compile in parallel.
 #pragma once
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 #include <type_traits>
 #include "stencil.cuh"
@@ -98,7 +101,10 @@ struct BlkLayout {
   static constexpr size_t s_rows = size_t(HC) * sizeof(int);
   static constexpr size_t SIDEB = s_rows + size_t(IC) * sizeof(int);
   static constexpr size_t o_side = NBUF * STAGE;
-  static constexpr size_t bytes = o_side + NSIDE * SIDEB;
+  // TMA fill: one mbarrier per data stage after the side ring
+  static constexpr size_t o_mbar = o_side + NSIDE * SIDEB;
+  static constexpr size_t bytes = o_mbar;
+  static constexpr size_t bytes_tma = o_mbar + NBUF * 8;
   static_assert(bytes * CTAS <= 232448 - 2048, "shared memory per CTA");
   static_assert(STAGE % 16 == 0 && SIDEB % 16 == 0, "16-byte copies");
   static constexpr int NMAPP = HC / 4, NROWP = IC / 4, NVP = IC / 2;  // 16-byte side/v pieces
@@ -138,13 +144,55 @@ __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, i
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
 }
 
+// TMA fill helpers (hand-written PTX).  The tensor map covers the input batch
+// as [rows][2 ld] elements with a box of 8 rows x one 128-byte chunk; the
+// column coordinate is a chunk start (a multiple of 128 bytes).
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count));
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a), "r"(bytes) : "memory");
+}
+// true once the phase of the given parity has completed
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}\n"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_rows(void *dst, const CUtensorMap *tm, int x, int y, uint64_t *bar) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(d),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(b)
+      : "memory");
+}
+// polls of a stage's mbarrier before the pass gives up (a TMA copy that never
+// lands: the kernel records HPSI_ERR_TIMEOUT in p.err and finishes without
+// waiting further)
+constexpr unsigned TMA_WAIT_LIMIT = 1u << 22;
+
 // grid: nitems (16 x 8 tiles x z blocks) * chunks.
 // Plane k of a CTA is halo plane zbeg + k: data stage k % NBUF, side slot
 // k % NSIDE.  Iteration k computes plane k and issues the data of plane
 // k + NBUF - 1 and the side data of plane k + 2 NBUF - 2 (one commit group).
 // One work unit: item ih (16 x 8 tile, z block) and state chunk `chunk`.
-template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX_, int RY_, bool CPLX, int TY_, int CB_>
-__device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const int chunk, unsigned char *smem) {
+template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX_, int RY_, bool CPLX, int TY_, int CB_,
+          bool TMA = false>
+__device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const int chunk, unsigned char *smem,
+                                         const CUtensorMap *tm = nullptr) {
   constexpr bool X0 = HORNER || OBS;
   using LY = BlkLayout<T, X0, RX_, RY_, CPLX, TY_, CB_>;
   using E = typename BlkElem<T, CPLX>::E;
@@ -163,6 +211,15 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 
   auto stage = [&](int k) { return smem + size_t(k % NBUF) * LY::STAGE; };
   auto side = [&](int k) { return smem + LY::o_side + size_t(k % NSIDE) * LY::SIDEB; };
+  // TMA fill: star segment s (star cells 8 s .. 8 s + 7, eight consecutive
+  // cells of one halo row) is one box copy when bit s of the plane's mask is
+  // set (its rows are eight consecutive rows of the batch)
+  static_assert(!TMA || (LY::TX == 16 && LY::TY == 8 && LY::CELLB == 128 && LY::SC == 320),
+                "TMA fill: 16 x 8 tiles, 128-byte chunks");
+  auto mbar = [&](int k) { return reinterpret_cast<uint64_t *>(smem + LY::o_mbar) + (k % NBUF); };
+  [[maybe_unused]] const size_t mask_row = TMA ? (size_t(it.y) * p.seg_tiles_x + it.x) * B.NZ : 0;
+  [[maybe_unused]] bool tma_dead = false;
+  [[maybe_unused]] const bool smem_a128 = (static_cast<unsigned>(__cvta_generic_to_shared(smem)) & 127u) == 0;
 
   // ---- copy roles ---------------------------------------------------------------
   const int cpc = tid / PCS, piece = tid % PCS;  // cell (+ NT / PCS per round) and 16-byte piece
@@ -210,15 +267,33 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
     const unsigned char *sd = side(k);
     const int *map = reinterpret_cast<const int *>(sd);
     T *halo = reinterpret_cast<T *>(st) + piece * EPP;
+    [[maybe_unused]] unsigned long long mask = 0;
+    if constexpr (TMA) {
+      if (p.phase_corr == nullptr && smem_a128) mask = __ldg(p.seg_mask + mask_row + (zbeg + k));
+      // the stage's mbarrier expects the bytes of every box of the plane (its
+      // phase completes at once when the plane has none)
+      if (tid == 0) mbar_arrive_expect_tx(mbar(k), unsigned(__popcll(mask)) * 8u * LY::CELLB);
+    }
     if (p.phase_corr == nullptr) {
       // every entry is a row or -1 (zero): one zero-filling copy per piece
 #pragma unroll
       for (int j = 0; j < LY::SROUNDS; ++j) {
         const int i = cpc + j * (LY::NT / PCS);
         if (LY::SPART && j == LY::SROUNDS - 1 && i >= LY::SC) break;
+        if constexpr (TMA)
+          if ((mask >> (i >> 3)) & 1ull) continue;  // this cell arrives with its segment's box
         const int cell = star_cell<LY>(i);
         const int src = map[cell];
         cp_async16_zfill(halo + cell * SL, in_base + max(src, 0) * in_ld2, src >= 0 ? 16 : 0);
+      }
+      if constexpr (TMA) {
+        // thread s < 40 copies segment s
+        if (tid < 40 && ((mask >> tid) & 1ull)) {
+          // (the mask is cleared above when the dynamic shared memory is not
+          // 128-byte aligned: box copies need 128-byte aligned destinations)
+          const int cell = star_cell<LY>(8 * tid);
+          tma_load_rows(reinterpret_cast<T *>(st) + cell * SL, tm, col, map[cell], mbar(k));
+        }
       }
     } else {
 #pragma unroll 1
@@ -271,6 +346,12 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 
   // ---- prologue: side data of planes 0..NBUF-2 synchronously, then the first
   // NBUF-1 groups (data of planes 0..NBUF-2, side of planes NBUF-1..2NBUF-3)
+  if constexpr (TMA) {
+    if (tid == 0) {
+      for (int b = 0; b < NBUF; ++b) mbar_init(mbar(b), 1);
+      mbar_init_fence();
+    }
+  }
   for (int k = 0; k < NBUF - 1 && k < nplanes; ++k) {
     unsigned char *sd = side(k);
     const int q = zbeg + k;
@@ -350,6 +431,18 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
     constexpr int S4 = (4 + K) % 9;  // running sum of output plane zbeg + k
     cp_async_wait<NBUF - 2>();
     __syncthreads();
+    if constexpr (TMA) {
+      // the plane's boxes (each thread observes the phase itself)
+      if (!tma_dead) {
+        unsigned n = 0;
+        while (!mbar_try_wait(mbar(k), unsigned(k / NBUF) & 1u))
+          if (++n == TMA_WAIT_LIMIT) {
+            tma_dead = true;
+            if (tid == 0 && p.err) atomicExch(p.err, HPSI_ERR_TIMEOUT);
+            break;
+          }
+      }
+    }
     // the refill of the stage read in plane k - 1 is issued after this
     // plane's arithmetic (every thread passed the barrier above, so the stage
     // is free): the arithmetic starts right after the barrier
@@ -596,12 +689,13 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   }
 }
 
-template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB>
+template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA>
 __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::NT,
                                   BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::CTAS)
-    pass_blk_kernel(const __grid_constant__ PassArgs p) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  blk_body<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem);
+    pass_blk_kernel(const __grid_constant__ PassArgs p, const __grid_constant__ CUtensorMap tm) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  blk_body<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem,
+                                                               &tm);
 }
 
 // Many systems in one persistent launch (Horner passes): each CTA takes
@@ -610,7 +704,7 @@ template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
 __global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT,
                                   BlkLayout<T, true, RX, RY, CPLX, TY, CB>::CTAS)
     pass_blk_group_kernel(const __grid_constant__ GroupArgs g) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int unit_s;
   for (;;) {
     if (threadIdx.x == 0) unit_s = atomicAdd(g.counter, 1);
@@ -624,36 +718,43 @@ __global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT,
   }
 }
 
-template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB>
-hpsi_status launch_blk_mode(const PassArgs &a, cudaStream_t st) {
+template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA>
+hpsi_status launch_blk_mode(const PassArgs &a, const CUtensorMap *tm, cudaStream_t st) {
   using LY = BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>;
-  auto kern = pass_blk_kernel<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB>;
+  constexpr size_t SMEM = TMA ? LY::bytes_tma : LY::bytes;
+  auto kern = pass_blk_kernel<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
-    attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LY::bytes));
+    attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM));
     if (attr == cudaSuccess && LY::CTAS > 1)
       attr = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   });
   HPSI_TRY_CUDA(attr);
+  if (TMA && (!tm || !a.seg_mask)) {
+    set_error("launch_pass_blk: TMA fill without its tensor map or segment masks");
+    return HPSI_ERR_ARG;
+  }
+  CUtensorMap none;
+  std::memset(&none, 0, sizeof(none));
   const unsigned nblocks = unsigned(a.nitems) * unsigned(a.chunks);
-  kern<<<nblocks, LY::NT, LY::bytes, st>>>(a);
+  kern<<<nblocks, LY::NT, SMEM, st>>>(a, tm ? *tm : none);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
 }
 
-template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
-hpsi_status launch_blk_u(const PassArgs &a, cudaStream_t st) {
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA = false>
+hpsi_status launch_blk_u(const PassArgs &a, const CUtensorMap *tm, cudaStream_t st) {
   const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr, rho = a.rho_part != nullptr;
   if (rho && (!horner || obs)) {
     set_error("launch_pass_blk: the density is fused into Horner passes without observables only");
     return HPSI_ERR_UNSUPPORTED;
   }
-  if (horner && obs) return launch_blk_mode<T, true, true, false, U, RX, RY, CPLX, TY, CB>(a, st);
-  if (horner && rho) return launch_blk_mode<T, true, false, true, U, RX, RY, CPLX, TY, CB>(a, st);
-  if (horner) return launch_blk_mode<T, true, false, false, U, RX, RY, CPLX, TY, CB>(a, st);
-  if (obs) return launch_blk_mode<T, false, true, false, U, RX, RY, CPLX, TY, CB>(a, st);
-  return launch_blk_mode<T, false, false, false, U, RX, RY, CPLX, TY, CB>(a, st);
+  if (horner && obs) return launch_blk_mode<T, true, true, false, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
+  if (horner && rho) return launch_blk_mode<T, true, false, true, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
+  if (horner) return launch_blk_mode<T, true, false, false, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
+  if (obs) return launch_blk_mode<T, false, true, false, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
+  return launch_blk_mode<T, false, false, false, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
 }
 
 template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>

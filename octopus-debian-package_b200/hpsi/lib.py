@@ -98,6 +98,7 @@ SIGNATURES = {
                                        C.c_void_p]),
     "hpsi_apply_h_horner": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.POINTER(Batch),
                                         C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_void_p]),
+    "hpsi_hamiltonian_status": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32)]),
     "hpsi_mesh_set_ghost_rows": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32]),
     "hpsi_apply_h_points": (C.c_int32, [C.c_void_p, C.POINTER(Batch), C.POINTER(Batch), C.c_int32, C.c_int32,
                                         C.c_int32, C.c_void_p]),
@@ -457,6 +458,13 @@ class Hamiltonian:
         else:
             check(load().hpsi_apply_h_points(self.handle, C.byref(bi), C.byref(bo), terms, 1 if set_bc else 0,
                                              int(points), _stream_ptr(stream)))
+
+    def status(self) -> int:
+        """Status word of the bounded waits of this Hamiltonian's passes
+        (hpsi_hamiltonian_status: 0, or 5 = HPSI_ERR_TIMEOUT); clears it."""
+        st = C.c_int32()
+        check(load().hpsi_hamiltonian_status(self.handle, C.byref(st)))
+        return int(st.value)
 
     def nprojections(self) -> int:
         n = C.c_int32()
