@@ -382,6 +382,9 @@ static hpsi_status autotune_t(hpsi_hamiltonian *h, int dtype, long long ld, cuda
       PassShape bt = b0;  // the default block with the TMA fill of contiguous halo runs
       bt.tma = 1;
       blocks.push_back(bt);
+      PassShape bm = b0;  // the default block with the mbarrier hand-over of the stages
+      bm.mb = 1;
+      blocks.push_back(bm);
     }
     for (const auto &b : blocks)
       for (int zb : {0, 16, 32, 48, 64, 1 << 20}) {

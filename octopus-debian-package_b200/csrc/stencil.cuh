@@ -72,6 +72,7 @@ struct PassShape {
   int rx = 0;      // blocked pass: cells per thread along x (ry along y)
   int cplx = 0;    // blocked pass: 1 = a thread owns a complex state, 0 = one real lane
   int tma = 0;     // blocked pass: contiguous halo runs filled by TMA box copies
+  int mb = 0;      // blocked pass: stages handed over by mbarriers (split arrive / wait)
 };
 
 // Launch the fused pass for a storage type (double -> FP64, float -> FP32).

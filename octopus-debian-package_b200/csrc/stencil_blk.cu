@@ -16,7 +16,8 @@
 // stored as zeros and Bloch-phase images are multiplied on load.  The load
 // map of each plane and the output rows four planes below travel in a side
 // ring two stage rounds ahead of the data, so every gather knows its rows
-// when it is issued.  One __syncthreads per plane.
+// when it is issued.  One __syncthreads per plane (or, PassShape::mb, a full
+// and an empty mbarrier per stage: a warp may run a plane ahead).
 //
 // A TMA tile::gather4 fill of the same 128-byte chunks (one producer warp,
 // mbarrier hand-over) was measured 3x slower than this form on the same
@@ -51,6 +52,12 @@ extern template hpsi_status launch_blk_u<double, 9, 2, 2, false, 8, 128, true>(c
                                                                                cudaStream_t);
 extern template hpsi_status launch_blk_u<float, 9, 2, 2, true, 8, 128, true>(const PassArgs &, const CUtensorMap *,
                                                                              cudaStream_t);
+extern template hpsi_status launch_blk_u<double, 9, 2, 2, false, 8, 128, false, true>(const PassArgs &,
+                                                                                      const CUtensorMap *,
+                                                                                      cudaStream_t);
+extern template hpsi_status launch_blk_u<float, 9, 2, 2, true, 8, 128, false, true>(const PassArgs &,
+                                                                                    const CUtensorMap *,
+                                                                                    cudaStream_t);
 }  // namespace blk
 
 
@@ -150,6 +157,17 @@ hpsi_status launch_pass_blk(const PassArgs &a, const PassShape &s, cudaStream_t 
       return launch_blk_u<T, 9, 2, 2, false, 8, 128, true>(a, &tm, st);
     else
       return launch_blk_u<T, 9, 2, 2, true, 8, 128, true>(a, &tm, st);
+  }
+  if (s.mb) {
+    // mbarrier hand-over of the stages: the default cell blocks
+    if (s.ty != 8 || cb != 128 || s.rx != 2 || s.ry != 2 || g != 9 || s.cplx != (sizeof(T) == 8 ? 0 : 1)) {
+      set_error("launch_pass_blk: no mbarrier-pipelined kernel for this cell block");
+      return HPSI_ERR_UNSUPPORTED;
+    }
+    if constexpr (sizeof(T) == 8)
+      return launch_blk_u<T, 9, 2, 2, false, 8, 128, false, true>(a, nullptr, st);
+    else
+      return launch_blk_u<T, 9, 2, 2, true, 8, 128, false, true>(a, nullptr, st);
   }
   if (s.ty == 8 && cb == 128) {
     if constexpr (sizeof(T) == 8) {

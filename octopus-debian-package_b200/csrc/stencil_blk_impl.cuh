@@ -105,7 +105,10 @@ struct BlkLayout {
   static constexpr size_t o_mbar = o_side + NSIDE * SIDEB;
   static constexpr size_t bytes = o_mbar;
   static constexpr size_t bytes_tma = o_mbar + NBUF * 8;
+  // mbarrier hand-over: a full and an empty barrier per data stage
+  static constexpr size_t bytes_mb = o_mbar + 2 * NBUF * 8;
   static_assert(bytes * CTAS <= 232448 - 2048, "shared memory per CTA");
+  static_assert(bytes_mb * CTAS <= 232448, "shared memory per CTA (mbarrier hand-over)");
   static_assert(STAGE % 16 == 0 && SIDEB % 16 == 0, "16-byte copies");
   static constexpr int NMAPP = HC / 4, NROWP = IC / 4, NVP = IC / 2;  // 16-byte side/v pieces
   static_assert(NMAPP + NROWP <= NT && NVP <= NT, "one side piece per thread");
@@ -184,13 +187,36 @@ __device__ __forceinline__ void tma_load_rows(void *dst, const CUtensorMap *tm, 
 // waiting further)
 constexpr unsigned TMA_WAIT_LIMIT = 1u << 22;
 
+// mbarrier hand-over of the stages (hand-written PTX).  The arrive-on of a
+// thread's cp.async copies fires once all of them have landed; .noinc: the
+// barrier's expected count already includes it.
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(a) : "memory");
+}
+// plain arrive (release: the thread's earlier shared stores are visible to a
+// thread that observes the phase)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(a) : "memory");
+}
+
 // grid: nitems (16 x 8 tiles x z blocks) * chunks.
 // Plane k of a CTA is halo plane zbeg + k: data stage k % NBUF, side slot
 // k % NSIDE.  Iteration k computes plane k and issues the data of plane
 // k + NBUF - 1 and the side data of plane k + 2 NBUF - 2 (one commit group).
 // One work unit: item ih (16 x 8 tile, z block) and state chunk `chunk`.
+//
+// MB: the stages change hands through mbarriers instead of one
+// __syncthreads per plane.  Full barrier of a stage (2 NT arrivals per
+// phase): every thread's cp.async arrive-on plus its plain arrive (covering
+// its plain shared stores) after issuing a plane.  Empty barrier (NT): a
+// thread arrives when it is done with a plane; the refill of that plane's
+// stage waits for it.  The arrive comes after the arithmetic and the wait
+// after the next plane's arithmetic, so a warp may run one plane ahead of the
+// slowest one.  Every wait is bounded (HPSI_ERR_TIMEOUT in p.err).
 template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX_, int RY_, bool CPLX, int TY_, int CB_,
-          bool TMA = false>
+          bool TMA = false, bool MB = false>
 __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const int chunk, unsigned char *smem,
                                          const CUtensorMap *tm = nullptr) {
   constexpr bool X0 = HORNER || OBS;
@@ -219,6 +245,21 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   auto mbar = [&](int k) { return reinterpret_cast<uint64_t *>(smem + LY::o_mbar) + (k % NBUF); };
   [[maybe_unused]] const size_t mask_row = TMA ? (size_t(it.y) * p.seg_tiles_x + it.x) * B.NZ : 0;
   [[maybe_unused]] bool tma_dead = false;
+  static_assert(!(TMA && MB), "one stage hand-over per kernel");
+  // MB: full barrier of plane k's stage, empty barrier after it
+  [[maybe_unused]] auto full_bar = [&](int k) { return reinterpret_cast<uint64_t *>(smem + LY::o_mbar) + (k % NBUF); };
+  [[maybe_unused]] auto empty_bar = [&](int k) { return reinterpret_cast<uint64_t *>(smem + LY::o_mbar) + NBUF + (k % NBUF); };
+  [[maybe_unused]] bool mb_dead = false;
+  [[maybe_unused]] auto mb_wait = [&](uint64_t *bar, unsigned parity) {
+    if (mb_dead) return;
+    unsigned n = 0;
+    while (!mbar_try_wait(bar, parity))
+      if (++n == TMA_WAIT_LIMIT) {
+        mb_dead = true;
+        if (p.err) atomicExch(p.err, HPSI_ERR_TIMEOUT);
+        return;
+      }
+  };
   [[maybe_unused]] const bool smem_a128 = (static_cast<unsigned>(__cvta_generic_to_shared(smem)) & 127u) == 0;
 
   // ---- copy roles ---------------------------------------------------------------
@@ -352,6 +393,15 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
       mbar_init_fence();
     }
   }
+  if constexpr (MB) {
+    if (tid == 0) {
+      for (int b = 0; b < NBUF; ++b) {
+        mbar_init(full_bar(b), 2 * LY::NT);
+        mbar_init(empty_bar(b), LY::NT);
+      }
+      mbar_init_fence();
+    }
+  }
   for (int k = 0; k < NBUF - 1 && k < nplanes; ++k) {
     unsigned char *sd = side(k);
     const int q = zbeg + k;
@@ -368,7 +418,14 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   for (int k = 0; k < NBUF - 1; ++k) {
     issue_data(k);
     issue_side(k + NBUF - 1);
-    cp_async_commit();
+    if constexpr (MB) {
+      if (k < nplanes) {
+        cp_async_arrive_noinc(full_bar(k));
+        mbar_arrive(full_bar(k));
+      }
+    } else {
+      cp_async_commit();
+    }
   }
 
   // ---- compute roles --------------------------------------------------------------
@@ -429,8 +486,14 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   auto plane = [&](auto Kc, int k) {
     constexpr int K = decltype(Kc)::value;
     constexpr int S4 = (4 + K) % 9;  // running sum of output plane zbeg + k
-    cp_async_wait<NBUF - 2>();
-    __syncthreads();
+    if constexpr (MB) {
+      // the plane's copies and stores of every thread (and the side data of
+      // plane k + NBUF - 1, issued with them)
+      mb_wait(full_bar(k), unsigned(k / NBUF) & 1u);
+    } else {
+      cp_async_wait<NBUF - 2>();
+      __syncthreads();
+    }
     if constexpr (TMA) {
       // the plane's boxes (each thread observes the phase itself)
       if (!tma_dead) {
@@ -616,9 +679,23 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 #pragma unroll
         for (int r = 0; r < RY; ++r) acc[cx][r][K] = ezero<E>();
     }
-    issue_data(k + NBUF - 1);
-    issue_side(k + LY::SIDE_AHEAD);
-    cp_async_commit();
+    if constexpr (MB) {
+      mbar_arrive(empty_bar(k));  // this thread is done with plane k
+      const int kn = k + NBUF - 1;
+      if (kn < nplanes) {
+        // stage of plane k - 1 and the side slot of plane k + 2 NBUF - 2
+        // (last held plane k - 1 or earlier): every thread done with k - 1
+        if (k >= 1) mb_wait(empty_bar(k - 1), unsigned((k - 1) / NBUF) & 1u);
+        issue_data(kn);
+        issue_side(k + LY::SIDE_AHEAD);
+        cp_async_arrive_noinc(full_bar(kn));
+        mbar_arrive(full_bar(kn));
+      }
+    } else {
+      issue_data(k + NBUF - 1);
+      issue_side(k + LY::SIDE_AHEAD);
+      cp_async_commit();
+    }
   };
 
   auto rotate = [&]() {
@@ -689,13 +766,14 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   }
 }
 
-template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA>
+template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA,
+          bool MB>
 __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::NT,
                                   BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::CTAS)
     pass_blk_kernel(const __grid_constant__ PassArgs p, const __grid_constant__ CUtensorMap tm) {
   extern __shared__ __align__(128) unsigned char smem[];
-  blk_body<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks, smem,
-                                                               &tm);
+  blk_body<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA, MB>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks,
+                                                                   smem, &tm);
 }
 
 // Many systems in one persistent launch (Horner passes): each CTA takes
@@ -718,11 +796,12 @@ __global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT,
   }
 }
 
-template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA>
+template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA,
+          bool MB>
 hpsi_status launch_blk_mode(const PassArgs &a, const CUtensorMap *tm, cudaStream_t st) {
   using LY = BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>;
-  constexpr size_t SMEM = TMA ? LY::bytes_tma : LY::bytes;
-  auto kern = pass_blk_kernel<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA>;
+  constexpr size_t SMEM = TMA ? LY::bytes_tma : MB ? LY::bytes_mb : LY::bytes;
+  auto kern = pass_blk_kernel<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA, MB>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
@@ -743,18 +822,18 @@ hpsi_status launch_blk_mode(const PassArgs &a, const CUtensorMap *tm, cudaStream
   return HPSI_OK;
 }
 
-template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA = false>
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA = false, bool MB = false>
 hpsi_status launch_blk_u(const PassArgs &a, const CUtensorMap *tm, cudaStream_t st) {
   const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr, rho = a.rho_part != nullptr;
   if (rho && (!horner || obs)) {
     set_error("launch_pass_blk: the density is fused into Horner passes without observables only");
     return HPSI_ERR_UNSUPPORTED;
   }
-  if (horner && obs) return launch_blk_mode<T, true, true, false, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
-  if (horner && rho) return launch_blk_mode<T, true, false, true, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
-  if (horner) return launch_blk_mode<T, true, false, false, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
-  if (obs) return launch_blk_mode<T, false, true, false, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
-  return launch_blk_mode<T, false, false, false, U, RX, RY, CPLX, TY, CB, TMA>(a, tm, st);
+  if (horner && obs) return launch_blk_mode<T, true, true, false, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
+  if (horner && rho) return launch_blk_mode<T, true, false, true, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
+  if (horner) return launch_blk_mode<T, true, false, false, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
+  if (obs) return launch_blk_mode<T, false, true, false, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
+  return launch_blk_mode<T, false, false, false, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
 }
 
 template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>

@@ -1,6 +1,6 @@
 // Explicit instantiations of the register-blocked pass, one cell-block shape
 // per object: the Makefile compiles this file once per HPSI_BLK_SHAPE
-// (0..11), so that the shapes, each a 9-plane unrolled kernel in five modes,
+// (0..13), so that the shapes, each a 9-plane unrolled kernel in five modes,
 // compile in parallel.  The list matches the extern declarations in
 // stencil_blk.cu.
 #include "stencil_blk_impl.cuh"
@@ -36,6 +36,12 @@ template hpsi_status launch_blk_u<float, 9, 1, 4, true, 16, 64>(const PassArgs &
 template hpsi_status launch_blk_u<double, 9, 2, 2, false, 8, 128, true>(const PassArgs &, const CUtensorMap *, cudaStream_t);
 #elif HPSI_BLK_SHAPE == 11
 template hpsi_status launch_blk_u<float, 9, 2, 2, true, 8, 128, true>(const PassArgs &, const CUtensorMap *, cudaStream_t);
+#elif HPSI_BLK_SHAPE == 12
+template hpsi_status launch_blk_u<double, 9, 2, 2, false, 8, 128, false, true>(const PassArgs &, const CUtensorMap *,
+                                                                               cudaStream_t);
+#elif HPSI_BLK_SHAPE == 13
+template hpsi_status launch_blk_u<float, 9, 2, 2, true, 8, 128, false, true>(const PassArgs &, const CUtensorMap *,
+                                                                             cudaStream_t);
 #else
 #error "unknown HPSI_BLK_SHAPE"
 #endif
