@@ -228,11 +228,12 @@ PassShape blk_shape(int dtype) {
 
 PassShape default_shape(int dtype, long long ld) {
   PassShape s = ld % blk_shape(dtype).sc == 0 ? blk_shape(dtype) : legacy_shape(dtype, ld);
-  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx,cplx,ty,tma,mb"
+  // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx,cplx,ty,tma,mb,mma"
   const char *env = std::getenv(dtype == HPSI_C128 ? "HPSI_PASS_SHAPE64" : "HPSI_PASS_SHAPE32");
   if (env) {
-    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0, cx = -1, ty = 0, tm = 0, mb = 0;
-    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx, &ty, &tm, &mb) >= 2 && a > 0 &&
+    int a = 0, b = 0, c = 0, u = 0, t = 0, x = 0, cx = -1, ty = 0, tm = 0, mb = 0, mm = 0;
+    if (std::sscanf(env, "%d,%d,%d,%d,%d,%d,%d,%d,%d,%d,%d", &a, &b, &c, &u, &t, &x, &cx, &ty, &tm, &mb, &mm) >= 2 &&
+        a > 0 &&
         ld % a == 0) {
       if (t) {
         s = blk_shape(dtype);  // chunk (128 or 64 bytes), block, element, z depth and group are taken
@@ -246,6 +247,7 @@ PassShape default_shape(int dtype, long long ld) {
         if (cx >= 0) s.cplx = cx;
         s.tma = tm ? 1 : 0;
         s.mb = mb ? 1 : 0;
+        s.mma = mm ? 1 : 0;
       } else {
         s = legacy_shape(dtype, ld);
         s.sc = a;

@@ -73,6 +73,7 @@ struct PassShape {
   int cplx = 0;    // blocked pass: 1 = a thread owns a complex state, 0 = one real lane
   int tma = 0;     // blocked pass: contiguous halo runs filled by TMA box copies
   int mb = 0;      // blocked pass: stages handed over by mbarriers (split arrive / wait)
+  int mma = 0;     // FP64 blocked pass with the x and y arms on the FP64 tensor cores (DMMA)
 };
 
 // Launch the fused pass for a storage type (double -> FP64, float -> FP32).

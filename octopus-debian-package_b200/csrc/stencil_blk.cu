@@ -158,6 +158,14 @@ hpsi_status launch_pass_blk(const PassArgs &a, const PassShape &s, cudaStream_t 
     else
       return launch_blk_u<T, 9, 2, 2, true, 8, 128, true>(a, &tm, st);
   }
+  if (s.mma) {
+    // FP64 only: in-plane arms as DMMA banded products, 8-state chunks
+    if (sizeof(T) != 8 || cb != 128 || s.ty != 8) {
+      set_error("launch_pass_blk: the tensor-core pass is FP64 with 8-state chunks");
+      return HPSI_ERR_UNSUPPORTED;
+    }
+    return launch_pass_mma(a, st);
+  }
   if (s.mb) {
     // mbarrier hand-over of the stages: the default cell blocks
     if (s.ty != 8 || cb != 128 || s.rx != 2 || s.ry != 2 || g != 9 || s.cplx != (sizeof(T) == 8 ? 0 : 1)) {

@@ -24,6 +24,10 @@ bool blk_pass_eligible(const PassArgs &a, long long ld, int sc);
 template <typename T>
 hpsi_status launch_pass_blk(const PassArgs &a, const PassShape &shape, cudaStream_t st);
 
+// FP64 pass with the in-plane arms on the FP64 tensor cores (stencil_mma.cu):
+// 16 x 8 tiles, chunks of 8 complex states, no fused density.
+hpsi_status launch_pass_mma(const PassArgs &a, cudaStream_t st);
+
 // Grouped systems in one persistent launch (Horner passes): every system's
 // arguments built with the blocked shape (items over 16 x 8 tiles).
 template <typename T>
