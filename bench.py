@@ -472,6 +472,32 @@ def run_configs(args):
           "grad_eps_norm": float(np.linalg.norm(ge)), "grad_v_norm": float(np.linalg.norm(gv))})
 
 
+def _adjoint_extra(dev, small):
+    """Config 4 in the headline line: one adjoint gradient (64^3 box, 16 states,
+    500 steps, checkpoints every 25), wall time around the call."""
+    import torch
+    from hpsi import fixtures, lib
+    from hpsi.stencil import laplacian_weights, star_points
+    s0 = fixtures.config0(nst=16)
+    m = s0.mesh
+    dm = lib.DeviceMesh(m)
+    ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=s0.v)
+    nsteps = 100 if small else 500
+    eps = np.random.default_rng(7).normal(0.0, 0.005, nsteps)
+    psi0 = torch.from_numpy(s0.psi).to(dev)
+    tg = torch.from_numpy(fixtures.random_states(m, 16, np.random.default_rng(8))).to(dev)
+    ham.adjoint_gradient(psi0, tg, eps[:4], 0.01, ckpt=2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, ge, gv, gc = ham.adjoint_gradient(psi0, tg, eps, 0.01, ckpt=25)
+    el = time.perf_counter() - t0
+    ham.close()
+    dm.close()
+    return {"workload": f"adjoint gradient, box 64^3 h=0.25, 16 states, {nsteps} steps dt=0.01, checkpoint 25",
+            "seconds_per_gradient": el, "forward_equiv_steps_per_s": nsteps / el, "J": J,
+            "grad_eps_norm": float(np.linalg.norm(ge))}
+
+
 def _group_extra(dev, small, timed):
     """Config 3: uneven independent systems advanced together (one persistent
     stencil launch per Horner level, CUDA graph), FP64 and FP32 storage.
@@ -664,6 +690,7 @@ def main():
     # ---- other configurations, measured in the same run --------------------------
     box = _box_extra(dev, timed, args.steps)
     group = _group_extra(dev, args.small, timed)
+    adjoint = _adjoint_extra(dev, args.small)
 
     # ---- e2e through the C ABI with pinned host buffers -----------------------
     xh = torch.from_numpy(sysm.psi).pin_memory()
@@ -719,6 +746,7 @@ def main():
                 **td,
                 "config0_box64": box,
                 "config3_group": group,
+                "config4_adjoint": adjoint,
             },
         }
         if err is not None:

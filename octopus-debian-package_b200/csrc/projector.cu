@@ -66,13 +66,26 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
   const int tid = threadIdx.x, warp = tid >> 5, ln = tid & 31;
   constexpr int EPC = 16 / int(sizeof(T));  // elements per 16-byte copy
 
+  // the map entries of the next staged block are loaded one block ahead into
+  // registers, so a row copy never waits for its own index load
+  constexpr int NIT = KB * CPR / 128;  // row pieces per thread and block
+  static_assert(KB * CPR % 128 == 0, "whole rounds of row pieces");
+  int mrow[NIT];
+  auto load_map = [&](int k0) {
+#pragma unroll
+    for (int t = 0; t < NIT; ++t) {
+      const int k = (tid + 128 * t) / CPR;
+      mrow[t] = k0 + k < npts ? __ldg(map + k0 + k) : 0;
+    }
+  };
   auto stage = [&](int k0, int b) {
-    for (int i = tid; i < KB * CPR; i += 128) {
+#pragma unroll
+    for (int t = 0; t < NIT; ++t) {
+      const int i = tid + 128 * t;
       const int k = i / CPR, part = i % CPR;
       T *d = &sA[b][k][part * EPC];
       if (k0 + k < npts && l0 + part * EPC < ld2) {
-        const int row = __ldg(map + k0 + k);
-        cp_async16(d, psi + row * ld2 + l0 + part * EPC);
+        cp_async16(d, psi + mrow[t] * ld2 + l0 + part * EPC);
       } else {
         *reinterpret_cast<float4 *>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
       }
@@ -86,14 +99,18 @@ __global__ void __launch_bounds__(128) bra_dmma_kernel(const ProjArgs p) {
 
   double c0[2] = {0.0, 0.0}, c1[2] = {0.0, 0.0};
   const int nblk = (npts + KB - 1) / KB;
+  load_map(0);
   if (nblk > 0) stage(0, 0);
   cp_async_commit();
+  load_map(KB);
   if (nblk > 1) stage(KB, 1);
   cp_async_commit();
+  load_map(2 * KB);
   for (int blk = 0; blk < nblk; ++blk) {
     const int b = blk % NS;
     if (blk + 2 < nblk) stage((blk + 2) * KB, (blk + 2) % NS);
     cp_async_commit();
+    load_map((blk + 3) * KB);
     cp_async_wait<2>();
     __syncthreads();
 #pragma unroll
