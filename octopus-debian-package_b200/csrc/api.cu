@@ -1468,13 +1468,14 @@ hpsi_status stage_batch(Workspace &ws, const hpsi_batch *b, int rows, bool copy_
 // boundary rows are then never read), np_part otherwise.
 template <typename T>
 hpsi_status apply_h_host_pipelined(hpsi_hamiltonian *h, const hpsi_batch *psi, hpsi_batch *hpsi, int terms,
-                                   int set_bc, long long w, cudaStream_t st) {
+                                   int set_bc, const std::vector<long long> &widths, cudaStream_t st) {
   hpsi_mesh *m = h->mesh;
   const size_t esz = 2 * sizeof(T);
   const long long ld = psi->ld, ldo = hpsi->ld;
-  const int nslab = int(ld / w);
+  const int nslab = int(widths.size());
+  const long long wmax = *std::max_element(widths.begin(), widths.end());
   const int rows_in = set_bc ? m->np : m->np_part;
-  const size_t in_bytes = size_t(m->np_part) * w * esz, out_bytes = size_t(m->np) * w * esz;
+  const size_t in_bytes = size_t(m->np_part) * wmax * esz, out_bytes = size_t(m->np) * wmax * esz;
   hpsi_status s = h->slab_in.ensure(2 * in_bytes);
   if (!s) s = h->slab_out.ensure(2 * out_bytes);
   if (s) return s;
@@ -1488,11 +1489,14 @@ hpsi_status apply_h_host_pipelined(hpsi_hamiltonian *h, const hpsi_batch *psi, h
   HPSI_TRY_CUDA(cudaEventRecord(comp_done[0], st));
   HPSI_TRY_CUDA(cudaStreamWaitEvent(h->xfer_in, comp_done[0], 0));
   HPSI_TRY_CUDA(cudaStreamWaitEvent(h->xfer_out, comp_done[0], 0));
+  long long c0 = 0;  // first state of slab i
   for (int i = 0; i < nslab; ++i) {
     const int b = i & 1;
+    const long long w = widths[i];
     T *din = reinterpret_cast<T *>(static_cast<char *>(h->slab_in.ptr) + b * in_bytes);
     T *dout = reinterpret_cast<T *>(static_cast<char *>(h->slab_out.ptr) + b * out_bytes);
-    const size_t col = size_t(i) * w * esz;
+    const size_t col = size_t(c0) * esz;
+    c0 += w;
     if (i >= 2) HPSI_TRY_CUDA(cudaStreamWaitEvent(h->xfer_in, comp_done[b], 0));
     HPSI_TRY_CUDA(cudaMemcpy2DAsync(din, w * esz, static_cast<const char *>(psi->ptr) + col, ld * esz, w * esz,
                                     rows_in, cudaMemcpyHostToDevice, h->xfer_in));
@@ -1503,8 +1507,8 @@ hpsi_status apply_h_host_pipelined(hpsi_hamiltonian *h, const hpsi_batch *psi, h
     if (s) return s;
     HPSI_TRY_CUDA(cudaEventRecord(comp_done[b], st));
     HPSI_TRY_CUDA(cudaStreamWaitEvent(h->xfer_out, comp_done[b], 0));
-    HPSI_TRY_CUDA(cudaMemcpy2DAsync(static_cast<char *>(hpsi->ptr) + size_t(i) * w * esz, ldo * esz, dout, w * esz,
-                                    w * esz, m->np, cudaMemcpyDeviceToHost, h->xfer_out));
+    HPSI_TRY_CUDA(cudaMemcpy2DAsync(static_cast<char *>(hpsi->ptr) + col, ldo * esz, dout, w * esz, w * esz, m->np,
+                                    cudaMemcpyDeviceToHost, h->xfer_out));
     HPSI_TRY_CUDA(cudaEventRecord(out_done[b], h->xfer_out));
   }
   HPSI_TRY_CUDA(cudaStreamSynchronize(h->xfer_out));
@@ -1512,21 +1516,43 @@ hpsi_status apply_h_host_pipelined(hpsi_hamiltonian *h, const hpsi_batch *psi, h
   return HPSI_OK;
 }
 
-// State slab width of the host pipeline: the most slabs (at most 4, override
-// HPSI_HOST_SLABS) whose width is a multiple of the blocked pass's chunk; 0
-// when the batch does not split.  Measured on 904,089 x 128 complex128 (two
-// 1.85 GB copies at 53-56 GB/s each way): 2 slabs 55.0 ms, 4 slabs 46.7 ms,
-// 8 slabs 53.5 ms (the strided copies of narrow slabs lose bandwidth); four
-// slabs with the last split in two halves (a shorter copy-back tail) measured
-// within the run-to-run spread of four.
-long long pipeline_slab(const hpsi_batch *psi, const hpsi_batch *hpsi) {
+// State slabs of the host pipeline (widths in states, each a multiple of the
+// blocked pass's chunk, summing to the batch width); empty when the batch does
+// not split.  Default: the most equal slabs, at most 4.  Measured on
+// 904,089 x 128 complex128 (two 1.85 GB copies at 53-56 GB/s each way): 2
+// slabs 55.0 ms, 4 slabs 46.7 ms, 8 slabs 53.5 ms (the strided copies of
+// narrow slabs lose bandwidth).  Tapered splits, which shorten the exposed
+// first copy-in and last copy-out, measured slower still: 16,32,32,32,16
+// 47.2 ms, 8,24,32,32,24,8 49.2 ms, 24,40,40,24 51.3 ms, 16,48,48,16 50.6 ms
+// against 46.4 ms for 4 x 32 (copies of 512-byte row pieces run fastest).
+// HPSI_HOST_SLAB_WIDTHS (a comma-separated list of widths) overrides the split
+// when it is valid for the batch.
+std::vector<long long> pipeline_slabs(const hpsi_batch *psi, const hpsi_batch *hpsi) {
   const long long chunk = psi->dtype == HPSI_C128 ? blk_chunk_states<double>() : blk_chunk_states<float>();
-  if (psi->ld != hpsi->ld || psi->nst != psi->ld) return 0;
+  std::vector<long long> out;
+  if (psi->ld != hpsi->ld || psi->nst != psi->ld) return out;
+  if (const char *e = std::getenv("HPSI_HOST_SLAB_WIDTHS")) {
+    long long sum = 0;
+    bool ok = true;
+    for (const char *q = e; *q;) {
+      char *end = nullptr;
+      const long long w = std::strtoll(q, &end, 10);
+      if (end == q || w <= 0 || w % chunk != 0) {
+        ok = false;
+        break;
+      }
+      out.push_back(w);
+      sum += w;
+      q = *end == ',' ? end + 1 : end;
+    }
+    if (ok && sum == psi->ld && out.size() >= 2) return out;
+    out.clear();
+  }
   int maxslab = 4;
   if (const char *e = std::getenv("HPSI_HOST_SLABS")) maxslab = std::max(1, std::atoi(e));
   for (int nslab = maxslab; nslab >= 2; --nslab)
-    if (psi->ld % (nslab * chunk) == 0) return psi->ld / nslab;
-  return 0;
+    if (psi->ld % (nslab * chunk) == 0) return std::vector<long long>(nslab, psi->ld / nslab);
+  return out;
 }
 
 }  // namespace hpsi
@@ -1551,10 +1577,10 @@ hpsi_status hpsi_apply_h(hpsi_hamiltonian *h, const hpsi_batch *psi, hpsi_batch 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const bool din = is_device_ptr(psi->ptr), dout = is_device_ptr(hpsi->ptr);
   if (!din && !dout) {
-    const long long w = pipeline_slab(psi, hpsi);
-    if (w > 0)
-      return psi->dtype == HPSI_C128 ? apply_h_host_pipelined<double>(h, psi, hpsi, terms, set_bc, w, st)
-                                     : apply_h_host_pipelined<float>(h, psi, hpsi, terms, set_bc, w, st);
+    const std::vector<long long> widths = pipeline_slabs(psi, hpsi);
+    if (!widths.empty())
+      return psi->dtype == HPSI_C128 ? apply_h_host_pipelined<double>(h, psi, hpsi, terms, set_bc, widths, st)
+                                     : apply_h_host_pipelined<float>(h, psi, hpsi, terms, set_bc, widths, st);
   }
   const void *pin = psi->ptr;
   void *pout = hpsi->ptr;
