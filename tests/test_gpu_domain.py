@@ -1,11 +1,21 @@
 """Domain-parallel H psi on one GPU: the partitions run one after another in
 this process, their ghost rows packed by hpsi_ghost_pack and delivered by
 device copies (the part NCCL does between GPUs) or hpsi_ghost_unpack; the
-partitions' H psi must equal the global H psi of the same states."""
+partitions' H psi must equal the global H psi of the same states, and the
+assembled partitioned result is also checked against the FP64 CPU oracle at
+the parity tolerances (FP64 1e-12, FP32 storage 2e-5, relative max-norm per
+state)."""
 import numpy as np
 import pytest
 
-from helpers import small_sphere_system
+from helpers import rel_maxnorm_per_state, small_sphere_system
+
+
+def _oracle(m, w, v, proj=None):
+    from hpsi.stencil import star_points
+    from oracle import oracle as O
+    P = O.Projectors(proj.maps, proj.mats, proj.scals) if proj is not None else None
+    return O.Hamiltonian(m, w, star_points(), v=v, projectors=P)
 
 pytestmark = pytest.mark.gpu
 
@@ -65,6 +75,7 @@ def test_partitioned_hpsi_equals_global(cuda, nparts, ld, dtype):
         locs.append(torch.from_numpy(b).to(cuda).to(tdt))
     _exchange_on_one_gpu(doms, locs, nst)
     tol = 1e-13 if dtype == "c128" else 2e-6
+    full = np.zeros((m.np, nst), dtype=np.complex128)
     for d, hm, b in zip(doms, hams, locs):
         n = d.np_local + d.np_ghost
         assert np.array_equal(b.cpu().numpy()[:n, :nst], g[d.global_rows[:n], :nst].astype(b.cpu().numpy().dtype))
@@ -72,6 +83,8 @@ def test_partitioned_hpsi_equals_global(cuda, nparts, ld, dtype):
         hm.ham.apply(b, out, nst=nst, set_bc=False)
         got = out.cpu().numpy()[:, :nst]
         assert np.max(np.abs(got - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+        full[d.inner_rows] = got
+    assert rel_maxnorm_per_state(full, _oracle(m, w, v).apply(psi)) <= (1e-12 if dtype == "c128" else 2e-5)
 
 
 def test_ghost_pack_rejects_host_buffers(cuda):
@@ -157,12 +170,15 @@ def test_partitioned_hpsi_with_kb_equals_global(cuda, nparts, ld, dtype):
         shares.append(pr)
     total = torch.stack(shares).sum(0)
     tol = 1e-13 if dtype == "c128" else 2e-6
+    full = np.zeros((m.np, nst), dtype=np.complex128)
     for d, hm, b in zip(doms, hams, locs):
         out = torch.zeros((d.np_local, ld), dtype=tdt, device=cuda)
         hm.ham.apply(b, out, nst=nst, terms=lib.TERM_KINETIC | lib.TERM_LOCAL_POTENTIAL, set_bc=False)
         hm.ham.projector_ket(total, out, nst=nst)
         got = out.cpu().numpy()[:, :nst]
         assert np.max(np.abs(got - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+        full[d.inner_rows] = got
+    assert rel_maxnorm_per_state(full, _oracle(m, w, v, proj).apply(psi)) <= (1e-12 if dtype == "c128" else 2e-5)
 
 
 @pytest.mark.parametrize("dtype", ["c128", "c64"])
@@ -268,9 +284,13 @@ def test_partitioned_taylor_step_equals_global(cuda, nparts, ld, dtype):
             outs.append(out)
         xs = outs
     tol = 1e-12 if dtype == "c128" else 1e-5
+    full = np.zeros((m.np, nst), dtype=np.complex128)
     for d, p in zip(doms, psis):
         got = p.cpu().numpy()[: d.np_local, :nst]
         assert np.max(np.abs(got - ref[d.inner_rows])) <= tol * np.max(np.abs(ref))
+        full[d.inner_rows] = got
+    oref = _oracle(m, w, v, proj).taylor(psi, dt, order=order)
+    assert rel_maxnorm_per_state(full, oref) <= (1e-12 if dtype == "c128" else 2e-5)
 
 
 def test_apply_h_horner_matches_apply(cuda):
