@@ -262,17 +262,22 @@ hpsi_status launch_bra(const ProjArgs &p, bool use_tensor, int ksplit, cudaStrea
 // energy partial Re(conj(psi0[row]) h) per state.  Each output element is
 // written by exactly one thread, in a fixed order: no atomics, deterministic.
 namespace {
-template <typename T, typename C2, bool PHASE>
+// RPW rows per warp: 1 for batches wider than 16 states; narrow batches (at
+// most 16 or 8 states) put 2 or 4 rows in a warp, one lane group of 32 / RPW
+// lanes per row, so the lanes past the batch width do not idle.
+template <typename T, typename C2, bool PHASE, int RPW = 1>
 __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
   // each thread serves two states (sb, sb + 32) of its rows: the row's
   // metadata and projector weights are loaded once for both (12 % faster than
   // one state per thread on the R = 12 sphere, 128 states; four states per
   // thread measured 30 % slower, the grid no longer filling the GPU)
-  constexpr int SPT = 2;
-  const int sb = blockIdx.x * 32 * SPT + threadIdx.x;
+  constexpr int L = 32 / RPW;            // lanes per row
+  constexpr int SPT = RPW == 1 ? 2 : 1;  // states per thread
+  const int lane = threadIdx.x % L, sub = threadIdx.x / L;
+  const int sb = blockIdx.x * L * SPT + lane;
   bool act[SPT];
 #pragma unroll
-  for (int u = 0; u < SPT; ++u) act[u] = sb + 32 * u < k.nst;
+  for (int u = 0; u < SPT; ++u) act[u] = sb + L * u < k.nst;
   const T *pt = static_cast<const T *>(k.pt);
   const C2 *proj = static_cast<const C2 *>(k.proj);
   C2 *out = static_cast<C2 *>(k.out);
@@ -284,11 +289,14 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
   // lie in the same few spheres, so their projections stay in L1
   const int per = (k.nk + gridDim.y - 1) / gridDim.y;
   const int r0 = blockIdx.y * per, r1 = min(k.nk, r0 + per);
-  for (int i = r0 + threadIdx.y; i < r1; i += 8) {
-    // density of the final row (each warp is one row: the shuffle below is
-    // reached by all its lanes, active or not)
+  for (int i0 = r0 + threadIdx.y * RPW; i0 < r1; i0 += 8 * RPW) {
+    // row of this lane group; density of the final row (the loop bound is
+    // the same for the whole warp: the shuffle below is reached by all its
+    // lanes, active or not)
+    const int i = i0 + sub;
+    const bool rv = i < r1;
     double rs = 0.0;
-    if (act[0]) {
+    if (act[0] && rv) {
     const int row = k.krows[i];
     // the output elements are loaded before the sums, so their latency
     // overlaps theirs (prefetching the next row's metadata as well, or four
@@ -297,7 +305,7 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
     C2 y[SPT], h[SPT];
 #pragma unroll
     for (int u = 0; u < SPT; ++u) {
-      if (act[u]) y[u] = o[32 * u];
+      if (act[u]) y[u] = o[L * u];
       h[u].x = 0;
       h[u].y = 0;
     }
@@ -311,7 +319,7 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
 #pragma unroll
           for (int u = 0; u < SPT; ++u) {
             if (!act[u]) continue;
-            const C2 v = pr[(long long)j * k.proj_ld + 32 * u];
+            const C2 v = pr[(long long)j * k.proj_ld + L * u];
             h[u].x += w * v.x;
             h[u].y += w * v.y;
           }
@@ -327,7 +335,7 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
 #pragma unroll
           for (int u = 0; u < SPT; ++u) {
             if (!act[u]) continue;
-            const C2 v = pr[(long long)j * k.proj_ld + 32 * u];
+            const C2 v = pr[(long long)j * k.proj_ld + L * u];
             g[u].x += w * v.x;
             g[u].y += w * v.y;
           }
@@ -352,17 +360,18 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
         y[u].x += h[u].x;
         y[u].y += h[u].y;
       }
-      o[32 * u] = y[u];
-      if (k.rho_ket) rs += k.rho_w[sb + 32 * u] * (double(y[u].x) * double(y[u].x) + double(y[u].y) * double(y[u].y));
+      o[L * u] = y[u];
+      if (k.rho_ket) rs += k.rho_w[sb + L * u] * (double(y[u].x) * double(y[u].x) + double(y[u].y) * double(y[u].y));
       if (k.obs) {
-        const C2 x = psi0[(long long)row * k.psi0_ld + sb + 32 * u];
+        const C2 x = psi0[(long long)row * k.psi0_ld + sb + L * u];
         kadd(ke[u], double(x.x) * double(h[u].x) + double(x.y) * double(h[u].y));
       }
     }
     }
     if (k.rho_ket) {
-      for (int off = 16; off > 0; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
-      if (threadIdx.x == 0) k.rho_ket[(long long)blockIdx.x * k.nk + i] = rs;
+      // sum over the row's lane group (xor offsets below L stay inside it)
+      for (int off = L / 2; off > 0; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
+      if (lane == 0 && rv) k.rho_ket[(long long)blockIdx.x * k.nk + i] = rs;
     }
   }
   if (k.obs) {
@@ -373,16 +382,17 @@ __global__ void __launch_bounds__(256) ket_kernel(const KetArgs k) {
       red[threadIdx.y][threadIdx.x + 32 * u][1] = ke[u].c;
     }
     __syncthreads();
-    if (threadIdx.y == 0) {
+    if (threadIdx.y == 0 && sub == 0) {
 #pragma unroll
       for (int u = 0; u < SPT; ++u) {
         if (!act[u]) continue;
         Kahan a = {0, 0};
-        for (int y = 0; y < 8; ++y) {
-          kadd(a, red[y][threadIdx.x + 32 * u][0]);
-          a.c += red[y][threadIdx.x + 32 * u][1];
-        }
-        double *o = k.obs + ((long long)blockIdx.y * k.obs_ld + sb + 32 * u) * 2;
+        for (int y = 0; y < 8; ++y)
+          for (int q = 0; q < RPW; ++q) {
+            kadd(a, red[y][q * L + lane + 32 * u][0]);
+            a.c += red[y][q * L + lane + 32 * u][1];
+          }
+        double *o = k.obs + ((long long)blockIdx.y * k.obs_ld + sb + L * u) * 2;
         o[0] = a.s;
         o[1] = a.c;
       }
@@ -407,10 +417,23 @@ hpsi_status launch_ket(const KetArgs &k, cudaStream_t st) {
   if (k.nk == 0) return HPSI_OK;
   using C2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   dim3 grid((k.nst + 63) / 64, ket_row_blocks(k.nk));  // two states per thread
-  if (k.phase)
-    ket_kernel<T, C2, true><<<grid, dim3(32, 8), 0, st>>>(k);
-  else
-    ket_kernel<T, C2, false><<<grid, dim3(32, 8), 0, st>>>(k);
+  // narrow batches: several rows per warp
+  const int rpw = k.nst <= 8 ? 4 : k.nst <= 16 ? 2 : 1;
+  if (k.phase) {
+    if (rpw == 4)
+      ket_kernel<T, C2, true, 4><<<grid, dim3(32, 8), 0, st>>>(k);
+    else if (rpw == 2)
+      ket_kernel<T, C2, true, 2><<<grid, dim3(32, 8), 0, st>>>(k);
+    else
+      ket_kernel<T, C2, true><<<grid, dim3(32, 8), 0, st>>>(k);
+  } else {
+    if (rpw == 4)
+      ket_kernel<T, C2, false, 4><<<grid, dim3(32, 8), 0, st>>>(k);
+    else if (rpw == 2)
+      ket_kernel<T, C2, false, 2><<<grid, dim3(32, 8), 0, st>>>(k);
+    else
+      ket_kernel<T, C2, false><<<grid, dim3(32, 8), 0, st>>>(k);
+  }
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
 }
