@@ -59,6 +59,8 @@ struct hpsi_mesh {
   long long column_planes = 0;          // sum of the tile z extents
   // work list per (z block depth, tile height): key 2 * zb + (height == 8)
   std::map<int, std::pair<int4 *, int>> items;
+  // z block depth of a single-system blocked pass, per state chunk count
+  mutable std::map<int, int> zb_single;
   // domain-parallel meshes: rows [ghost_first, ghost_first + ghost_count) hold
   // other partitions' points; work lists split into the tiles/planes whose
   // stencil reads no ghost row (part 1) and the rest (part 2), per (zb, ty)
