@@ -227,8 +227,26 @@ PassShape blk_shape(int dtype) {
   return s;
 }
 
+// Register-blocked pass over half chunks (64 bytes: FP64 4 states, FP32 8),
+// 16 x 8 tiles, 1 x 4 cells, 256 threads and two CTAs per SM: the default
+// for widths that are a multiple of the half chunk but not of the chunk.
+// Measured on the R = 12 sphere against the one-complex pass: FP32 8 / 24 /
+// 40 states 0.144 / 0.302 / 0.414 -> 0.111 / 0.208 / 0.326 ms, FP64 4 / 12 /
+// 20 states 0.133 / 0.284 / 0.384 -> 0.106 / 0.201 / 0.323 ms.
+PassShape half_chunk_shape(int dtype) {
+  PassShape s = blk_shape(dtype);
+  s.sc /= 2;
+  s.ty = 8;
+  s.rx = 1;
+  s.ry = 4;
+  return s;
+}
+
 PassShape default_shape(int dtype, long long ld) {
-  PassShape s = ld % blk_shape(dtype).sc == 0 ? blk_shape(dtype) : legacy_shape(dtype, ld);
+  const PassShape b = blk_shape(dtype);
+  PassShape s = ld % b.sc == 0         ? b
+                : ld % (b.sc / 2) == 0 ? half_chunk_shape(dtype)
+                                       : legacy_shape(dtype, ld);
   // experiment override: HPSI_PASS_SHAPE64 / HPSI_PASS_SHAPE32 = "sc,ry,zb,unroll,blk,rx,cplx,ty,tma,mb,mma"
   const char *env = std::getenv(dtype == HPSI_C128 ? "HPSI_PASS_SHAPE64" : "HPSI_PASS_SHAPE32");
   if (env) {
@@ -885,7 +903,8 @@ int choose_zb(const hpsi_mesh *m, int chunks, int ty) {
 int choose_zb(const hpsi_mesh *m, int chunks) { return choose_zb(m, chunks, 16); }
 
 // z block depth of a single-system pass over 16 x 8 tiles (the blocked pass,
-// one CTA per SM): the candidate with the shortest simulated makespan.  The
+// ctas_per_sm resident CTAs per SM): the candidate with the shortest
+// simulated makespan.  The
 // work units, in launch order (z band, then raster over the tiles; the state
 // chunks of a unit consecutive), go one after another to the CTA slot that
 // frees first, as the block scheduler hands them out; a unit costs its output
@@ -893,13 +912,14 @@ int choose_zb(const hpsi_mesh *m, int chunks) { return choose_zb(m, chunks, 16);
 // shallower ones balance the tail: on the R = 12 sphere (108 tile columns) the
 // choice is within 0.2 % of the best measured depth for 1 to 16 chunks, where
 // a fixed four-wave target was up to 9.5 % slower with one or two chunks.
-int choose_zb_single(const hpsi_mesh *m, int chunks) {
-  auto it = m->zb_single.find(chunks);
+int choose_zb_single(const hpsi_mesh *m, int chunks, int ctas_per_sm) {
+  const int key = 4 * chunks + ctas_per_sm;
+  auto it = m->zb_single.find(key);
   if (it != m->zb_single.end()) return it->second;
   const int cands[] = {1 << 20, 96, 64, 48, 32, 24, 16};
   int best = 16;
   double best_t = 1e300;
-  const int slots = std::max(1, m->num_sms);
+  const int slots = std::max(1, m->num_sms * ctas_per_sm);
   for (int zb : cands) {
     std::vector<int4> u;  // {band, tile y, tile x, planes}
     for (int by = 0; by < m->tiles_y8; ++by)
@@ -928,16 +948,18 @@ int choose_zb_single(const hpsi_mesh *m, int chunks) {
       best = zb;
     }
   }
-  m->zb_single[chunks] = best;
+  m->zb_single[key] = best;
   return best;
 }
 
 // z block depth of a single-system pass of a shape: the simulated choice for
-// the one-CTA-per-SM blocked shapes over 16 x 8 tiles, the four-wave target
-// otherwise
+// the blocked shapes over 16 x 8 tiles (128-byte chunks: one CTA per SM,
+// 64-byte chunks with 1 x 4 cells: two), the four-wave target otherwise
 int pass_zb(const hpsi_mesh *m, const PassShape &sh, int dtype, int chunks) {
   const int ty = sh.blk ? sh.ty : 16;
-  if (sh.blk && ty == 8 && sh.sc == blk_shape(dtype).sc) return choose_zb_single(m, chunks);
+  const PassShape b = blk_shape(dtype);
+  if (sh.blk && ty == 8 && sh.sc == b.sc) return choose_zb_single(m, chunks, 1);
+  if (sh.blk && ty == 8 && sh.sc == b.sc / 2 && sh.rx == 1 && sh.ry == 4) return choose_zb_single(m, chunks, 2);
   return choose_zb(m, chunks, ty);
 }
 

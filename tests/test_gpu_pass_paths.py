@@ -2,10 +2,11 @@
 
 The register-blocked pass (one real lane per thread, 16 x 8 tiles) serves
 batches whose width is a multiple of its state chunk (8 complex states FP64,
-16 FP32); the one-complex-per-thread pass serves the rest.  Both
-are forced here through the shape override and compared with the oracle and
-with each other: FP64 to 1e-12 relative max-norm per state, FP32 storage to
-2e-5.
+16 FP32); its half-chunk form (64 bytes: 4 FP64, 8 FP32 states, two CTAs per
+SM) serves widths that are a multiple of half a chunk only (FP64 12, FP32 24
+below); the one-complex-per-thread pass serves the rest.  The kernels are
+forced here through the shape override and compared with the oracle and with
+each other: FP64 to 1e-12 relative max-norm per state, FP32 storage to 2e-5.
 """
 import numpy as np
 import pytest
@@ -64,7 +65,8 @@ def _set_path(monkeypatch, path, zb=0):
 
 @pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("dtype,ld,nst", [(np.complex128, 16, 13), (np.complex128, 8, 8),
-                                          (np.complex64, 16, 11), (np.complex64, 32, 20)])
+                                          (np.complex64, 16, 11), (np.complex64, 32, 20),
+                                          (np.complex128, 12, 10), (np.complex64, 24, 21)])
 def test_apply_and_taylor(cuda, monkeypatch, path, dtype, ld, nst):
     import torch
     from hpsi import lib
