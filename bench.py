@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--impl", default="hpsi", choices=["hpsi", "reference"])
     ap.add_argument("--small", action="store_true", help="small case (for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline H.psi and its roofline only (no e2e, FP32, Taylor, TD or other "
+                         "configurations): a short process for profiler captures of the full-size pass")
     ap.add_argument("--configs", action="store_true",
                     help="instead of the headline line, one line per other configuration "
                          "(64^3 box, 2000-step TD, 64 grouped systems, adjoint gradient)")
@@ -640,71 +643,85 @@ def main():
     peak, peak_kind = peaks()
     traffic = profile_traffic()
 
-    # ---- e2e through the C ABI with pinned host buffers (right after the timed
-    # region, before the other workloads) --------------------------------------
-    xh = torch.from_numpy(sysm.psi).pin_memory()
-    yh = torch.zeros((m.np, nst), dtype=torch.complex128).pin_memory()
-    ke = args.steps
-    ham.apply(xh, yh)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(ke):
+    extra = None
+    e2e = None
+    ke = 0
+    if not args.no_extras:
+        # ---- e2e through the C ABI with pinned host buffers (right after the timed
+        # region, before the other workloads) --------------------------------------
+        xh = torch.from_numpy(sysm.psi).pin_memory()
+        yh = torch.zeros((m.np, nst), dtype=torch.complex128).pin_memory()
+        ke = args.steps
         ham.apply(xh, yh)
-    torch.cuda.synchronize()
-    el = max_over_ranks(time.perf_counter() - t0)
-    e2e = world * m.np * nst * ke / el / 1e9
-
-    # ---- extras: FP32 storage, Taylor steps ----------------------------------
-    x32 = x.to(torch.complex64)
-    y32 = y.to(torch.complex64)
-    ms32 = timed(lambda: ham.apply(x32, y32), args.steps, 2)
-    value32 = world * m.np * nst * args.steps / (ms32 / 1e3) / 1e9
-    tk = max(2, args.steps // 4)
-    xt = x.clone()
-    ms_t64 = timed(lambda: ham.taylor_step(xt, 0.02), tk, 1)
-    xt32 = x32.clone()
-    ms_t32 = timed(lambda: ham.taylor_step(xt32, 0.02), tk, 1)
-    # the Taylor step with the density of the propagated batch fused into its
-    # last pass (the fuse_density_exp_apply of the reference's propagation)
-    rho_t = torch.zeros(m.np, dtype=torch.float64, device=dev)
-    wts = np.full(nst, 2.0)
-    ms_td = timed(lambda: ham.taylor_step_density(xt, 0.02, wts, rho=rho_t), tk, 1)
-    ms_rho = timed(lambda: dm.density(xt, wts, rho=rho_t), tk, 1)
-    del xt, xt32
-
-    # ---- TD steps (exp_mid + laser): FP64 plain launches vs FP32 graph replay --
-    # dt = 0.005: at h = 0.2 the order-4 star Laplacian reaches E_max ~ 244 Ha, and
-    # the 4th-order Taylor series is stable only for dt * E_max <= 2 sqrt(2); dt = 0.02
-    # (dt * E_max = 4.9) diverges within a few steps in any implementation.  The
-    # FP32-vs-FP64 observables are compared over the whole 200-step run.
-    dt_td = 0.005
-    ntd = 200
-    laser = dict(E0=0.01, omega=0.057, T=ntd * dt_td)
-    td = {}
-    for name, xs, graph in (("td_fp64_plain", x.clone(), False), ("td_fp32_graph", x32.clone(), True)):
-        xw = xs.clone()
-        ham.td_propagate(xw, 1, dt_td, graph=graph, **laser)  # warm-up (workspaces, graph path)
-        del xw
-        torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
-        E, D, N = ham.td_propagate(xs, ntd, dt_td, graph=graph, **laser)
+        for _ in range(ke):
+            ham.apply(xh, yh)
+        torch.cuda.synchronize()
         el = max_over_ranks(time.perf_counter() - t0)
-        td[name] = {"steps_per_s": ntd / el, "ms_per_step": el / ntd * 1e3, "energy": E, "dipole": D, "norm": N}
-        del xs
-    e64, e32 = td["td_fp64_plain"].pop("energy"), td["td_fp32_graph"].pop("energy")
-    d64, d32 = td["td_fp64_plain"].pop("dipole"), td["td_fp32_graph"].pop("dipole")
-    nn64, nn32 = td["td_fp64_plain"].pop("norm"), td["td_fp32_graph"].pop("norm")
-    td["fp32_vs_fp64"] = {"energy_rel_err_max": float(np.max(np.abs(e32 - e64) / np.abs(e64))),
-                          "dipole_abs_err_max": float(np.max(np.abs(d32 - d64))),
-                          "dipole_rel_err_max": float(np.max(np.abs(d32 - d64)) / max(np.max(np.abs(d64)), 1e-300)),
-                          "norm_rel_err_max": float(np.max(np.abs(nn32 - nn64) / nn64)),
-                          "steps": ntd, "dt": dt_td, "laser": "E0=0.01 w=0.057 sin^2 envelope over the run"}
+        e2e = world * m.np * nst * ke / el / 1e9
 
-    # ---- other configurations, measured in the same run --------------------------
-    box = _box_extra(dev, timed, args.steps)
-    group = _group_extra(dev, args.small, timed)
-    adjoint = _adjoint_extra(dev, args.small)
+        # ---- extras: FP32 storage, Taylor steps ----------------------------------
+        x32 = x.to(torch.complex64)
+        y32 = y.to(torch.complex64)
+        ms32 = timed(lambda: ham.apply(x32, y32), args.steps, 2)
+        value32 = world * m.np * nst * args.steps / (ms32 / 1e3) / 1e9
+        tk = max(2, args.steps // 4)
+        xt = x.clone()
+        ms_t64 = timed(lambda: ham.taylor_step(xt, 0.02), tk, 1)
+        xt32 = x32.clone()
+        ms_t32 = timed(lambda: ham.taylor_step(xt32, 0.02), tk, 1)
+        # the Taylor step with the density of the propagated batch fused into its
+        # last pass (the fuse_density_exp_apply of the reference's propagation)
+        rho_t = torch.zeros(m.np, dtype=torch.float64, device=dev)
+        wts = np.full(nst, 2.0)
+        ms_td = timed(lambda: ham.taylor_step_density(xt, 0.02, wts, rho=rho_t), tk, 1)
+        ms_rho = timed(lambda: dm.density(xt, wts, rho=rho_t), tk, 1)
+        del xt, xt32
+
+        # ---- TD steps (exp_mid + laser): FP64 plain launches vs FP32 graph replay --
+        # dt = 0.005: at h = 0.2 the order-4 star Laplacian reaches E_max ~ 244 Ha, and
+        # the 4th-order Taylor series is stable only for dt * E_max <= 2 sqrt(2); dt = 0.02
+        # (dt * E_max = 4.9) diverges within a few steps in any implementation.  The
+        # FP32-vs-FP64 observables are compared over the whole 200-step run.
+        dt_td = 0.005
+        ntd = 200
+        laser = dict(E0=0.01, omega=0.057, T=ntd * dt_td)
+        td = {}
+        for name, xs, graph in (("td_fp64_plain", x.clone(), False), ("td_fp32_graph", x32.clone(), True)):
+            xw = xs.clone()
+            ham.td_propagate(xw, 1, dt_td, graph=graph, **laser)  # warm-up (workspaces, graph path)
+            del xw
+            torch.cuda.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            E, D, N = ham.td_propagate(xs, ntd, dt_td, graph=graph, **laser)
+            el = max_over_ranks(time.perf_counter() - t0)
+            td[name] = {"steps_per_s": ntd / el, "ms_per_step": el / ntd * 1e3, "energy": E, "dipole": D, "norm": N}
+            del xs
+        e64, e32 = td["td_fp64_plain"].pop("energy"), td["td_fp32_graph"].pop("energy")
+        d64, d32 = td["td_fp64_plain"].pop("dipole"), td["td_fp32_graph"].pop("dipole")
+        nn64, nn32 = td["td_fp64_plain"].pop("norm"), td["td_fp32_graph"].pop("norm")
+        td["fp32_vs_fp64"] = {"energy_rel_err_max": float(np.max(np.abs(e32 - e64) / np.abs(e64))),
+                              "dipole_abs_err_max": float(np.max(np.abs(d32 - d64))),
+                              "dipole_rel_err_max": float(np.max(np.abs(d32 - d64)) / max(np.max(np.abs(d64)), 1e-300)),
+                              "norm_rel_err_max": float(np.max(np.abs(nn32 - nn64) / nn64)),
+                              "steps": ntd, "dt": dt_td, "laser": "E0=0.01 w=0.057 sin^2 envelope over the run"}
+
+        # ---- other configurations, measured in the same run --------------------------
+        box = _box_extra(dev, timed, args.steps)
+        group = _group_extra(dev, args.small, timed)
+        adjoint = _adjoint_extra(dev, args.small)
+        extra = {
+            "fp32_storage_hpsi": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps},
+            "taylor4_fp64": {"steps_per_s": tk / (ms_t64 / 1e3), "ms_per_step": ms_t64 / tk},
+            "taylor4_fp32": {"steps_per_s": tk / (ms_t32 / 1e3), "ms_per_step": ms_t32 / tk},
+            "taylor4_fp64_with_density": {"ms_per_step": ms_td / tk, "ms_density_pass_alone": ms_rho / tk},
+            **td,
+            "config0_box64": box,
+            "config3_group": group,
+            "config4_adjoint": adjoint,
+        }
 
     # ---- CPU baseline and the oracle check of the timed run (rank 0, N=1) -----
     cpu = None
@@ -724,12 +741,10 @@ def main():
                        "step": "one H.psi (kinetic + local + KB) over the whole batch",
                        "l2": "inputs (2.2 GB) larger than L2; no flush",
                        "parallelism": f"replicas x{world}"},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(m.np * nst * S),
-                    "d2h_bytes_per_step": int(m.np * nst * S), "calls": ke},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "traffic_kind": "ncu DRAM bytes of a smaller case of the same kernel, scaled by "
-                                         "point-states (committed profile summary)",
+                         "traffic_kind": "ncu DRAM bytes (read + write) of one full-size launch of the same "
+                                         "kernel (committed profile summary)",
                          "kernel": "pass_blk_kernel FP64 (fused stencil + local potential)",
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": pass_avg_ms,
                          "timing": "pass alone (apply without the KB term), CUDA events over the launches"},
@@ -739,17 +754,12 @@ def main():
                         "ket_fp64": {"launches": nket, "ms": ket_ms}},
             "gpu_launches": launches,
             "clocks": clk.summary(),
-            "extra": {
-                "fp32_storage_hpsi": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps},
-                "taylor4_fp64": {"steps_per_s": tk / (ms_t64 / 1e3), "ms_per_step": ms_t64 / tk},
-                "taylor4_fp32": {"steps_per_s": tk / (ms_t32 / 1e3), "ms_per_step": ms_t32 / tk},
-                "taylor4_fp64_with_density": {"ms_per_step": ms_td / tk, "ms_density_pass_alone": ms_rho / tk},
-                **td,
-                "config0_box64": box,
-                "config3_group": group,
-                "config4_adjoint": adjoint,
-            },
         }
+        if e2e is not None:
+            line["e2e"] = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(m.np * nst * S),
+                           "d2h_bytes_per_step": int(m.np * nst * S), "calls": ke}
+        if extra is not None:
+            line["extra"] = extra
         if err is not None:
             line["err_vs_oracle"] = err
         if cpu:
