@@ -905,8 +905,8 @@ int choose_zb(const hpsi_mesh *m, int chunks) { return choose_zb(m, chunks, 16);
 // z block depth of a single-system pass over 16 x 8 tiles (the blocked pass,
 // ctas_per_sm resident CTAs per SM): the candidate with the shortest
 // simulated makespan.  The
-// work units, in launch order (z band, then raster over the tiles; the state
-// chunks of a unit consecutive), go one after another to the CTA slot that
+// work units, in launch order (z band, then column-major over the tiles; the
+// state chunks of a unit consecutive), go one after another to the CTA slot that
 // frees first, as the block scheduler hands them out; a unit costs its output
 // planes + 8 halo planes + 4 (prologue).  Deeper blocks read fewer halo planes,
 // shallower ones balance the tail: on the R = 12 sphere (108 tile columns) the
@@ -921,12 +921,12 @@ int choose_zb_single(const hpsi_mesh *m, int chunks, int ctas_per_sm) {
   double best_t = 1e300;
   const int slots = std::max(1, m->num_sms * ctas_per_sm);
   for (int zb : cands) {
-    std::vector<int4> u;  // {band, tile y, tile x, planes}
+    std::vector<int4> u;  // {band, tile x, tile y, planes}
     for (int by = 0; by < m->tiles_y8; ++by)
       for (int bx = 0; bx < m->tiles_x; ++bx) {
         const int2 t = m->tile_z8[size_t(by) * m->tiles_x + bx];
         if (t.y < 0) continue;
-        for (int z = t.x; z <= t.y; z += zb) u.push_back(make_int4(z / zb, by, bx, std::min(zb, t.y + 1 - z)));
+        for (int z = t.x; z <= t.y; z += zb) u.push_back(make_int4(z / zb, bx, by, std::min(zb, t.y + 1 - z)));
       }
     std::stable_sort(u.begin(), u.end(), [](const int4 &a, const int4 &b) {
       if (a.x != b.x) return a.x < b.x;
@@ -978,13 +978,19 @@ hpsi_status mesh_items(hpsi_mesh *m, int zb, int ty, const int4 **items, int *ni
         if (t.y < 0) continue;
         for (int z = t.x; z <= t.y; z += zb) v.push_back(make_int4(bx, by, z, std::min(z + zb, t.y + 1)));
       }
-    // launch order: by z band, then raster over the tiles, so that the CTAs in
-    // flight together are spatial neighbours and share their halo rows in L2
+    // launch order: by z band, then column-major over the tiles (tile y
+    // fastest), so that the CTAs in flight together are spatial neighbours and
+    // share their halo rows in L2.  A tile's y halo (4 rows above and below,
+    // 128 cells) is twice its x halo (64 cells): with y fastest the y
+    // neighbours run together.  On the R = 12 sphere (128 states, FP64) the
+    // pass read 3.29 GB from DRAM instead of 4.09 GB in raster order and ran
+    // 0.5 % faster (FP32 1.1 %); strips of 2-6 tile columns and Morton order
+    // measured slower.
     std::stable_sort(v.begin(), v.end(), [zb](const int4 &a, const int4 &b) {
       const int za = a.z / zb, zbb = b.z / zb;
       if (za != zbb) return za < zbb;
-      if (a.y != b.y) return a.y < b.y;
-      return a.x < b.x;
+      if (a.x != b.x) return a.x < b.x;
+      return a.y < b.y;
     });
     int4 *d = nullptr;
     hpsi_status s = dev_alloc(reinterpret_cast<void **>(&d), std::max<size_t>(1, v.size()) * sizeof(int4));
