@@ -47,29 +47,41 @@ struct AdjPtrs {
   const double2 *P[KMAX];      // H^m psi_n
 };
 
-// One warp per mesh row.  For each state: s = sum_j conj(L_j) Phi_j with
+// RPW mesh rows per warp (32 / RPW lanes per row: 2 or 4 rows for batches of
+// at most 16 or 8 states, so lanes past the batch width do not idle), K the
+// Taylor order (a template parameter: the per-element terms stay in registers).
+// For each state: s = sum_j conj(L_j) Phi_j with
 // Phi_j = sum_{m <= K-1-j} c_{j+m+1} P_m; lambda_new = sum_k conj(c_k) L_k
 // written over L_0.  w(r) = sum_i Re s_i; gv[r] += 2 dV w; the eps gradient
 // partial of the block += 2 dV z(r) w, and the same for the leading term.
+template <int K, int RPW>
 __global__ void __launch_bounds__(256) adj_accumulate_kernel(double2 *L0, const AdjPtrs ptr, long long ld, int nst,
                                                              int np, const AdjCoef c, const double *zrow, double dv,
                                                              double *gv, double *geps_partial,
                                                              double *gcont_partial) {
+  constexpr int LN = 32 / RPW;  // lanes per row
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int rows_per_block = blockDim.x >> 5;
+  const int sub = lane / LN, li = lane % LN;
+  const int rows_per_block = (blockDim.x >> 5) * RPW;
   Kahan ke = {0, 0}, kc = {0, 0};
-  for (long long r = (long long)blockIdx.x * rows_per_block + warp; r < np;
-       r += (long long)gridDim.x * rows_per_block) {
+  for (long long r0 = (long long)blockIdx.x * rows_per_block + warp * RPW; r0 < np;
+       r0 += (long long)gridDim.x * rows_per_block) {
+    const long long r = r0 + sub;
+    const bool rv = r < np;
     double wr = 0.0, wc = 0.0;
-    for (int i = lane; i < nst; i += 32) {
+    for (int i = li; rv && i < nst; i += LN) {
       const long long o = r * ld + i;
-      double2 Pm[KMAX], Lk[KMAX + 1];
-      for (int m = 0; m < c.K; ++m) Pm[m] = ptr.P[m][o];
-      for (int k = 0; k <= c.K; ++k) Lk[k] = ptr.L[k][o];
+      double2 Pm[K], Lk[K + 1];
+#pragma unroll
+      for (int m = 0; m < K; ++m) Pm[m] = ptr.P[m][o];
+#pragma unroll
+      for (int k = 0; k <= K; ++k) Lk[k] = ptr.L[k][o];
       double sre = 0.0;
-      for (int j = 0; j < c.K; ++j) {
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
         double pre = 0.0, pim = 0.0;  // Phi_j
-        for (int m = 0; m + j <= c.K - 1; ++m) {
+#pragma unroll
+        for (int m = 0; m + j <= K - 1; ++m) {
           const double ar = c.cre[j + m + 1], ai = c.cim[j + m + 1];
           pre += ar * Pm[m].x - ai * Pm[m].y;
           pim += ar * Pm[m].y + ai * Pm[m].x;
@@ -81,21 +93,35 @@ __global__ void __launch_bounds__(256) adj_accumulate_kernel(double2 *L0, const 
       const double cr = Lk[0].x * Pm[0].x + Lk[0].y * Pm[0].y, ci = Lk[0].x * Pm[0].y - Lk[0].y * Pm[0].x;
       wc += c.cre[1] * cr - c.cim[1] * ci;
       double nre = 0.0, nim = 0.0;  // lambda_new = sum conj(c_k) L_k
-      for (int k = 0; k <= c.K; ++k) {
+#pragma unroll
+      for (int k = 0; k <= K; ++k) {
         const double ar = c.cre[k], ai = -c.cim[k];
         nre += ar * Lk[k].x - ai * Lk[k].y;
         nim += ar * Lk[k].y + ai * Lk[k].x;
       }
       L0[o] = make_double2(nre, nim);
     }
-    for (int off = 16; off > 0; off >>= 1) {
+    // sum over the row's lanes (xor offsets below LN stay inside the group)
+    for (int off = LN / 2; off > 0; off >>= 1) {
       wr += __shfl_xor_sync(0xffffffffu, wr, off);
       wc += __shfl_xor_sync(0xffffffffu, wc, off);
     }
-    if (lane == 0) {
+    if (li == 0 && rv) {
       if (gv) gv[r] += 2.0 * dv * wr;
       kadd(ke, 2.0 * dv * wr * zrow[r]);
       kadd(kc, 2.0 * dv * wc * zrow[r]);
+    }
+  }
+  // the row groups' partials into lane 0, in a fixed order
+#pragma unroll
+  for (int q = 1; q < RPW; ++q) {
+    const double es = __shfl_sync(0xffffffffu, ke.s, q * LN), ec = __shfl_sync(0xffffffffu, ke.c, q * LN);
+    const double cs = __shfl_sync(0xffffffffu, kc.s, q * LN), cc = __shfl_sync(0xffffffffu, kc.c, q * LN);
+    if (lane == 0) {
+      kadd(ke, es);
+      ke.c += ec;
+      kadd(kc, cs);
+      kc.c += cc;
     }
   }
   __shared__ double red[8][4];
@@ -108,7 +134,7 @@ __global__ void __launch_bounds__(256) adj_accumulate_kernel(double2 *L0, const 
   __syncthreads();
   if (threadIdx.x == 0) {
     Kahan a = {0, 0}, b = {0, 0};
-    for (int w = 0; w < rows_per_block; ++w) {
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) {
       kadd(a, red[w][0]);
       a.c += red[w][1];
       kadd(b, red[w][2]);
@@ -121,14 +147,37 @@ __global__ void __launch_bounds__(256) adj_accumulate_kernel(double2 *L0, const 
   }
 }
 
-__global__ void adj_sum_partials(const double *part, int n, double *out) {
-  if (threadIdx.x || blockIdx.x) return;
+template <int K>
+void launch_adj_accumulate(int rpw, unsigned grid, cudaStream_t st, double2 *L0, const AdjPtrs &ptr, long long ld,
+                           int nst, int np, const AdjCoef &c, const double *zrow, double dv, double *gv, double *gp,
+                           double *gcp) {
+  if (rpw == 4)
+    adj_accumulate_kernel<K, 4><<<grid, 256, 0, st>>>(L0, ptr, ld, nst, np, c, zrow, dv, gv, gp, gcp);
+  else if (rpw == 2)
+    adj_accumulate_kernel<K, 2><<<grid, 256, 0, st>>>(L0, ptr, ld, nst, np, c, zrow, dv, gv, gp, gcp);
+  else
+    adj_accumulate_kernel<K, 1><<<grid, 256, 0, st>>>(L0, ptr, ld, nst, np, c, zrow, dv, gv, gp, gcp);
+}
+
+// The two block-partial sums of a step (warp 0: the eps gradient, warp 1: its
+// leading-term form): each lane a compensated sum over a stride of the
+// partials, then lane 0 over the 32 lane sums in lane order (fixed order:
+// deterministic).
+__global__ void adj_sum_partials(const double *part, const double *partc, int n, double *out, double *outc) {
+  const int lane = threadIdx.x & 31;
+  const double *p = threadIdx.x < 32 ? part : partc;
   Kahan a = {0, 0};
-  for (int i = 0; i < n; ++i) {
-    kadd(a, part[2 * i]);
-    a.c += part[2 * i + 1];
+  for (int i = lane; i < n; i += 32) {
+    kadd(a, p[2 * i]);
+    a.c += p[2 * i + 1];
   }
-  *out = a.s + a.c;
+  Kahan t = {0, 0};
+  for (int q = 0; q < 32; ++q) {
+    const double s = __shfl_sync(0xffffffffu, a.s, q), c = __shfl_sync(0xffffffffu, a.c, q);
+    kadd(t, s);
+    t.c += c;
+  }
+  if (lane == 0) *(threadIdx.x < 32 ? out : outc) = t.s + t.c;
 }
 
 // lambda_i = phi_i * ov_i (ov = per-state complex overlap <phi_i|psi_i>, interleaved)
@@ -319,12 +368,28 @@ static hpsi_status adjoint_step_dev(const AdjointRun &R, double eps, double2 *la
   for (int k = 1; k <= R.K && !s; ++k) s = adj_apply(R, eps, ptr.L[k - 1], B.L[k]);
   if (s) return s;
   const double dv = R.h->mesh->box.h[0] * R.h->mesh->box.h[1] * R.h->mesh->box.h[2];
-  adj_accumulate_kernel<<<ADJ_NBLK, 256, 0, R.st>>>(lam, ptr, R.ld, R.nst, R.np, coef, B.zrow, dv, gv, B.part,
-                                                     B.partc);
+  const int rpw = R.nst <= 8 ? 4 : R.nst <= 16 ? 2 : 1;
+  switch (R.K) {
+#define HPSI_ADJ_ACC(KK)                                                                                      \
+  case KK:                                                                                                    \
+    launch_adj_accumulate<KK>(rpw, ADJ_NBLK, R.st, lam, ptr, R.ld, R.nst, R.np, coef, B.zrow, dv, gv, B.part, \
+                              B.partc);                                                                       \
+    break;
+    HPSI_ADJ_ACC(1)
+    HPSI_ADJ_ACC(2)
+    HPSI_ADJ_ACC(3)
+    HPSI_ADJ_ACC(4)
+    HPSI_ADJ_ACC(5)
+    HPSI_ADJ_ACC(6)
+    HPSI_ADJ_ACC(7)
+    HPSI_ADJ_ACC(8)
+#undef HPSI_ADJ_ACC
+    default:
+      set_error("adjoint step: Taylor order out of range");
+      return HPSI_ERR_ARG;
+  }
   HPSI_CHECK_LAUNCH();
-  adj_sum_partials<<<1, 32, 0, R.st>>>(B.part, ADJ_NBLK, geps);
-  HPSI_CHECK_LAUNCH();
-  adj_sum_partials<<<1, 32, 0, R.st>>>(B.partc, ADJ_NBLK, gcont);
+  adj_sum_partials<<<1, 64, 0, R.st>>>(B.part, B.partc, ADJ_NBLK, geps, gcont);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
 }
