@@ -44,8 +44,11 @@ def test_adjoint_forward_matches_oracle(cuda):
     assert np.array_equal(x.cpu().numpy(), psi)  # the input batch is untouched
 
 
-def test_adjoint_gradients_match_finite_differences(cuda):
-    m, v, psi, phi, eps, dm, ham, x, t = _setup(cuda)
+@pytest.mark.parametrize("nst", [4, 12])
+def test_adjoint_gradients_match_finite_differences(cuda, nst):
+    """4 states: four mesh rows per warp in the gradient accumulation; 12
+    states: two rows per warp."""
+    m, v, psi, phi, eps, dm, ham, x, t = _setup(cuda, nst=nst)
     J, ge, gv, gc = ham.adjoint_gradient(x, t, eps, 0.02, ckpt=7)
     rng = np.random.default_rng(3)
     h = 1e-4
