@@ -514,6 +514,7 @@ hpsi_status hpsi_hamiltonian_create(hpsi_mesh *mesh, hpsi_hamiltonian **out) {
   // experiment override: HPSI_BRA_OVERLAP=0 runs the KB bra on the caller's
   // stream before the pass
   if (const char *e = std::getenv("HPSI_BRA_OVERLAP")) h->overlap_bra = std::atoi(e) != 0;
+  if (const char *e = std::getenv("HPSI_PASS_PRIORITY")) h->prio_pass = std::atoi(e) != 0;
   // experiment override: HPSI_FUSED_DENSITY=1 fuses the density of
   // hpsi_taylor_step_density into the last pass
   if (const char *e = std::getenv("HPSI_FUSED_DENSITY")) h->fuse_density = std::atoi(e) != 0;
@@ -543,6 +544,8 @@ hpsi_status hpsi_hamiltonian_destroy(hpsi_hamiltonian *h) {
   dev_free(h->d_err);
   h->lzsmall.release();
   if (h->bra_stream) cudaStreamDestroy(h->bra_stream);
+  if (h->pass_stream) cudaStreamDestroy(h->pass_stream);
+  if (h->pass_join) cudaEventDestroy(h->pass_join);
   if (h->bra_fork) cudaEventDestroy(h->bra_fork);
   if (h->bra_join) cudaEventDestroy(h->bra_join);
   if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
@@ -563,6 +566,10 @@ hpsi_status hpsi_hamiltonian::ensure_bra_stream() {
   HPSI_TRY_CUDA(cudaStreamCreateWithFlags(&bra_stream, cudaStreamNonBlocking));
   HPSI_TRY_CUDA(cudaEventCreateWithFlags(&bra_fork, cudaEventDisableTiming));
   HPSI_TRY_CUDA(cudaEventCreateWithFlags(&bra_join, cudaEventDisableTiming));
+  int least = 0, greatest = 0;
+  HPSI_TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  HPSI_TRY_CUDA(cudaStreamCreateWithPriority(&pass_stream, cudaStreamNonBlocking, greatest));
+  HPSI_TRY_CUDA(cudaEventCreateWithFlags(&pass_join, cudaEventDisableTiming));
   return HPSI_OK;
 }
 
@@ -1343,20 +1350,10 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
     const size_t pbytes = size_t(h->nprojections) * ld * 2 * sizeof(T);
     hpsi_status s = h->projbuf.ensure(pbytes);
     if (s) return s;
-    cudaStream_t bst = st;
     if (h->overlap_bra) {
       s = h->ensure_bra_stream();
       if (s) return s;
-      HPSI_TRY_CUDA(cudaEventRecord(h->bra_fork, st));
-      HPSI_TRY_CUDA(cudaStreamWaitEvent(h->bra_stream, h->bra_fork, 0));
-      bst = h->bra_stream;
       forked = true;
-    }
-    s = run_bra<T>(h, in, in_ld, static_cast<T *>(h->projbuf.ptr), bst);
-    if (forked) HPSI_TRY_CUDA(cudaEventRecord(h->bra_join, bst));
-    if (s) {
-      if (forked) cudaStreamWaitEvent(st, h->bra_join, 0);
-      return s;
     }
   }
   if (obs_partial) {
@@ -1371,12 +1368,38 @@ hpsi_status run_pass(hpsi_hamiltonian *h, int terms, const int *src_map, const T
     rho->fused = true;
   }
   const bool rho_fused = rho && rho->fused;
-  {
-    ProfScope prof(sizeof(T) == 8 ? "pass_fp64" : "pass_fp32", st);
-    hpsi_status s = launch_pass_any<T>(a, shape, pass_in_rows(h, src_map), st);
-    if (forked) HPSI_TRY_CUDA(cudaStreamWaitEvent(st, h->bra_join, 0));
-    if (s) return s;
+  // with the bra on its side stream the pass goes first, on the handle's
+  // high-priority stream: the block scheduler hands freed SMs to pending pass
+  // CTAs before bra CTAs (a pass CTA fills an SM's shared memory, so the two
+  // never share an SM), and the bra mostly fills the pass's last, partial wave
+  const bool pass_side = forked && h->prio_pass;
+  if (forked) HPSI_TRY_CUDA(cudaEventRecord(h->bra_fork, st));
+  cudaStream_t pst = st;
+  if (pass_side) {
+    HPSI_TRY_CUDA(cudaStreamWaitEvent(h->pass_stream, h->bra_fork, 0));
+    pst = h->pass_stream;
   }
+  hpsi_status sp = HPSI_OK;
+  {
+    ProfScope prof(sizeof(T) == 8 ? "pass_fp64" : "pass_fp32", pst);
+    sp = launch_pass_any<T>(a, shape, pass_in_rows(h, src_map), pst);
+  }
+  if (pass_side) HPSI_TRY_CUDA(cudaEventRecord(h->pass_join, pst));
+  hpsi_status sb = HPSI_OK;
+  if (nl) {
+    cudaStream_t bst = st;
+    if (forked) {
+      HPSI_TRY_CUDA(cudaStreamWaitEvent(h->bra_stream, h->bra_fork, 0));
+      bst = h->bra_stream;
+    }
+    // the bra reads only psi, like the pass
+    sb = run_bra<T>(h, in, in_ld, static_cast<T *>(h->projbuf.ptr), bst);
+    if (forked) HPSI_TRY_CUDA(cudaEventRecord(h->bra_join, bst));
+  }
+  if (pass_side) HPSI_TRY_CUDA(cudaStreamWaitEvent(st, h->pass_join, 0));
+  if (forked) HPSI_TRY_CUDA(cudaStreamWaitEvent(st, h->bra_join, 0));
+  if (sp) return sp;
+  if (sb) return sb;
   if (nl) {
     double *kobs = nullptr;
     if (obs_partial) {

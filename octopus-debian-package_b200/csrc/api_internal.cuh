@@ -113,6 +113,11 @@ struct hpsi_hamiltonian {
   bool fuse_density = false;  // hpsi_taylor_step_density: density in the last pass (slower, kept for measurement)
   cudaStream_t bra_stream = nullptr;
   cudaEvent_t bra_fork = nullptr, bra_join = nullptr;
+  // the pass of an H psi with a side-stream bra runs on a high-priority stream
+  // of its own, so that pending pass CTAs take freed SMs before bra CTAs
+  bool prio_pass = true;
+  cudaStream_t pass_stream = nullptr;
+  cudaEvent_t pass_join = nullptr;
   hpsi_status ensure_bra_stream();
   cudaStream_t capture_stream = nullptr;  // graph capture / replay stream of TD runs
   cudaEvent_t capture_event = nullptr;
