@@ -465,7 +465,9 @@ def run_configs(args):
     eps = np.random.default_rng(7).normal(0.0, 0.005, nsteps)
     psi0 = torch.from_numpy(s0.psi).to(dev)
     tg = torch.from_numpy(fixtures.random_states(m, 16, np.random.default_rng(8))).to(dev)
-    ham.adjoint_gradient(psi0, tg, eps[:4], 0.01, ckpt=2)
+    # warm-up with the same call: the checkpoint workspace (3 GB at these sizes)
+    # is allocated once per Hamiltonian, as in repeated optimiser iterations
+    ham.adjoint_gradient(psi0, tg, eps, 0.01, ckpt=25)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     J, ge, gv, gc = ham.adjoint_gradient(psi0, tg, eps, 0.01, ckpt=25)
@@ -489,7 +491,9 @@ def _adjoint_extra(dev, small):
     eps = np.random.default_rng(7).normal(0.0, 0.005, nsteps)
     psi0 = torch.from_numpy(s0.psi).to(dev)
     tg = torch.from_numpy(fixtures.random_states(m, 16, np.random.default_rng(8))).to(dev)
-    ham.adjoint_gradient(psi0, tg, eps[:4], 0.01, ckpt=2)
+    # warm-up with the same call: the checkpoint workspace (3 GB at these sizes)
+    # is allocated once per Hamiltonian, as in repeated optimiser iterations
+    ham.adjoint_gradient(psi0, tg, eps, 0.01, ckpt=25)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     J, ge, gv, gc = ham.adjoint_gradient(psi0, tg, eps, 0.01, ckpt=25)
