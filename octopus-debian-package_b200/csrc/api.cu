@@ -1223,10 +1223,11 @@ hpsi_status run_bra(hpsi_hamiltonian *h, const T *psi, long long ld, T *proj, cu
 template <typename T>
 hpsi_status run_ket(hpsi_hamiltonian *h, const T *proj, long long ld, int nst, T *out, long long out_ld, int mode,
                     double a_re, double a_im, const T *psi0, long long psi0_ld, double *obs, cudaStream_t st,
-                    double *rho_ket = nullptr, const double *rho_w = nullptr) {
+                    double *rho_ket = nullptr, const double *rho_w = nullptr, int row_blocks = 0) {
   KetArgs k;
   k.rho_ket = rho_ket;
   k.rho_w = rho_w;
+  k.row_blocks = row_blocks;
   k.nk = h->nk;
   k.krows = h->d_krows;
   k.kptr = h->d_kptr;
@@ -1425,10 +1426,10 @@ template hpsi_status run_bra<double>(hpsi_hamiltonian *, const double *, long lo
 template hpsi_status run_bra<float>(hpsi_hamiltonian *, const float *, long long, float *, cudaStream_t);
 template hpsi_status run_ket<double>(hpsi_hamiltonian *, const double *, long long, int, double *, long long, int,
                                      double, double, const double *, long long, double *, cudaStream_t, double *,
-                                     const double *);
+                                     const double *, int);
 template hpsi_status run_ket<float>(hpsi_hamiltonian *, const float *, long long, int, float *, long long, int,
                                     double, double, const float *, long long, double *, cudaStream_t, double *,
-                                    const double *);
+                                    const double *, int);
 
 const int *load_map(const hpsi_hamiltonian *h, int set_bc) {
   const hpsi_mesh *m = h->mesh;

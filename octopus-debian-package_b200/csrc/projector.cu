@@ -416,7 +416,8 @@ template <typename T>
 hpsi_status launch_ket(const KetArgs &k, cudaStream_t st) {
   if (k.nk == 0) return HPSI_OK;
   using C2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
-  dim3 grid((k.nst + 63) / 64, ket_row_blocks(k.nk));  // two states per thread
+  const int rb = k.row_blocks > 0 ? std::min(k.row_blocks, ket_row_blocks(k.nk)) : ket_row_blocks(k.nk);
+  dim3 grid((k.nst + 63) / 64, rb);  // two states per thread
   // narrow batches: several rows per warp
   const int rpw = k.nst <= 8 ? 4 : k.nst <= 16 ? 2 : 1;
   if (k.phase) {

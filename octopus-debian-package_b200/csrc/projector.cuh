@@ -47,6 +47,9 @@ struct KetArgs {
   // CTA's states of w_i |out_i(row)|^2, or null
   double *rho_ket = nullptr;
   const double *rho_w = nullptr;
+  // CTA rows of the launch, 0: ket_row_blocks(nk) (a launch that has the GPU
+  // to itself); a grouped step gives each of its concurrent kets fewer
+  int row_blocks = 0;
 };
 
 int bra_ksplit(const ProjArgs &p, int num_sms);
