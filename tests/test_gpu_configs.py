@@ -147,3 +147,51 @@ def test_box64_taylor_fp64(box64):
 def test_box64_taylor_fp32(box64):
     import torch
     _check_taylor(box64, SAMPLE0, torch.complex64, TOL32, 0.01)
+
+
+def test_sphere128_hpsi_linearity(sphere128):
+    """Linearity of the full-size H psi over the whole 128-state batch:
+    H(x1 + c x2) = H x1 + c H x2 for x2 the batch with its states rotated and
+    a complex c, every state compared (not only the oracle's sample)."""
+    import torch
+    s = sphere128
+    m = s.cfg.mesh
+    x1 = s.x
+    x2 = torch.roll(s.x, shifts=37, dims=1)
+    c = 0.3 - 0.7j
+    y1 = torch.zeros((m.np, x1.shape[1]), dtype=x1.dtype, device=x1.device)
+    y2 = torch.zeros_like(y1)
+    y3 = torch.zeros_like(y1)
+    s.ham.apply(x1, y1)
+    s.ham.apply(x2, y2)
+    s.ham.apply(x1 + c * x2, y3)
+    ref = (y1 + c * y2).cpu().numpy()
+    assert rel_maxnorm_per_state(y3.cpu().numpy(), ref) <= 1e-13
+
+
+def test_config3_group_at_full_size(cuda):
+    """Eight of the uneven systems of the grouped configuration at their real
+    sizes (boxes of 32 to 95 cells a side, 4 to 58 states, KB atoms): two
+    grouped Taylor steps (one persistent launch per pass, CUDA graph) against
+    the same systems propagated one by one."""
+    import torch
+    from hpsi import fixtures, lib
+    from hpsi.stencil import laplacian_weights, star_points
+    systems = fixtures.config3(nsys=64)[:8]
+    keep, xs, refs = [], [], []
+    for sy in systems:
+        dm = lib.DeviceMesh(sy.mesh)
+        h = lib.Hamiltonian(dm, laplacian_weights(sy.mesh.spacing), star_points(), v=sy.v, projectors=sy.proj)
+        x = torch.from_numpy(sy.psi).to(cuda)
+        r = x.clone()
+        for _ in range(2):
+            h.taylor_step(r, 0.01)
+        keep.append((dm, h))
+        xs.append(x)
+        refs.append(r)
+    g = lib.Group([h for _, h in keep])
+    g.taylor_steps(xs, 2, 0.01)
+    for sy, x, r in zip(systems, xs, refs):
+        n = sy.mesh.np
+        assert rel_maxnorm_per_state(x[:n].cpu().numpy(), r[:n].cpu().numpy()) <= 1e-13
+    g.close()
