@@ -195,3 +195,30 @@ def test_config3_group_at_full_size(cuda):
         n = sy.mesh.np
         assert rel_maxnorm_per_state(x[:n].cpu().numpy(), r[:n].cpu().numpy()) <= 1e-13
     g.close()
+
+
+def test_config4_adjoint_gradient_full_size(cuda):
+    """The adjoint configuration at its real size (64^3 box, h = 0.25, 16
+    states, 500 steps, checkpoints every 25): the gradient with respect to
+    three control amplitudes against central finite differences of J."""
+    import torch
+    from hpsi import fixtures, lib
+    from hpsi.stencil import laplacian_weights, star_points
+    s0 = fixtures.config0(nst=16)
+    m = s0.mesh
+    dm = lib.DeviceMesh(m)
+    ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=s0.v)
+    eps = np.random.default_rng(7).normal(0.0, 0.005, 500)
+    psi0 = torch.from_numpy(s0.psi).to(cuda)
+    tg = torch.from_numpy(fixtures.random_states(m, 16, np.random.default_rng(8))).to(cuda)
+    J, ge, gv, gc = ham.adjoint_gradient(psi0, tg, eps, 0.01, ckpt=25, want_v=False)
+    assert np.all(np.isfinite(ge))
+    h = 1e-4
+    for k in (3, 250, 497):
+        ep, em = eps.copy(), eps.copy()
+        ep[k] += h
+        em[k] -= h
+        jp = ham.adjoint_gradient(psi0, tg, ep, 0.01, ckpt=25, want_v=False)[0]
+        jm = ham.adjoint_gradient(psi0, tg, em, 0.01, ckpt=25, want_v=False)[0]
+        fd = (jp - jm) / (2 * h)
+        assert abs(fd - ge[k]) <= 1e-5 * np.max(np.abs(ge)), (k, fd, ge[k])
