@@ -268,7 +268,12 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   const T *in_base = static_cast<const T *>(p.in) + col + piece * EPP;
   const long long in_ld2 = 2 * p.in_ld;
   const T *x0_base = static_cast<const T *>(p.psi0) + col + piece * EPP;
-  const long long x0_ld2 = 2 * p.psi0_ld;
+  // row strides in bytes (below 4 GiB, checked at launch): a row address is
+  // one 32 x 32 -> 64-bit multiply-add of a non-negative row index
+  const char *in_bytes = reinterpret_cast<const char *>(in_base);
+  const unsigned in_rb = unsigned(in_ld2) * unsigned(sizeof(T));
+  const char *x0_bytes = reinterpret_cast<const char *>(x0_base);
+  const unsigned x0_rb = unsigned(2 * p.psi0_ld) * unsigned(sizeof(T));
   // side piece of this thread: map cells 4t..4t+3 (t < NMAPP), or rows cells
   long long side_src = 0;
   int side_dst = -1, side_kind = 0;  // 1 map, 2 rows
@@ -325,7 +330,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
           if ((mask >> (i >> 3)) & 1ull) continue;  // this cell arrives with its segment's box
         const int cell = star_cell<LY>(i);
         const int src = map[cell];
-        cp_async16_zfill(halo + cell * SL, in_base + max(src, 0) * in_ld2, src >= 0 ? 16 : 0);
+        cp_async16_zfill(halo + cell * SL, in_bytes + size_t(unsigned(max(src, 0))) * in_rb, src >= 0 ? 16 : 0);
       }
       if constexpr (TMA) {
         // thread s < 40 copies segment s
@@ -373,7 +378,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
         if (LY::IPART && j == LY::IROUNDS - 1 && cell >= LY::IC) break;
         const int row = rows[cell];
         const bool ok = row >= 0 && row < p.np;
-        cp_async16_zfill(x0 + cell * SL, x0_base + (ok ? row : 0) * x0_ld2, ok ? 16 : 0);
+        cp_async16_zfill(x0 + cell * SL, x0_bytes + size_t(unsigned(ok ? row : 0)) * x0_rb, ok ? 16 : 0);
       }
     }
     if (tid < LY::NVP) {
@@ -443,8 +448,9 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   // density weight of this lane's state (fused density of the output)
   [[maybe_unused]] const double wrho = RHO ? p.rho_w[col / 2 + (CPLX ? l : l / 2)] : 0.0;
   E *out = static_cast<E *>(p.out);
-  const long long out_lde = 2 * p.out_ld / LY::LW;  // elements per output row
   const int ocol = col / LY::LW + l;
+  char *out_bytes = reinterpret_cast<char *>(out + ocol);
+  const unsigned out_rb = unsigned(2 * p.out_ld) * unsigned(sizeof(T));  // bytes per output row
   // observables: plain per-thread sums over the thread's z march (a few
   // hundred terms); the sums over threads and CTAs are compensated.  The x/y
   // part of the dipole weight of the thread's first cell, dxy00, is the only
@@ -634,7 +640,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
             pn += n2;
             if (cx || r) pd += n2 * (double(cx) * (p.obs_pol[0] * B.h[0]) + double(r) * (p.obs_pol[1] * B.h[1]));
           }
-          out[row * out_lde + ocol] = val;
+          *reinterpret_cast<E *>(out_bytes + size_t(unsigned(row)) * out_rb) = val;
         }
       if constexpr (RHO) {
         // sum the NC = RX RY cell shares over the SLE lanes of the chunk: a
@@ -796,6 +802,18 @@ __global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT,
   }
 }
 
+// The pass forms row addresses from 32-bit byte strides: every batch row
+// (input, psi0, output) must be shorter than 4 GiB.
+template <typename T>
+bool blk_strides_ok(const PassArgs &a) {
+  const long long lim = 0xffffffffll / (2 * (long long)sizeof(T));
+  if (a.in_ld > lim || a.out_ld > lim || (a.psi0 && a.psi0_ld > lim)) {
+    set_error("launch_pass_blk: a batch row is 4 GiB or longer");
+    return false;
+  }
+  return true;
+}
+
 template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA,
           bool MB>
 hpsi_status launch_blk_mode(const PassArgs &a, const CUtensorMap *tm, cudaStream_t st) {
@@ -814,6 +832,7 @@ hpsi_status launch_blk_mode(const PassArgs &a, const CUtensorMap *tm, cudaStream
     set_error("launch_pass_blk: TMA fill without its tensor map or segment masks");
     return HPSI_ERR_ARG;
   }
+  if (!blk_strides_ok<T>(a)) return HPSI_ERR_ARG;
   CUtensorMap none;
   std::memset(&none, 0, sizeof(none));
   const unsigned nblocks = unsigned(a.nitems) * unsigned(a.chunks);
@@ -846,6 +865,8 @@ hpsi_status launch_blk_group_v(const GroupArgs &g, int grid, cudaStream_t st) {
     attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LY::bytes));
   });
   HPSI_TRY_CUDA(attr);
+  for (int s = 0; s < GROUP_MAX && g.sys[s].in != nullptr; ++s)
+    if (!blk_strides_ok<T>(g.sys[s])) return HPSI_ERR_ARG;
   kern<<<grid, LY::NT, LY::bytes, st>>>(g);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
