@@ -141,6 +141,25 @@ __device__ __forceinline__ int star_cell(int i) {
   return (HAL + TY + i / TX) * HX + HAL + i % TX;
 }
 
+// Halo-plane cell of copy round j of copy cell c (c < NT / PCS) of the fill.
+// With 16 x 8 tiles and 64 copy cells per round the five rounds cover the 320
+// star cells as blocks with two per-thread bases: round 0 the top HAL rows over
+// the tile's columns (row c / 16), round 4 the bottom rows (the same cells 12
+// rows lower), rounds 1-3 the eight rows beside and across the tile in three
+// column blocks of eight (row 4 + c / 8, column c % 8 + 8 (j - 1)), so that
+// every round's cell is a base plus a constant.  Other shapes (and the TMA
+// fill, whose segments follow the star order) use the star order.
+template <class LY, bool STAR_ORDER>
+__device__ __forceinline__ int fill_cell(int c, int j) {
+  constexpr int HX = LY::HX, HAL = LY::HAL, TX = LY::TX;
+  if constexpr (!STAR_ORDER && TX == 16 && LY::TY == 8 && LY::NT / LY::PCS == 64) {
+    if (j == 0 || j == 4) return (c >> 4) * HX + HAL + (c & 15) + (j == 4 ? 12 * HX : 0);
+    return (HAL + (c >> 3)) * HX + (c & 7) + 8 * (j - 1);
+  } else {
+    return star_cell<LY>(c + j * (LY::NT / LY::PCS));
+  }
+}
+
 // 16-byte cp.async that reads `bytes` (16 or 0) and zero-fills the rest
 __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, int bytes) {
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -328,7 +347,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
         if (LY::SPART && j == LY::SROUNDS - 1 && i >= LY::SC) break;
         if constexpr (TMA)
           if ((mask >> (i >> 3)) & 1ull) continue;  // this cell arrives with its segment's box
-        const int cell = star_cell<LY>(i);
+        const int cell = fill_cell<LY, TMA>(cpc, j);
         const int src = map[cell];
         cp_async16_zfill(halo + cell * SL, in_bytes + size_t(unsigned(max(src, 0))) * in_rb, src >= 0 ? 16 : 0);
       }
@@ -377,7 +396,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
         const int cell = cpc + j * (LY::NT / PCS);
         if (LY::IPART && j == LY::IROUNDS - 1 && cell >= LY::IC) break;
         const int row = rows[cell];
-        const bool ok = row >= 0 && row < p.np;
+        const bool ok = unsigned(row) < unsigned(p.np);  // row >= 0 && row < np
         cp_async16_zfill(x0 + cell * SL, x0_bytes + size_t(unsigned(ok ? row : 0)) * x0_rb, ok ? 16 : 0);
       }
     }
@@ -617,7 +636,7 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
             }
           }
           const int row = rowv[cx][r];
-          const bool ok = row >= 0 && row < p.np;
+          const bool ok = unsigned(row) < unsigned(p.np);  // row >= 0 && row < np
           if constexpr (RHO) {
             // this lane's share of the output's density, w_i |val_i|^2
             if constexpr (CPLX)
