@@ -567,10 +567,13 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 #pragma unroll
             for (int c2 = 0; c2 < RX; ++c2)
               if (c2 != cx) acc[c2][r][S4] = fmae(wsel_t<T>(p.wx, p.wxf, cx - c2 + 4), val, acc[c2][r][S4]);
+            // slot (K + 8) % 9 was emitted by the previous plane: this is the
+            // first term of its next output plane (no reset after the emit)
 #pragma unroll
             for (int j = 0; j < 9; ++j)
               if (j != 4)
-                acc[cx][r][(j + K) % 9] = fmae(wsel_t<T>(p.wz, p.wzf, 8 - j), val, acc[cx][r][(j + K) % 9]);
+                acc[cx][r][(j + K) % 9] = fmae(wsel_t<T>(p.wz, p.wzf, 8 - j), val,
+                                               j == 8 ? ezero<E>() : acc[cx][r][(j + K) % 9]);
           }
         }
       }
@@ -589,6 +592,12 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
           }
         }
       }
+    } else {
+      // skipped plane: the slot emitted by the previous plane starts at zero
+#pragma unroll
+      for (int cx = 0; cx < RX; ++cx)
+#pragma unroll
+        for (int r = 0; r < RY; ++r) acc[cx][r][(K + 8) % 9] = ezero<E>();
     }
 
     // outputs of plane zo = pz - 4 are complete (slot K)
@@ -623,7 +632,6 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
         for (int r = 0; r < RY; ++r) {
           [[maybe_unused]] const int cell = (by + r) * TX + bx + cx;
           const E h = acc[cx][r][K];
-          acc[cx][r][K] = ezero<E>();
           E val = h;
           if constexpr (HORNER) {
             const E x0 = x0s[cell * SLE];
@@ -698,11 +706,6 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
         sn += pn;
         sd += pn * (dxy00 + p.obs_pol[2] * B.h[2] * double(zo + B.lo[2])) + pd;
       }
-    } else {
-#pragma unroll
-      for (int cx = 0; cx < RX; ++cx)
-#pragma unroll
-        for (int r = 0; r < RY; ++r) acc[cx][r][K] = ezero<E>();
     }
     if constexpr (MB) {
       mbar_arrive(empty_bar(k));  // this thread is done with plane k
