@@ -235,7 +235,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // after the next plane's arithmetic, so a warp may run one plane ahead of the
 // slowest one.  Every wait is bounded (HPSI_ERR_TIMEOUT in p.err).
 template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX_, int RY_, bool CPLX, int TY_, int CB_,
-          bool TMA = false, bool MB = false>
+          bool TMA = false, bool MB = false, bool FLD = true>
 __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const int chunk, unsigned char *smem,
                                          const CUtensorMap *tm = nullptr) {
   constexpr bool X0 = HORNER || OBS;
@@ -461,7 +461,8 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
   const double fz = p.fld[2] * fscale * B.h[2];
   const double fx0 = fscale * p.fld[0] * B.h[0], fy0 = fscale * p.fld[1] * B.h[1];
   const double fxy0 = fx0 * double(cx0 + bx + B.lo[0]) + fy0 * double(cy0 + by + B.lo[1]);
-  const bool has_field = fz != 0.0 || fx0 != 0.0 || fy0 != 0.0;  // uniform over the grid
+  // uniform over the grid; FLD = false: compiled without the field term
+  const bool has_field = FLD && (fz != 0.0 || fx0 != 0.0 || fy0 != 0.0);
   const T are = static_cast<T>(p.a_re), aim = static_cast<T>(p.a_im);
   const bool odd = !CPLX && (l & 1) != 0;
   // density weight of this lane's state (fused density of the output)
@@ -795,13 +796,13 @@ __device__ __forceinline__ void blk_body(const PassArgs &p, const int ih, const 
 }
 
 template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA,
-          bool MB>
+          bool MB, bool FLD>
 __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::NT,
                                   BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>::CTAS)
     pass_blk_kernel(const __grid_constant__ PassArgs p, const __grid_constant__ CUtensorMap tm) {
   extern __shared__ __align__(128) unsigned char smem[];
-  blk_body<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA, MB>(p, blockIdx.x / p.chunks, blockIdx.x % p.chunks,
-                                                                   smem, &tm);
+  blk_body<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA, MB, FLD>(p, blockIdx.x / p.chunks,
+                                                                        blockIdx.x % p.chunks, smem, &tm);
 }
 
 // Many systems in one persistent launch (Horner passes): each CTA takes
@@ -837,11 +838,11 @@ bool blk_strides_ok(const PassArgs &a) {
 }
 
 template <typename T, bool HORNER, bool OBS, bool RHO, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA,
-          bool MB>
+          bool MB, bool FLD>
 hpsi_status launch_blk_mode(const PassArgs &a, const CUtensorMap *tm, cudaStream_t st) {
   using LY = BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, CB>;
   constexpr size_t SMEM = TMA ? LY::bytes_tma : MB ? LY::bytes_mb : LY::bytes;
-  auto kern = pass_blk_kernel<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA, MB>;
+  auto kern = pass_blk_kernel<T, HORNER, OBS, RHO, U, RX, RY, CPLX, TY, CB, TMA, MB, FLD>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
@@ -863,6 +864,16 @@ hpsi_status launch_blk_mode(const PassArgs &a, const CUtensorMap *tm, cudaStream
   return HPSI_OK;
 }
 
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA, bool MB, bool FLD>
+hpsi_status launch_blk_modes(const PassArgs &a, const CUtensorMap *tm, cudaStream_t st) {
+  const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr, rho = a.rho_part != nullptr;
+  if (horner && obs) return launch_blk_mode<T, true, true, false, U, RX, RY, CPLX, TY, CB, TMA, MB, FLD>(a, tm, st);
+  if (horner && rho) return launch_blk_mode<T, true, false, true, U, RX, RY, CPLX, TY, CB, TMA, MB, FLD>(a, tm, st);
+  if (horner) return launch_blk_mode<T, true, false, false, U, RX, RY, CPLX, TY, CB, TMA, MB, FLD>(a, tm, st);
+  if (obs) return launch_blk_mode<T, false, true, false, U, RX, RY, CPLX, TY, CB, TMA, MB, FLD>(a, tm, st);
+  return launch_blk_mode<T, false, false, false, U, RX, RY, CPLX, TY, CB, TMA, MB, FLD>(a, tm, st);
+}
+
 template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB, bool TMA = false, bool MB = false>
 hpsi_status launch_blk_u(const PassArgs &a, const CUtensorMap *tm, cudaStream_t st) {
   const bool horner = a.mode == PASS_HORNER, obs = a.obs != nullptr, rho = a.rho_part != nullptr;
@@ -870,11 +881,13 @@ hpsi_status launch_blk_u(const PassArgs &a, const CUtensorMap *tm, cudaStream_t 
     set_error("launch_pass_blk: the density is fused into Horner passes without observables only");
     return HPSI_ERR_UNSUPPORTED;
   }
-  if (horner && obs) return launch_blk_mode<T, true, true, false, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
-  if (horner && rho) return launch_blk_mode<T, true, false, true, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
-  if (horner) return launch_blk_mode<T, true, false, false, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
-  if (obs) return launch_blk_mode<T, false, true, false, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
-  return launch_blk_mode<T, false, false, false, U, RX, RY, CPLX, TY, CB, TMA, MB>(a, tm, st);
+  // the default 16 x 8 shapes also come without the laser term, for passes
+  // with no field set (fewer registers and branches per plane)
+  constexpr bool NOFLD = !TMA && !MB && U == 9 && RX == 2 && RY == 2 && TY == 8 && CB == 128;
+  if constexpr (NOFLD)
+    if (a.fld[0] == 0.0 && a.fld[1] == 0.0 && a.fld[2] == 0.0)
+      return launch_blk_modes<T, U, RX, RY, CPLX, TY, CB, TMA, MB, false>(a, tm, st);
+  return launch_blk_modes<T, U, RX, RY, CPLX, TY, CB, TMA, MB, true>(a, tm, st);
 }
 
 template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
