@@ -807,7 +807,8 @@ __global__ void __launch_bounds__(BlkLayout<T, HORNER || OBS, RX, RY, CPLX, TY, 
 
 // Many systems in one persistent launch (Horner passes): each CTA takes
 // (system, item, chunk) units from a list sorted by cost until it is empty.
-template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
+// FLD = false: no system of the launch has a laser field.
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB, bool FLD>
 __global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT,
                                   BlkLayout<T, true, RX, RY, CPLX, TY, CB>::CTAS)
     pass_blk_group_kernel(const __grid_constant__ GroupArgs g) {
@@ -820,7 +821,7 @@ __global__ void __launch_bounds__(BlkLayout<T, true, RX, RY, CPLX, TY, CB>::NT,
     __syncthreads();
     if (u >= g.nunits) break;
     const int4 W = g.units[u];  // {system, item, chunk, -}
-    blk_body<T, true, false, false, U, RX, RY, CPLX, TY, CB>(g.sys[W.x], W.y, W.z, smem);
+    blk_body<T, true, false, false, U, RX, RY, CPLX, TY, CB, false, false, FLD>(g.sys[W.x], W.y, W.z, smem);
     __syncthreads();
   }
 }
@@ -890,21 +891,30 @@ hpsi_status launch_blk_u(const PassArgs &a, const CUtensorMap *tm, cudaStream_t 
   return launch_blk_modes<T, U, RX, RY, CPLX, TY, CB, TMA, MB, true>(a, tm, st);
 }
 
-template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
-hpsi_status launch_blk_group_v(const GroupArgs &g, int grid, cudaStream_t st) {
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB, bool FLD>
+hpsi_status launch_blk_group_f(const GroupArgs &g, int grid, cudaStream_t st) {
   using LY = BlkLayout<T, true, RX, RY, CPLX, TY, CB>;
-  auto kern = pass_blk_group_kernel<T, U, RX, RY, CPLX, TY, CB>;
+  auto kern = pass_blk_group_kernel<T, U, RX, RY, CPLX, TY, CB, FLD>;
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [&] {
     attr = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LY::bytes));
   });
   HPSI_TRY_CUDA(attr);
-  for (int s = 0; s < GROUP_MAX && g.sys[s].in != nullptr; ++s)
-    if (!blk_strides_ok<T>(g.sys[s])) return HPSI_ERR_ARG;
   kern<<<grid, LY::NT, LY::bytes, st>>>(g);
   HPSI_CHECK_LAUNCH();
   return HPSI_OK;
+}
+
+template <typename T, int U, int RX, int RY, bool CPLX, int TY, int CB>
+hpsi_status launch_blk_group_v(const GroupArgs &g, int grid, cudaStream_t st) {
+  bool fld = false;
+  for (int s = 0; s < GROUP_MAX && g.sys[s].in != nullptr; ++s) {
+    if (!blk_strides_ok<T>(g.sys[s])) return HPSI_ERR_ARG;
+    fld = fld || g.sys[s].fld[0] != 0.0 || g.sys[s].fld[1] != 0.0 || g.sys[s].fld[2] != 0.0;
+  }
+  return fld ? launch_blk_group_f<T, U, RX, RY, CPLX, TY, CB, true>(g, grid, st)
+             : launch_blk_group_f<T, U, RX, RY, CPLX, TY, CB, false>(g, grid, st);
 }
 
 // chunk bytes of a shape: sc complex states of the storage type
