@@ -104,3 +104,42 @@ def test_group_blocked_pass_matches_single_systems(cuda, dtype):
             b = r.cpu().numpy()[:, :nst].astype(np.complex128)
             assert rel_maxnorm_per_state(a, b) <= tol
     g.close()
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_group_with_laser_field_matches_single_systems(cuda, dtype):
+    """Systems with a laser field in the group (the persistent pass with the
+    field term; without a field in any system it takes the field-free form):
+    each system as its own Taylor steps with the same field."""
+    import torch
+    from hpsi import lib
+    from hpsi.stencil import laplacian_weights, star_points
+    tdt = torch.complex128 if dtype == "c128" else torch.complex64
+    chunk = 8 if dtype == "c128" else 16
+    specs = [(21, 14, chunk, 2), (22, 17, 2 * chunk, 0), (23, 11, chunk, 1)]
+    fields = [((0.3, -0.5, 0.8), 0.05), None, ((0.0, 0.0, 1.0), -0.02)]
+    hams, xs, refs = [], [], []
+    for (seed, n, nst, natoms), fld in zip(specs, fields):
+        m, v, proj, psi = _system(seed, n, nst, natoms)
+        dm = lib.DeviceMesh(m)
+        ham = lib.Hamiltonian(dm, laplacian_weights(m.spacing), star_points(), v=v, projectors=proj)
+        if fld is not None:
+            ham.set_field(*fld)
+        x = torch.zeros((m.np_part, nst), dtype=tdt, device=cuda)
+        x[:, :nst] = torch.from_numpy(psi).to(tdt)
+        r = x.clone()
+        for _ in range(3):
+            ham.taylor_step(r, 0.02)
+        hams.append((dm, ham))
+        xs.append(x)
+        refs.append(r)
+    g = lib.Group([h for _, h in hams])
+    tol = 1e-13 if dtype == "c128" else 1e-6
+    ys = [x.clone() for x in xs]
+    g.taylor_steps(ys, 3, 0.02)
+    torch.cuda.synchronize()
+    for y, r in zip(ys, refs):
+        a = y.cpu().numpy().astype(np.complex128)
+        b = r.cpu().numpy().astype(np.complex128)
+        assert rel_maxnorm_per_state(a, b) <= tol
+    g.close()
